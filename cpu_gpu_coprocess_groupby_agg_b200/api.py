@@ -1,0 +1,231 @@
+"""Python host API over the C ABI (``include/gba.h``).
+
+``Context.groupby`` takes device-resident torch tensors; ``Context.groupby_host``
+takes numpy arrays in host memory (pinned or not) and returns numpy results.
+Every call goes through ``libgba.so``; there is no fallback path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Sequence
+
+import numpy as np
+
+from . import _abi as A
+
+_OPS = {"sum": A.SUM, "count": A.COUNT, "min": A.MIN, "max": A.MAX}
+
+
+def _np_type(a: np.ndarray) -> int:
+    return {np.dtype(np.int32): A.I32, np.dtype(np.uint32): A.U32, np.dtype(np.int64): A.I64,
+            np.dtype(np.float32): A.F32}[a.dtype]
+
+
+def _torch_type(t, unsigned: bool = False) -> int:
+    import torch
+    m = {torch.int32: A.U32 if unsigned else A.I32, torch.int64: A.I64, torch.float32: A.F32}
+    if t.dtype not in m:
+        raise TypeError(f"unsupported column dtype {t.dtype}")
+    return m[t.dtype]
+
+
+def parse_aggs(aggs: Sequence) -> list[tuple[int, int]]:
+    """[("sum", 0), ("count", None), ...] -> [(op, col), ...]"""
+    out = []
+    for op, col in aggs:
+        o = _OPS[op] if isinstance(op, str) else int(op)
+        out.append((o, 0 if col is None else int(col)))
+    return out
+
+
+def agg_is_fp(op: int, col_type: int) -> bool:
+    return op == A.SUM and col_type == A.F32
+
+
+def make_knobs(**kw) -> A.Knobs:
+    k = A.Knobs()
+    A.lib().gba_default_knobs(C.byref(k))
+    for name, val in kw.items():
+        if name == "sizing" and isinstance(val, str):
+            val = {"plain": A.SIZING_PLAIN, "learned": A.SIZING_LEARNED, "fixed": A.SIZING_FIXED}[val]
+        if name == "strategy" and isinstance(val, str):
+            val = {"auto": A.STRATEGY_AUTO, "table": A.STRATEGY_TABLE, "partition": A.STRATEGY_PARTITION}[val]
+        setattr(k, name, val)
+    return k
+
+
+def build_query(n: int, key_ptr: int, key_type: int, cols: Sequence[tuple[int, int]],
+                aggs: Sequence[tuple[int, int]]) -> A.Query:
+    q = A.Query()
+    q.n_rows = n
+    q.key.type = key_type
+    q.key.data = key_ptr
+    q.n_cols = len(cols)
+    for i, (ptr, t) in enumerate(cols):
+        q.cols[i].type = t
+        q.cols[i].data = ptr
+    q.n_aggs = len(aggs)
+    for i, (op, col) in enumerate(aggs):
+        q.aggs[i].op = op
+        q.aggs[i].col = col
+    return q
+
+
+@dataclass
+class Result:
+    keys: object
+    aggs: list
+    n_groups: int
+    stats: dict = field(default_factory=dict)
+
+
+class Context:
+    """One device context (workspace, streams, estimator weights)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = A.lib()
+        h = C.c_void_p()
+        A.check(self._lib.gba_create(C.byref(h), device))
+        self._h = h
+        self.device = device
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.gba_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def stats(self) -> dict:
+        s = A.Stats()
+        A.check(self._lib.gba_last_stats(self._h, C.byref(s)), self._h)
+        d = {name: getattr(s, name) for name, _ in A.Stats._fields_}
+        d["kernel_ms"] = list(s.kernel_ms)
+        return d
+
+    # ---- device-resident ---------------------------------------------------
+    def groupby(self, keys, cols: Sequence = (), aggs: Sequence = (("count", None),), knobs=None,
+                capacity: int | None = None, unsigned_keys: bool = False, stream=None, out=None) -> Result:
+        import torch
+        if not keys.is_cuda:
+            raise ValueError("groupby() takes device tensors; use groupby_host() for host arrays")
+        n = keys.numel()
+        aggs_p = parse_aggs(aggs)
+        col_specs = [(c.data_ptr(), _torch_type(c)) for c in cols]
+        ktype = _torch_type(keys, unsigned_keys)
+        q = build_query(n, keys.data_ptr(), ktype, col_specs, aggs_p)
+        if out is None:
+            cap = capacity if capacity is not None else max(n, 1) + 1
+            okeys = torch.empty(cap, dtype=keys.dtype, device=keys.device)
+            oaggs = [torch.empty(cap, dtype=torch.float64 if agg_is_fp(op, col_specs[col][1] if op != A.COUNT else 0)
+                                 else torch.int64, device=keys.device) for op, col in aggs_p]
+        else:
+            okeys, oaggs = out
+            cap = okeys.numel()
+        o = A.Output()
+        o.keys = okeys.data_ptr()
+        for i, t in enumerate(oaggs):
+            o.aggs[i] = t.data_ptr()
+        o.capacity = cap
+        kn = knobs if isinstance(knobs, A.Knobs) else make_knobs(**(knobs or {}))
+        ng = C.c_int64(0)
+        s = stream if stream is not None else torch.cuda.current_stream(keys.device)
+        st = self._lib.gba_groupby(self._h, C.byref(q), C.byref(o), C.byref(kn), C.c_void_p(s.cuda_stream),
+                                   C.byref(ng))
+        A.check(st, self._h)
+        g = ng.value
+        return Result(okeys[:g], [t[:g] for t in oaggs], g, self.stats())
+
+    # ---- host-resident -----------------------------------------------------
+    def groupby_host(self, keys: np.ndarray, cols: Sequence[np.ndarray] = (), aggs: Sequence = (("count", None),),
+                     knobs=None, capacity: int | None = None, stream=None, out=None) -> Result:
+        n = keys.shape[0]
+        aggs_p = parse_aggs(aggs)
+        keys = np.ascontiguousarray(keys)
+        cols = [np.ascontiguousarray(c) for c in cols]
+        col_specs = [(c.ctypes.data, _np_type(c)) for c in cols]
+        q = build_query(n, keys.ctypes.data, _np_type(keys), col_specs, aggs_p)
+        if out is None:
+            cap = capacity if capacity is not None else max(n, 1) + 1
+            okeys = np.empty(cap, dtype=keys.dtype)
+            oaggs = [np.empty(cap, dtype=np.float64 if (op != A.COUNT and agg_is_fp(op, col_specs[col][1]))
+                              else np.int64) for op, col in aggs_p]
+        else:
+            okeys, oaggs = out
+            cap = okeys.shape[0]
+        o = A.Output()
+        o.keys = okeys.ctypes.data
+        for i, t in enumerate(oaggs):
+            o.aggs[i] = t.ctypes.data
+        o.capacity = cap
+        kn = knobs if isinstance(knobs, A.Knobs) else make_knobs(**(knobs or {}))
+        ng = C.c_int64(0)
+        sp = 0 if stream is None else stream.cuda_stream
+        A.check(self._lib.gba_groupby_host(self._h, C.byref(q), C.byref(o), C.byref(kn), C.c_void_p(sp),
+                                           C.byref(ng)), self._h)
+        g = ng.value
+        return Result(okeys[:g], [t[:g] for t in oaggs], g, self.stats())
+
+
+# ---- seeded synthetic data -------------------------------------------------------
+def gen_spec(seed: int, key_bits: int, ndv: int, zipf_s: float = 0.0, cols: Sequence = (),
+             permute_ids: bool = True, avoid_all_ones: bool = False) -> A.GenSpec:
+    """cols: sequence of ("u32"|"i32"|"i64", lo, hi) uniform, ("normal",), ("ones",)."""
+    sp = A.GenSpec()
+    sp.seed = seed
+    sp.key_bits = key_bits
+    sp.ndv = ndv
+    sp.zipf_s = zipf_s
+    sp.permute_ids = int(permute_ids)
+    sp.avoid_all_ones = int(avoid_all_ones)
+    sp.ncols = len(cols)
+    for i, c in enumerate(cols):
+        kind = c[0]
+        if kind == "normal":
+            sp.col_kind[i] = A.GEN_NORMAL_F32
+        elif kind == "ones":
+            sp.col_kind[i] = A.GEN_ONES_I32
+        else:
+            sp.col_kind[i] = A.GEN_UNIFORM_I64 if kind == "i64" else A.GEN_UNIFORM_I32
+            sp.col_lo[i], sp.col_hi[i] = int(c[1]), int(c[2])
+    return sp
+
+
+def _col_dtype(kind: int):
+    return {A.GEN_UNIFORM_I32: np.int32, A.GEN_UNIFORM_I64: np.int64, A.GEN_NORMAL_F32: np.float32,
+            A.GEN_ONES_I32: np.int32}[kind]
+
+
+def gen_host(spec: A.GenSpec, n: int, row0: int = 0, nthreads: int = 8, key_unsigned: bool = False,
+             out=None):
+    """Generates rows [row0, row0+n) into numpy arrays (or the given ones)."""
+    if out is None:
+        kd = np.int64 if spec.key_bits == 64 else (np.uint32 if key_unsigned else np.int32)
+        keys = np.empty(n, dtype=kd)
+        cols = [np.empty(n, dtype=_col_dtype(spec.col_kind[i])) for i in range(spec.ncols)]
+    else:
+        keys, cols = out
+    ptrs = (C.c_void_p * 4)(*([c.ctypes.data for c in cols] + [None] * (4 - len(cols))))
+    A.check(A.lib().gba_gen_host(C.byref(spec), row0, n, C.c_void_p(keys.ctypes.data), ptrs, nthreads))
+    return keys, cols
+
+
+def gen_device(spec: A.GenSpec, n: int, row0: int = 0, device: int = 0, stream=None):
+    import torch
+    tmap = {np.int32: torch.int32, np.int64: torch.int64, np.float32: torch.float32}
+    keys = torch.empty(n, dtype=torch.int64 if spec.key_bits == 64 else torch.int32, device=f"cuda:{device}")
+    cols = [torch.empty(n, dtype=tmap[_col_dtype(spec.col_kind[i])], device=keys.device) for i in range(spec.ncols)]
+    ptrs = (C.c_void_p * 4)(*([c.data_ptr() for c in cols] + [None] * (4 - len(cols))))
+    s = stream if stream is not None else torch.cuda.current_stream(keys.device)
+    A.check(A.lib().gba_gen_device(C.byref(spec), row0, n, C.c_void_p(keys.data_ptr()), ptrs,
+                                   C.c_void_p(s.cuda_stream)))
+    return keys, cols

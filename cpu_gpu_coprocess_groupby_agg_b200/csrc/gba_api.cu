@@ -1,0 +1,431 @@
+// C ABI: contexts, workspace, query validation and the single-query driver.
+//
+// The reference drives one query as a host loop over tiles with ~6 blocking
+// stream syncs per tile (tiled_groupby_agg_partition/src/group_then_partition.cu:
+// 332-424) and a second host loop over merged partitions
+// (groupby_agg_intra_partition.cu:183-277).  Here one query is three to five
+// kernel launches on one stream with a single host sync at the end, which reads
+// the overflow flags and the group count.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "gba_context.h"
+#include "gba_plan.h"
+
+size_t gba_round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+uint64_t gba_pow2_ceil(uint64_t x) {
+  uint64_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+extern "C" void gba_default_knobs(gba_knobs* k) {
+  std::memset(k, 0, sizeof(*k));
+  k->sizing = GBA_SIZING_PLAIN;
+  k->strategy = GBA_STRATEGY_AUTO;
+  k->load_factor = 0.5;
+  k->preagg = -1;
+  k->use_tma = -1;
+  k->coalesce = -1;
+  k->max_regrow = 4;
+}
+
+extern "C" const char* gba_status_string(gba_status s) {
+  switch (s) {
+    case GBA_OK: return "ok";
+    case GBA_ERR_INVALID_ARG: return "invalid argument";
+    case GBA_ERR_CUDA: return "CUDA error";
+    case GBA_ERR_OOM: return "out of device memory";
+    case GBA_ERR_OUTPUT_CAPACITY: return "output capacity too small";
+    case GBA_ERR_TABLE_OVERFLOW: return "hash table overflow after regrow limit";
+    case GBA_ERR_TIMEOUT: return "bounded device wait timed out";
+    case GBA_ERR_UNSUPPORTED: return "unsupported";
+    case GBA_ERR_BUDGET: return "request exceeds the device-memory budget";
+  }
+  return "unknown status";
+}
+
+extern "C" gba_status gba_create(gba_context** out, int32_t device) {
+  if (!out) return GBA_ERR_INVALID_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return GBA_ERR_CUDA;
+  gba_context* ctx = new gba_context();
+  ctx->device = device;
+  cudaSetDevice(device);
+  cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device);
+  cudaDeviceGetAttribute(&ctx->max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  if (cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return GBA_ERR_CUDA;
+  }
+  for (auto& e : ctx->ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+  for (auto& e : ctx->tev) cudaEventCreate(&e);
+  gba_status st = gba_small_reserve(ctx, 1 << 16);
+  if (st != GBA_OK) {
+    gba_destroy(ctx);
+    return st;
+  }
+  *out = ctx;
+  return GBA_OK;
+}
+
+extern "C" gba_status gba_destroy(gba_context* ctx) {
+  if (!ctx) return GBA_ERR_INVALID_ARG;
+  cudaSetDevice(ctx->device);
+  cudaDeviceSynchronize();
+  if (ctx->ws) cudaFree(ctx->ws);
+  if (ctx->stage) cudaFree(ctx->stage);
+  if (ctx->d_small) cudaFree(ctx->d_small);
+  if (ctx->h_small) cudaFreeHost(ctx->h_small);
+  if (ctx->d_est) cudaFree(ctx->d_est);
+  for (auto& e : ctx->ev)
+    if (e) cudaEventDestroy(e);
+  for (auto& e : ctx->tev)
+    if (e) cudaEventDestroy(e);
+  if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+  delete ctx;
+  return GBA_OK;
+}
+
+extern "C" const char* gba_last_error(const gba_context* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+extern "C" gba_status gba_last_stats(const gba_context* ctx, gba_stats* out) {
+  if (!ctx || !out) return GBA_ERR_INVALID_ARG;
+  *out = ctx->stats;
+  return GBA_OK;
+}
+
+gba_status gba_ws_reserve(gba_context* ctx, size_t bytes, cudaStream_t s) {
+  if (bytes <= ctx->ws_bytes) return GBA_OK;
+  if (ctx->ws) {
+    GBA_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    GBA_CUDA_TRY(ctx, cudaDeviceSynchronize());
+    cudaFree(ctx->ws);
+    ctx->ws = nullptr;
+    ctx->ws_bytes = 0;
+  }
+  const size_t want = gba_round_up(std::max(bytes, size_t(1) << 24), size_t(1) << 21);
+  cudaError_t e = cudaMalloc(&ctx->ws, want);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    ctx->ws = nullptr;
+    ctx->err = std::string("workspace cudaMalloc(") + std::to_string(want) + "): " + cudaGetErrorString(e);
+    return GBA_ERR_OOM;
+  }
+  ctx->ws_bytes = want;
+  return GBA_OK;
+}
+
+gba_status gba_stage_reserve(gba_context* ctx, size_t bytes, cudaStream_t s) {
+  if (bytes <= ctx->stage_bytes) return GBA_OK;
+  if (ctx->stage) {
+    GBA_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    GBA_CUDA_TRY(ctx, cudaDeviceSynchronize());
+    cudaFree(ctx->stage);
+    ctx->stage = nullptr;
+    ctx->stage_bytes = 0;
+  }
+  const size_t want = gba_round_up(std::max(bytes, size_t(1) << 24), size_t(1) << 21);
+  cudaError_t e = cudaMalloc(&ctx->stage, want);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    ctx->stage = nullptr;
+    ctx->err = std::string("staging cudaMalloc(") + std::to_string(want) + "): " + cudaGetErrorString(e);
+    return GBA_ERR_OOM;
+  }
+  ctx->stage_bytes = want;
+  return GBA_OK;
+}
+
+gba_status gba_small_reserve(gba_context* ctx, size_t bytes) {
+  if (bytes <= ctx->d_small_bytes) return GBA_OK;
+  cudaDeviceSynchronize();
+  if (ctx->d_small) cudaFree(ctx->d_small);
+  if (ctx->h_small) cudaFreeHost(ctx->h_small);
+  ctx->d_small = nullptr;
+  ctx->h_small = nullptr;
+  ctx->d_small_bytes = ctx->h_small_bytes = 0;
+  GBA_CUDA_TRY(ctx, cudaMalloc(&ctx->d_small, bytes));
+  GBA_CUDA_TRY(ctx, cudaMallocHost(&ctx->h_small, bytes));
+  ctx->d_small_bytes = ctx->h_small_bytes = bytes;
+  return GBA_OK;
+}
+
+void GbaTimer::begin(int r) {
+  if (!on || n >= 8) return;
+  role[n] = r;
+  cudaEventRecord(ctx->tev[2 * n], s);
+}
+void GbaTimer::end() {
+  if (!on || n >= 8) return;
+  cudaEventRecord(ctx->tev[2 * n + 1], s);
+  ++n;
+}
+void GbaTimer::collect() {
+  for (int i = 0; i < n; ++i) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, ctx->tev[2 * i], ctx->tev[2 * i + 1]) == cudaSuccess)
+      ctx->stats.kernel_ms[role[i]] += ms;
+  }
+  n = 0;
+}
+
+gba_status gba_build_qdesc(gba_context* ctx, const gba_query* q, QDesc* d) {
+  if (!q) return GBA_ERR_INVALID_ARG;
+  std::memset(d, 0, sizeof(*d));
+  if (q->n_rows < 0) {
+    ctx->err = "n_rows < 0";
+    return GBA_ERR_INVALID_ARG;
+  }
+  if (q->key.type != GBA_I32 && q->key.type != GBA_U32 && q->key.type != GBA_I64) {
+    ctx->err = "key type must be GBA_I32, GBA_U32 or GBA_I64";
+    return GBA_ERR_INVALID_ARG;
+  }
+  if (q->n_cols < 0 || q->n_cols > GBA_MAX_COLS || q->n_aggs < 1 || q->n_aggs > GBA_MAX_AGGS) {
+    ctx->err = "n_cols must be in [0, 4] and n_aggs in [1, 8]";
+    return GBA_ERR_INVALID_ARG;
+  }
+  if (q->n_rows > 0 && !q->key.data) {
+    ctx->err = "null key column";
+    return GBA_ERR_INVALID_ARG;
+  }
+  d->keys = q->key.data;
+  d->n = q->n_rows;
+  d->key64 = q->key.type == GBA_I64;
+  d->ncols = q->n_cols;
+  for (int c = 0; c < q->n_cols; ++c) {
+    const int t = q->cols[c].type;
+    if (t != GBA_I32 && t != GBA_U32 && t != GBA_I64 && t != GBA_F32) {
+      ctx->err = "bad column type";
+      return GBA_ERR_INVALID_ARG;
+    }
+    if (q->n_rows > 0 && !q->cols[c].data) {
+      ctx->err = "null value column";
+      return GBA_ERR_INVALID_ARG;
+    }
+    d->cols[c] = q->cols[c].data;
+    d->col_type[c] = t;
+  }
+  d->naccs = q->n_aggs;
+  for (int a = 0; a < q->n_aggs; ++a) {
+    const int op = q->aggs[a].op, c = q->aggs[a].col;
+    if (op == GBA_COUNT) {
+      d->acc_op[a] = ACC_CNT;
+      d->acc_col[a] = 0;
+      d->acc_ctype[a] = GBA_I64;
+      continue;
+    }
+    if (c < 0 || c >= q->n_cols) {
+      ctx->err = "aggregate column index out of range";
+      return GBA_ERR_INVALID_ARG;
+    }
+    const int t = q->cols[c].type;
+    d->acc_col[a] = c;
+    d->acc_ctype[a] = t;
+    if (t == GBA_F32) {
+      if (op != GBA_SUM) {
+        ctx->err = "only SUM is supported on fp32 columns";
+        return GBA_ERR_UNSUPPORTED;
+      }
+      d->acc_op[a] = ACC_ADD_F;
+    } else if (op == GBA_SUM) d->acc_op[a] = ACC_ADD_I;
+    else if (op == GBA_MIN) d->acc_op[a] = ACC_MIN_I;
+    else if (op == GBA_MAX) d->acc_op[a] = ACC_MAX_I;
+    else {
+      ctx->err = "unknown aggregate op";
+      return GBA_ERR_INVALID_ARG;
+    }
+  }
+  return GBA_OK;
+}
+
+static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// ---------------------------------------------------------------------------
+// Plan: everything the single-query driver decides before launching.
+void gba_make_plan(const gba_context* ctx, const QDesc& q, const gba_knobs& k, double predicted_groups,
+                   GbaPlan* p) {
+  p->block = k.block_threads > 0 ? k.block_threads : 512;
+  p->block = std::min(512, std::max(128, p->block / 32 * 32));
+  p->tile_rows = k.tile_rows > 0 ? k.tile_rows : 2048;
+  p->tile_rows = std::max(p->block, p->tile_rows / p->block * p->block);
+  p->nstages = k.nstages > 0 ? std::min(4, k.nstages) : 3;
+  const int64_t ntiles = (q.n + p->tile_rows - 1) / p->tile_rows;
+  const int bps = k.blocks_per_sm > 0 ? k.blocks_per_sm : 1;
+  p->grid = int(std::max<int64_t>(1, std::min<int64_t>(ntiles, int64_t(ctx->sms) * bps)));
+
+  bool tma_ok = aligned16(q.keys) && q.n >= p->tile_rows;
+  for (int c = 0; c < q.ncols; ++c) tma_ok = tma_ok && aligned16(q.cols[c]);
+  p->use_tma = k.use_tma == 0 ? 0 : (tma_ok ? 1 : 0);
+  p->coalesce = k.coalesce == 0 ? 0 : 1;
+
+  const double lf = (k.load_factor > 0.05 && k.load_factor < 0.95) ? k.load_factor : 0.5;
+  double groups_bound;
+  if (k.sizing == GBA_SIZING_FIXED && k.table_slots > 0) groups_bound = double(k.table_slots) * lf;
+  else if (k.sizing == GBA_SIZING_LEARNED && predicted_groups > 0)
+    groups_bound = std::min(double(std::max<int64_t>(q.n, 1)), predicted_groups * 1.5 + 64.0);
+  else groups_bound = double(std::max<int64_t>(q.n, 1));
+  uint64_t cap = (k.sizing == GBA_SIZING_FIXED && k.table_slots > 0) ? uint64_t(k.table_slots)
+                                                                      : gba_pow2_ceil(uint64_t(groups_bound / lf));
+  p->table_slots = std::max<uint64_t>(cap, 64);
+  p->probe_cap = k.probe_cap > 0 ? k.probe_cap : 256;
+
+  // shared-memory table: whatever the pipeline leaves of the opt-in budget
+  int preagg = k.preagg;
+  if (preagg < 0) {
+    preagg = 1;
+    if (k.sizing == GBA_SIZING_LEARNED && predicted_groups > 0 && q.n > 0 &&
+        predicted_groups > 0.5 * double(q.n))
+      preagg = 0;  // nearly all keys distinct: pre-aggregation only costs time
+  }
+  p->preagg = preagg;
+  const size_t fixed = gba_preagg_smem_bytes(q, 0, p->tile_rows, p->nstages, p->use_tma);
+  const size_t slot_bytes = (q.key64 ? 8 : 4) + 8 * size_t(q.naccs);
+  int S = 0;
+  if (preagg) {
+    const size_t room = size_t(ctx->max_smem_optin) > fixed + 1024 ? size_t(ctx->max_smem_optin) - fixed - 1024 : 0;
+    S = int(std::min<size_t>(room / slot_bytes, 16384));
+    if (k.smem_slots > 0) S = std::min(S, k.smem_slots);
+    if (S < 32) S = 0;
+  }
+  p->smem_slots = S;
+  p->smem_probe_cap = k.smem_probe_cap > 0 ? k.smem_probe_cap : 32;
+  p->partition_bits = k.partition_bits;
+}
+
+// One attempt of the table strategy with capacity p.table_slots.
+static gba_status run_table_once(gba_context* ctx, const QDesc& q, const gba_output* out, const GbaPlan& p,
+                                 cudaStream_t s, bool timing, unsigned* flags_out, unsigned long long* count_out) {
+  GbaTimer tm{ctx, s, timing};
+  const size_t stride = 1 + size_t(q.naccs);
+  const size_t table_bytes = (p.table_slots + 1) * stride * 8;
+  gba_status st = gba_ws_reserve(ctx, table_bytes, s);
+  if (st != GBA_OK) return st;
+  unsigned* d_flags = reinterpret_cast<unsigned*>(ctx->d_small);
+  unsigned long long* d_count = reinterpret_cast<unsigned long long*>(ctx->d_small + 8);
+  GBA_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_small, 0, 64, s));
+  GTable t;
+  t.base = static_cast<unsigned long long*>(ctx->ws);
+  t.cap = p.table_slots;
+  t.probe_cap = p.probe_cap;
+  const int init_grid = int(std::min<uint64_t>(uint64_t(ctx->sms) * 16, (table_bytes / 8 + 255) / 256 + 1));
+  tm.begin(0);
+  GBA_CUDA_TRY(ctx, gba_launch_table_init(t, q, init_grid, s));
+  tm.end();
+  int launches = 1;
+  if (q.n > 0) {
+    PreaggCfg c;
+    c.grid = p.grid;
+    c.block = p.block;
+    c.smem_slots = p.smem_slots;
+    c.smem_probe_cap = p.smem_probe_cap;
+    c.tile_rows = p.tile_rows;
+    c.nstages = p.nstages;
+    c.use_tma = p.use_tma;
+    c.coalesce = p.coalesce;
+    tm.begin(1);
+    GBA_CUDA_TRY(ctx, gba_launch_preagg(q, t, c, d_flags, s));
+    tm.end();
+    ++launches;
+  }
+  OutDesc o;
+  o.keys = out->keys;
+  for (int a = 0; a < GBA_MAX_AGGS; ++a) o.accs[a] = static_cast<unsigned long long*>(out->aggs[a]);
+  o.capacity = out->capacity;
+  o.count = d_count;
+  const int cgrid = int(std::min<uint64_t>(uint64_t(ctx->sms) * 8, (p.table_slots + 255) / 256));
+  tm.begin(2);
+  GBA_CUDA_TRY(ctx, gba_launch_compact(t, q, o, std::max(cgrid, 1), s));
+  tm.end();
+  ++launches;
+  GBA_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_small, ctx->d_small, 16, cudaMemcpyDeviceToHost, s));
+  GBA_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+  tm.collect();
+  *flags_out = *reinterpret_cast<unsigned*>(ctx->h_small);
+  *count_out = *reinterpret_cast<unsigned long long*>(ctx->h_small + 8);
+  ctx->stats.kernel_launches += launches;
+  return GBA_OK;
+}
+
+gba_status gba_run_table(gba_context* ctx, const QDesc& q, const gba_output* out, const gba_knobs& k, GbaPlan p,
+                         cudaStream_t s, int64_t* n_groups) {
+  ctx->stats.strategy = GBA_STRATEGY_TABLE;
+  for (int attempt = 0;; ++attempt) {
+    unsigned flags = 0;
+    unsigned long long count = 0;
+    gba_status st = run_table_once(ctx, q, out, p, s, k.timing != 0, &flags, &count);
+    if (st != GBA_OK) return st;
+    ctx->stats.table_slots = int64_t(p.table_slots);
+    ctx->stats.preagg = p.smem_slots > 0;
+    if (flags & GBA_FLAG_WAIT_TIMEOUT) {
+      ctx->err = "a bounded TMA wait timed out";
+      return GBA_ERR_TIMEOUT;
+    }
+    if (flags & GBA_FLAG_TABLE_OVERFLOW) {
+      if (attempt >= k.max_regrow) {
+        ctx->err = "HBM hash table overflow after " + std::to_string(attempt) + " regrows";
+        return GBA_ERR_TABLE_OVERFLOW;
+      }
+      ctx->stats.regrows++;
+      p.table_slots *= 4;
+      continue;
+    }
+    *n_groups = int64_t(count);
+    ctx->stats.n_groups = int64_t(count);
+    if (int64_t(count) > out->capacity) {
+      ctx->err = "output capacity " + std::to_string(out->capacity) + " < " + std::to_string(count) + " groups";
+      return GBA_ERR_OUTPUT_CAPACITY;
+    }
+    return GBA_OK;
+  }
+}
+
+static gba_status check_output(gba_context* ctx, const gba_query* q, const gba_output* out) {
+  if (!out || out->capacity < 0 || (out->capacity > 0 && !out->keys)) {
+    ctx->err = "bad output descriptor";
+    return GBA_ERR_INVALID_ARG;
+  }
+  for (int a = 0; a < q->n_aggs; ++a)
+    if (out->capacity > 0 && !out->aggs[a]) {
+      ctx->err = "null output aggregate column";
+      return GBA_ERR_INVALID_ARG;
+    }
+  return GBA_OK;
+}
+
+extern "C" gba_status gba_groupby(gba_context* ctx, const gba_query* q, const gba_output* out,
+                                  const gba_knobs* knobs, void* stream, int64_t* n_groups) {
+  if (!ctx || !q || !n_groups) return GBA_ERR_INVALID_ARG;
+  cudaSetDevice(ctx->device);
+  ctx->stats = gba_stats{};
+  ctx->stats.predicted_groups = -1;
+  gba_knobs k;
+  if (knobs) k = *knobs;
+  else gba_default_knobs(&k);
+  QDesc qd;
+  gba_status st = gba_build_qdesc(ctx, q, &qd);
+  if (st != GBA_OK) return st;
+  st = check_output(ctx, q, out);
+  if (st != GBA_OK) return st;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+
+  double pred = -1;
+  if (k.sizing == GBA_SIZING_LEARNED) {
+    if (!ctx->est_loaded) {
+      ctx->err = "learned sizing requested but no estimator weights are loaded";
+      return GBA_ERR_INVALID_ARG;
+    }
+    st = gba_predict_groups(ctx, qd, s, &pred);
+    if (st != GBA_OK) return st;
+    ctx->stats.predicted_groups = pred;
+  }
+  GbaPlan p;
+  gba_make_plan(ctx, qd, k, pred, &p);
+  int strategy = k.strategy;
+  if (strategy == GBA_STRATEGY_AUTO) strategy = gba_choose_strategy(ctx, qd, k, pred, p);
+  if (strategy == GBA_STRATEGY_PARTITION) return gba_run_partition(ctx, qd, out, k, p, pred, s, n_groups);
+  return gba_run_table(ctx, qd, out, k, p, s, n_groups);
+}

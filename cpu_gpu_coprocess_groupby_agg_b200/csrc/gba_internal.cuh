@@ -1,0 +1,185 @@
+// Device-side building blocks shared by the group-by kernels (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "gba_kernels.h"
+
+#define GBA_FULL_MASK 0xffffffffu
+
+static constexpr unsigned long long EMPTY64 = ~0ull;
+static constexpr unsigned EMPTY32 = ~0u;
+
+// ---------------------------------------------------------------------------
+// MurmurHash3_x86_32 of a 4-byte or 8-byte little-endian key (the hash the
+// reference uses through cuco::detail::MurmurHash3_32, kernel.cu:22).
+__device__ __forceinline__ uint32_t mm3_round(uint32_t h, uint32_t k) {
+  k *= 0xcc9e2d51u;
+  k = __funnelshift_l(k, k, 15);
+  k *= 0x1b873593u;
+  h ^= k;
+  h = __funnelshift_l(h, h, 13);
+  return h * 5u + 0xe6546b64u;
+}
+__device__ __forceinline__ uint32_t mm3_fmix(uint32_t h) {
+  h ^= h >> 16;
+  h *= 0x85ebca6bu;
+  h ^= h >> 13;
+  h *= 0xc2b2ae35u;
+  h ^= h >> 16;
+  return h;
+}
+__device__ __forceinline__ uint32_t murmur3_32(uint32_t key, uint32_t seed) {
+  return mm3_fmix(mm3_round(seed, key) ^ 4u);
+}
+__device__ __forceinline__ uint32_t murmur3_64(uint64_t key, uint32_t seed) {
+  uint32_t h = mm3_round(seed, uint32_t(key));
+  h = mm3_round(h, uint32_t(key >> 32));
+  return mm3_fmix(h ^ 8u);
+}
+template <bool K64>
+__device__ __forceinline__ uint32_t key_hash(uint64_t k, uint32_t seed) {
+  if constexpr (K64) return murmur3_64(k, seed);
+  else return murmur3_32(uint32_t(k), seed);
+}
+
+// Seed of the table/partition hash used by the engine (the reference's own
+// seed-0 partition function is used only by the drop-in layout).
+static constexpr uint32_t GBA_TABLE_SEED = 0x9747b28cu;
+
+// ---------------------------------------------------------------------------
+// Row access.
+__device__ __forceinline__ uint64_t load_key_g(const QDesc& q, int64_t r) {
+  if (q.key64) return __ldg(static_cast<const unsigned long long*>(q.keys) + r);
+  return __ldg(static_cast<const unsigned*>(q.keys) + r);
+}
+
+// Contribution of row value `raw` (8 raw bytes as loaded) to accumulator a.
+// raw holds the column value bits: i32/u32 in the low word, f32 bits in the low
+// word, i64 in full.
+__device__ __forceinline__ unsigned long long acc_contrib(int op, int ctype, unsigned long long raw) {
+  switch (op) {
+    case ACC_CNT: return 1ull;
+    case ACC_ADD_F: {
+      double d = double(__uint_as_float(unsigned(raw)));
+      return __double_as_longlong(d);
+    }
+    default: {
+      long long v;
+      if (ctype == GBA_I32) v = (long long)(int)(unsigned)raw;
+      else if (ctype == GBA_U32) v = (long long)(unsigned)raw;
+      else v = (long long)raw;
+      return (unsigned long long)v;
+    }
+  }
+}
+
+__device__ __forceinline__ unsigned long long acc_identity(int op) {
+  switch (op) {
+    case ACC_MIN_I: return 0x7fffffffffffffffull;
+    case ACC_MAX_I: return 0x8000000000000000ull;
+    default: return 0ull;  // integer 0 and +0.0 share the bit pattern
+  }
+}
+
+// combine two partial accumulators (register arithmetic)
+__device__ __forceinline__ unsigned long long acc_combine(int op, unsigned long long a, unsigned long long b) {
+  switch (op) {
+    case ACC_MIN_I: return (long long)a < (long long)b ? a : b;
+    case ACC_MAX_I: return (long long)a > (long long)b ? a : b;
+    case ACC_ADD_F: return __double_as_longlong(__longlong_as_double(a) + __longlong_as_double(b));
+    default: return a + b;
+  }
+}
+
+// atomic combine into shared or global memory (generic address)
+__device__ __forceinline__ void acc_atomic(int op, unsigned long long* p, unsigned long long v) {
+  switch (op) {
+    case ACC_MIN_I: atomicMin(reinterpret_cast<long long*>(p), (long long)v); break;
+    case ACC_MAX_I: atomicMax(reinterpret_cast<long long*>(p), (long long)v); break;
+    case ACC_ADD_F: atomicAdd(reinterpret_cast<double*>(p), __longlong_as_double(v)); break;
+    default: atomicAdd(p, v);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Global table insert of one (key, partial accumulators) pair.  Linear probing
+// from the hashed slot, capped at t.probe_cap probes; on failure the overflow
+// flag is raised and the pair is dropped (the host re-runs the query with a
+// larger table, so a result is never reported from an overflowed table).
+template <bool K64>
+__device__ __forceinline__ void gtable_insert(const GTable& t, int naccs, const int* ops, uint64_t key, uint32_t h,
+                                              const unsigned long long* vals, unsigned* flags) {
+  const int stride = 1 + naccs;
+  unsigned long long* slotp;
+  if (key == (K64 ? EMPTY64 : uint64_t(EMPTY32))) {
+    slotp = t.base + t.cap * stride;
+    if (slotp[0] == 0ull) atomicExch(slotp, 1ull);
+  } else {
+    uint64_t s = (uint64_t(h) * t.cap) >> 32;  // cap <= 2^32
+    int p = 0;
+    for (;;) {
+      slotp = t.base + s * stride;
+      unsigned long long cur = *(volatile unsigned long long*)slotp;
+      if (cur == key) break;
+      if (cur == EMPTY64) {
+        unsigned long long prev = atomicCAS(slotp, EMPTY64, key);
+        if (prev == EMPTY64 || prev == key) break;
+      }
+      if (++p >= t.probe_cap) {
+        atomicOr(flags, GBA_FLAG_TABLE_OVERFLOW);
+        return;
+      }
+      s = (s + 1 == t.cap) ? 0 : s + 1;
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < GBA_MAX_AGGS; ++a)
+    if (a < naccs) acc_atomic(ops[a], slotp + 1 + a, vals[a]);
+}
+
+// ---------------------------------------------------------------------------
+// TMA bulk copy + mbarrier helpers (no multicast anywhere in this library).
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: returns false (and raises the timeout flag) after max_iter
+// unsuccessful polls.  try_wait itself suspends for a hardware-chosen interval,
+// so max_iter = 1<<22 bounds the wait to well under a few seconds.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, unsigned* flags) {
+  for (unsigned it = 0; it < (1u << 22); ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  atomicOr(flags, GBA_FLAG_WAIT_TIMEOUT);
+  return false;
+}
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }

@@ -1,0 +1,423 @@
+// Tiled hash pre-aggregation + global table + final compaction (sm_100a).
+//
+// Replaces the reference's per-tile aggregation chain (tiled_groupby_agg_partition/
+// src/kernel.cu:9-186 driven by group_then_partition.cu:24-246: a one-probe
+// "one-third" table in HBM, three CUB scans, a linear-probe spill table and two
+// compaction kernels, with three host round-trips per tile) by:
+//
+//   k_table_init   - fills the HBM table with the empty key and identities.
+//   k_preagg       - persistent CTAs stream row tiles into shared memory with
+//                    TMA bulk copies (cp.async.bulk + mbarrier, no multicast),
+//                    coalesce equal keys inside each warp with __match_any_sync,
+//                    aggregate into a shared-memory open-addressing table with a
+//                    capped probe count, send rows that do not fit to the HBM
+//                    table, and flush the shared table to HBM at the end.
+//   k_compact      - the final reduce: writes every occupied slot once to the
+//                    caller's output columns (warp-aggregated output cursor).
+#include "gba_internal.cuh"
+#include <type_traits>
+
+namespace {
+
+struct PreaggParams {
+  QDesc q;
+  GTable gt;
+  int S;          // shared-memory table slots (0 = no pre-aggregation)
+  int sprobe;     // probe cap in the shared table
+  int T;          // rows per tile (multiple of blockDim.x and of 4)
+  int nstages;    // TMA pipeline depth (1..4)
+  int use_tma;    // 1: full tiles arrive by cp.async.bulk
+  int coalesce;   // 1: __match_any_sync pre-combining
+  unsigned* flags;
+};
+
+constexpr int kMaxStages = 4;
+
+__host__ __device__ inline int key_bytes(const QDesc& q) { return q.key64 ? 8 : 4; }
+__host__ __device__ inline int col_bytes(int t) { return t == GBA_I64 ? 8 : 4; }
+__host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+__host__ __device__ inline size_t stage_bytes(const QDesc& q, int T) {
+  size_t b = align16(size_t(T) * key_bytes(q));
+#pragma unroll
+  for (int c = 0; c < GBA_MAX_COLS; ++c)
+    if (c < q.ncols) b += align16(size_t(T) * col_bytes(q.col_type[c]));
+  return b;
+}
+
+// value bits of column c (selected without dynamic register indexing)
+__device__ __forceinline__ unsigned long long pick(int c, unsigned long long r0, unsigned long long r1,
+                                                   unsigned long long r2, unsigned long long r3) {
+  return c == 0 ? r0 : c == 1 ? r1 : c == 2 ? r2 : r3;
+}
+
+template <bool K64>
+struct SmemTable {
+  typedef typename std::conditional<K64, unsigned long long, unsigned>::type KeyW;
+  KeyW* keys;
+  unsigned long long* acc;  // [naccs][S]
+  unsigned long long* side; // [naccs]
+  unsigned* side_present;
+  int S;
+};
+
+template <bool K64>
+__device__ __forceinline__ int smem_find_or_insert(const SmemTable<K64>& t, uint64_t key, uint32_t h, int cap) {
+  typedef typename SmemTable<K64>::KeyW KeyW;
+  const KeyW kk = KeyW(key);
+  const KeyW empty = KeyW(K64 ? EMPTY64 : EMPTY32);
+  int s = int((uint64_t(h) * unsigned(t.S)) >> 32);
+  for (int p = 0; p < cap; ++p) {
+    KeyW cur = *(volatile KeyW*)&t.keys[s];
+    if (cur == kk) return s;
+    if (cur == empty) {
+      KeyW prev = atomicCAS(&t.keys[s], empty, kk);
+      if (prev == empty || prev == kk) return s;
+    }
+    s = (s + 1 == t.S) ? 0 : s + 1;
+  }
+  return -1;
+}
+
+// One warp-wide insertion step: every lane holds at most one row.
+template <bool K64>
+__device__ __forceinline__ void warp_insert(const PreaggParams& P, const SmemTable<K64>& st, bool valid,
+                                            uint64_t key, unsigned long long (&v)[GBA_MAX_AGGS]) {
+  const QDesc& q = P.q;
+  const unsigned lane = lane_id();
+  const uint64_t emptyk = K64 ? EMPTY64 : uint64_t(EMPTY32);
+  const bool sent = valid && key == emptyk;
+  if (__any_sync(GBA_FULL_MASK, sent) && sent) {
+    if (P.S > 0) {
+      if (*(volatile unsigned*)st.side_present == 0u) atomicExch(st.side_present, 1u);
+#pragma unroll
+      for (int a = 0; a < GBA_MAX_AGGS; ++a)
+        if (a < q.naccs) acc_atomic(q.acc_op[a], &st.side[a], v[a]);
+    } else {
+      gtable_insert<K64>(P.gt, q.naccs, q.acc_op, key, 0u, v, P.flags);
+    }
+  }
+  const bool live = valid && !sent;
+  const unsigned live_mask = __ballot_sync(GBA_FULL_MASK, live);
+  if (live_mask == 0) return;
+  if (!live) key = emptyk;
+  bool leader = live;
+  if (P.coalesce) {
+    unsigned peers;
+    if constexpr (K64) peers = __match_any_sync(GBA_FULL_MASK, (unsigned long long)key);
+    else peers = __match_any_sync(GBA_FULL_MASK, unsigned(key));
+    peers &= live_mask;
+    const unsigned gsize = live ? __popc(peers) : 0u;
+    const unsigned maxg = __reduce_max_sync(GBA_FULL_MASK, gsize);
+    if (maxg > 1) {
+      unsigned rem = live ? (peers & ~(1u << lane)) : 0u;
+      for (unsigned i = 1; i < maxg; ++i) {
+        const int src = rem ? __ffs(rem) - 1 : int(lane);
+#pragma unroll
+        for (int a = 0; a < GBA_MAX_AGGS; ++a) {
+          if (a < q.naccs) {
+            unsigned long long x = __shfl_sync(GBA_FULL_MASK, v[a], src);
+            if (rem) v[a] = acc_combine(q.acc_op[a], v[a], x);
+          }
+        }
+        rem &= rem - 1u;
+      }
+    }
+    leader = live && ((peers & ((1u << lane) - 1u)) == 0u);
+  }
+  if (!leader) return;
+  const uint32_t h = key_hash<K64>(key, GBA_TABLE_SEED);
+  int slot = -1;
+  if (P.S > 0) slot = smem_find_or_insert<K64>(st, key, h, P.sprobe);
+  if (slot >= 0) {
+#pragma unroll
+    for (int a = 0; a < GBA_MAX_AGGS; ++a)
+      if (a < q.naccs) acc_atomic(q.acc_op[a], &st.acc[size_t(a) * st.S + slot], v[a]);
+  } else {
+    gtable_insert<K64>(P.gt, q.naccs, q.acc_op, key, h, v, P.flags);
+  }
+}
+
+template <bool K64>
+__global__ void __launch_bounds__(512) k_preagg(PreaggParams P) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  const QDesc& q = P.q;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int T = P.T;
+  const int64_t n = q.n;
+  const int64_t ntiles = (n + T - 1) / T;
+  const int64_t nfull = n / T;
+  const int kb = K64 ? 8 : 4;
+
+  // ---- carve shared memory ------------------------------------------------------
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
+  size_t off = 128;
+  const size_t sb = stage_bytes(q, T);
+  unsigned char* stage0 = smem + off;
+  if (P.use_tma) off += sb * P.nstages;
+  SmemTable<K64> st;
+  st.S = P.S;
+  st.keys = reinterpret_cast<typename SmemTable<K64>::KeyW*>(smem + off);
+  off += align16(size_t(P.S) * kb);
+  st.acc = reinterpret_cast<unsigned long long*>(smem + off);
+  off += size_t(P.S) * q.naccs * 8;
+  st.side = reinterpret_cast<unsigned long long*>(smem + off);
+  off += GBA_MAX_AGGS * 8;
+  st.side_present = reinterpret_cast<unsigned*>(smem + off);
+  __shared__ int s_abort;
+
+  // column offsets inside a stage
+  size_t coff[GBA_MAX_COLS];
+  {
+    size_t o = align16(size_t(T) * kb);
+#pragma unroll
+    for (int c = 0; c < GBA_MAX_COLS; ++c) {
+      coff[c] = o;
+      if (c < q.ncols) o += align16(size_t(T) * col_bytes(q.col_type[c]));
+    }
+  }
+
+  for (int i = tid; i < P.S; i += nthr) {
+    st.keys[i] = typename SmemTable<K64>::KeyW(K64 ? EMPTY64 : EMPTY32);
+#pragma unroll
+    for (int a = 0; a < GBA_MAX_AGGS; ++a)
+      if (a < q.naccs) st.acc[size_t(a) * P.S + i] = acc_identity(q.acc_op[a]);
+  }
+  if (tid == 0) {
+#pragma unroll
+    for (int a = 0; a < GBA_MAX_AGGS; ++a) st.side[a] = a < q.naccs ? acc_identity(q.acc_op[a]) : 0ull;
+    *st.side_present = 0u;
+    s_abort = 0;
+    if (P.use_tma) {
+      for (int s = 0; s < P.nstages; ++s) mbar_init(&bars[s], 1);
+      mbar_fence_init();
+    }
+  }
+  __syncthreads();
+
+  auto issue = [&](int64_t tile, int s) {
+    unsigned char* dst = stage0 + size_t(s) * sb;
+    const int64_t r0 = tile * T;
+    uint32_t bytes = uint32_t(size_t(T) * kb);
+#pragma unroll
+    for (int c = 0; c < GBA_MAX_COLS; ++c)
+      if (c < q.ncols) bytes += uint32_t(size_t(T) * col_bytes(q.col_type[c]));
+    mbar_arrive_expect_tx(&bars[s], bytes);
+    bulk_g2s(dst, static_cast<const unsigned char*>(q.keys) + r0 * kb, uint32_t(size_t(T) * kb), &bars[s]);
+#pragma unroll
+    for (int c = 0; c < GBA_MAX_COLS; ++c) {
+      if (c < q.ncols) {
+        const int cb = col_bytes(q.col_type[c]);
+        bulk_g2s(dst + coff[c], static_cast<const unsigned char*>(q.cols[c]) + r0 * cb,
+                 uint32_t(size_t(T) * cb), &bars[s]);
+      }
+    }
+  };
+
+  // prologue: fill the pipeline
+  if (P.use_tma && tid == 0) {
+    for (int s = 0; s < P.nstages; ++s) {
+      const int64_t tile = blockIdx.x + int64_t(s) * gridDim.x;
+      if (tile < nfull) issue(tile, s);
+    }
+  }
+
+  unsigned phase = 0;  // bit s = parity to wait for on stage s
+  int64_t it = 0;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+    const int s = int(it % P.nstages);
+    const int64_t r0 = tile * T;
+    const int rows = int(n - r0 < int64_t(T) ? n - r0 : int64_t(T));
+    const bool via_tma = P.use_tma && tile < nfull;
+    if (via_tma) {
+      if (!mbar_wait_bounded(&bars[s], (phase >> s) & 1u, P.flags)) s_abort = 1;
+      phase ^= 1u << s;
+    }
+    __syncthreads();
+    if (s_abort) break;
+    const unsigned char* sbase = stage0 + size_t(s) * sb;
+    for (int j0 = 0; j0 < T; j0 += nthr) {
+      const int j = j0 + tid;
+      const bool valid = j < rows;
+      uint64_t key = 0;
+      unsigned long long r[GBA_MAX_COLS] = {0ull, 0ull, 0ull, 0ull};
+      if (valid) {
+        if (via_tma) {
+          key = K64 ? reinterpret_cast<const unsigned long long*>(sbase)[j]
+                    : reinterpret_cast<const unsigned*>(sbase)[j];
+#pragma unroll
+          for (int c = 0; c < GBA_MAX_COLS; ++c)
+            if (c < q.ncols)
+              r[c] = col_bytes(q.col_type[c]) == 8
+                         ? reinterpret_cast<const unsigned long long*>(sbase + coff[c])[j]
+                         : reinterpret_cast<const unsigned*>(sbase + coff[c])[j];
+        } else {
+          key = load_key_g(q, r0 + j);
+#pragma unroll
+          for (int c = 0; c < GBA_MAX_COLS; ++c)
+            if (c < q.ncols)
+              r[c] = col_bytes(q.col_type[c]) == 8
+                         ? __ldg(static_cast<const unsigned long long*>(q.cols[c]) + r0 + j)
+                         : __ldg(static_cast<const unsigned*>(q.cols[c]) + r0 + j);
+        }
+      }
+      unsigned long long v[GBA_MAX_AGGS];
+#pragma unroll
+      for (int a = 0; a < GBA_MAX_AGGS; ++a) {
+        if (a < q.naccs) {
+          v[a] = acc_contrib(q.acc_op[a], q.acc_ctype[a], pick(q.acc_col[a], r[0], r[1], r[2], r[3]));
+        } else {
+          v[a] = 0ull;
+        }
+      }
+      warp_insert<K64>(P, st, valid, key, v);
+    }
+    __syncthreads();  // stage s fully consumed
+    if (via_tma && tid == 0) {
+      const int64_t nxt = tile + int64_t(P.nstages) * gridDim.x;
+      if (nxt < nfull) {
+        fence_proxy_async_smem();
+        issue(nxt, s);
+      }
+    }
+  }
+
+  if (s_abort) {
+    // drain: wait (bounded) for copies this CTA still has in flight
+    if (tid == 0 && P.use_tma) {
+      for (int s = 0; s < P.nstages; ++s) {
+        for (unsigned k = 0; k < (1u << 20); ++k)
+          if (mbar_try_wait(&bars[s], (phase >> s) & 1u)) break;
+      }
+    }
+    return;
+  }
+
+  // ---- flush the shared table into the HBM table -------------------------------
+  __syncthreads();
+  for (int i = tid; i < P.S; i += nthr) {
+    const uint64_t k = st.keys[i];
+    if (k == (K64 ? EMPTY64 : uint64_t(EMPTY32))) continue;
+    unsigned long long v[GBA_MAX_AGGS];
+#pragma unroll
+    for (int a = 0; a < GBA_MAX_AGGS; ++a) v[a] = a < q.naccs ? st.acc[size_t(a) * P.S + i] : 0ull;
+    gtable_insert<K64>(P.gt, q.naccs, q.acc_op, k, key_hash<K64>(k, GBA_TABLE_SEED), v, P.flags);
+  }
+  if (tid == 0 && P.S > 0 && *st.side_present) {
+    unsigned long long v[GBA_MAX_AGGS];
+#pragma unroll
+    for (int a = 0; a < GBA_MAX_AGGS; ++a) v[a] = st.side[a];
+    gtable_insert<K64>(P.gt, q.naccs, q.acc_op, K64 ? EMPTY64 : uint64_t(EMPTY32), 0u, v, P.flags);
+  }
+}
+
+__global__ void k_table_init(GTable t, int naccs, QDesc q) {
+  const int stride = 1 + naccs;
+  const uint64_t total = (t.cap + 1) * stride;
+  for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < total;
+       i += uint64_t(gridDim.x) * blockDim.x) {
+    const uint64_t slot = i / stride;
+    const int w = int(i - slot * stride);
+    unsigned long long v;
+    if (w == 0) v = slot == t.cap ? 0ull : EMPTY64;
+    else {
+      v = 0ull;
+#pragma unroll
+      for (int a = 0; a < GBA_MAX_AGGS; ++a)
+        if (a == w - 1) v = acc_identity(q.acc_op[a]);
+    }
+    t.base[i] = v;
+  }
+}
+
+template <bool K64>
+__global__ void k_compact(GTable t, QDesc q, OutDesc o) {
+  const int stride = 1 + q.naccs;
+  const unsigned lane = lane_id();
+  const uint64_t warp = (blockIdx.x * uint64_t(blockDim.x) + threadIdx.x) >> 5;
+  const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+  for (uint64_t base = warp * 32; base < t.cap; base += nwarps * 32) {
+    const uint64_t i = base + lane;
+    unsigned long long k = EMPTY64;
+    if (i < t.cap) k = t.base[i * stride];
+    const bool occ = k != EMPTY64;
+    const unsigned m = __ballot_sync(GBA_FULL_MASK, occ);
+    if (m == 0) continue;
+    unsigned long long pos0 = 0;
+    if (lane == 0) pos0 = atomicAdd(o.count, (unsigned long long)__popc(m));
+    pos0 = __shfl_sync(GBA_FULL_MASK, pos0, 0);
+    if (occ) {
+      const unsigned long long pos = pos0 + __popc(m & ((1u << lane) - 1u));
+      if (pos < (unsigned long long)o.capacity) {
+        if (K64) static_cast<unsigned long long*>(o.keys)[pos] = k;
+        else static_cast<unsigned*>(o.keys)[pos] = unsigned(k);
+#pragma unroll
+        for (int a = 0; a < GBA_MAX_AGGS; ++a)
+          if (a < q.naccs) o.accs[a][pos] = t.base[i * stride + 1 + a];
+      }
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const unsigned long long* side = t.base + t.cap * stride;
+    if (side[0] != 0ull) {
+      const unsigned long long pos = atomicAdd(o.count, 1ull);
+      if (pos < (unsigned long long)o.capacity) {
+        if (K64) static_cast<unsigned long long*>(o.keys)[pos] = EMPTY64;
+        else static_cast<unsigned*>(o.keys)[pos] = EMPTY32;
+#pragma unroll
+        for (int a = 0; a < GBA_MAX_AGGS; ++a)
+          if (a < q.naccs) o.accs[a][pos] = side[1 + a];
+      }
+    }
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Host launchers.
+size_t gba_preagg_smem_bytes(const QDesc& q, int S, int T, int nstages, int use_tma) {
+  size_t b = 128;
+  if (use_tma) b += stage_bytes(q, T) * nstages;
+  b += align16(size_t(S) * key_bytes(q));
+  b += size_t(S) * q.naccs * 8;
+  b += GBA_MAX_AGGS * 8 + 16;
+  return b;
+}
+
+cudaError_t gba_launch_table_init(const GTable& t, const QDesc& q, int grid, cudaStream_t s) {
+  k_table_init<<<grid, 256, 0, s>>>(t, q.naccs, q);
+  return cudaGetLastError();
+}
+
+cudaError_t gba_launch_preagg(const QDesc& q, const GTable& t, const PreaggCfg& c, unsigned* flags,
+                              cudaStream_t s) {
+  PreaggParams P;
+  P.q = q;
+  P.gt = t;
+  P.S = c.smem_slots;
+  P.sprobe = c.smem_probe_cap;
+  P.T = c.tile_rows;
+  P.nstages = c.nstages < 1 ? 1 : (c.nstages > kMaxStages ? kMaxStages : c.nstages);
+  P.use_tma = c.use_tma;
+  P.coalesce = c.coalesce;
+  P.flags = flags;
+  const size_t smem = gba_preagg_smem_bytes(q, P.S, P.T, P.nstages, P.use_tma);
+  cudaError_t e;
+  if (q.key64) {
+    e = cudaFuncSetAttribute(k_preagg<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    k_preagg<true><<<c.grid, c.block, smem, s>>>(P);
+  } else {
+    e = cudaFuncSetAttribute(k_preagg<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    k_preagg<false><<<c.grid, c.block, smem, s>>>(P);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t gba_launch_compact(const GTable& t, const QDesc& q, const OutDesc& o, int grid, cudaStream_t s) {
+  if (q.key64) k_compact<true><<<grid, 256, 0, s>>>(t, q, o);
+  else k_compact<false><<<grid, 256, 0, s>>>(t, q, o);
+  return cudaGetLastError();
+}

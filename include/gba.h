@@ -1,0 +1,207 @@
+/* B200-native hash GROUP BY aggregation: the C ABI.
+ *
+ * Plain C types only (pointers, sizes, enums); `stream` arguments are
+ * cudaStream_t passed as void*.  Every entry point returns a gba_status and
+ * never exits the process.  A context is not shared between threads without
+ * external locking; separate contexts run concurrently.
+ *
+ * Reference interfaces replaced (PneNPproof/cpu_gpu_coprocess_groupby_agg):
+ *   - groupby_agg_partition<K,V>(host_keys, host_vals, kv_buffer_len, tile_len,
+ *     P, par_result_vec, nstreams)          tiled_groupby_agg_partition/include/
+ *                                           lib_header.hpp:6-12,
+ *                                           group_then_partition.cuh:5-11
+ *   - groupby_agg_intra_partition(par_result_vec, keys_out, vals_out, Capacity,
+ *     min_load_num, max_load_num, nstreams, par_kv_begin, par_result_kv_num)
+ *                                           groupby_agg_intra_partition.cuh:5-13
+ * Together they compute an exact GROUP BY SUM of u32 values by u32 key.  The
+ * C++ drop-ins with those exact signatures are declared in
+ * tiled_groupby_agg_partition.hpp and are built on the functions below.
+ */
+#ifndef GBA_H
+#define GBA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GBA_MAX_COLS 4
+#define GBA_MAX_AGGS 8
+
+typedef enum gba_status {
+  GBA_OK = 0,
+  GBA_ERR_INVALID_ARG = 1,
+  GBA_ERR_CUDA = 2,
+  GBA_ERR_OOM = 3,
+  GBA_ERR_OUTPUT_CAPACITY = 4, /* more groups than gba_output.capacity; *n_groups holds the count */
+  GBA_ERR_TABLE_OVERFLOW = 5,  /* table still overflowing after the regrow limit */
+  GBA_ERR_TIMEOUT = 6,         /* a bounded device wait gave up */
+  GBA_ERR_UNSUPPORTED = 7,
+  GBA_ERR_BUDGET = 8           /* serving: request larger than the device-memory budget */
+} gba_status;
+
+/* Column and key types.  GBA_U32 is the reference's key_type/val_type
+ * (u_int32_t, tiled_groupby_agg_partition/include/util.cuh:6-7). */
+typedef enum gba_type { GBA_I32 = 0, GBA_I64 = 1, GBA_F32 = 2, GBA_U32 = 3 } gba_type;
+
+/* Aggregates.  SUM/COUNT/MIN/MAX of integer columns accumulate in int64 and are
+ * exact (SUM wraps mod 2^64); SUM of an F32 column accumulates in fp64.  The
+ * reference computes SUM only, in u32 (kernel.cu:48,152,334). */
+typedef enum gba_op { GBA_SUM = 0, GBA_COUNT = 1, GBA_MIN = 2, GBA_MAX = 3 } gba_op;
+
+typedef struct gba_column {
+  int32_t type;     /* gba_type */
+  const void* data; /* n_rows elements, device (or host for *_host calls) */
+} gba_column;
+
+typedef struct gba_agg {
+  int32_t op;  /* gba_op */
+  int32_t col; /* index into gba_query.cols; ignored for COUNT */
+} gba_agg;
+
+typedef struct gba_query {
+  int64_t n_rows;
+  gba_column key; /* GBA_I32, GBA_U32 or GBA_I64 */
+  int32_t n_cols;
+  gba_column cols[GBA_MAX_COLS];
+  int32_t n_aggs;
+  gba_agg aggs[GBA_MAX_AGGS];
+} gba_query;
+
+/* Output columns: one row per distinct key, in no particular order.  aggs[a]
+ * holds capacity 8-byte values: int64, or double for SUM of an F32 column. */
+typedef struct gba_output {
+  void* keys;
+  void* aggs[GBA_MAX_AGGS];
+  int64_t capacity;
+} gba_output;
+
+typedef enum gba_sizing {
+  GBA_SIZING_PLAIN = 0,   /* fixed load factor on the row count, overflow -> regrow */
+  GBA_SIZING_LEARNED = 1, /* MLP cardinality estimate, overflow -> regrow */
+  GBA_SIZING_FIXED = 2    /* table_slots as given, overflow -> regrow */
+} gba_sizing;
+
+typedef enum gba_strategy {
+  GBA_STRATEGY_AUTO = 0,
+  GBA_STRATEGY_TABLE = 1,    /* shared-memory pre-aggregation + one HBM table */
+  GBA_STRATEGY_PARTITION = 2 /* radix hash partition + per-partition shared-memory tables */
+} gba_strategy;
+
+/* Tuning knobs; 0 / -1 fields mean "choose automatically". */
+typedef struct gba_knobs {
+  int32_t sizing;         /* gba_sizing */
+  int32_t strategy;       /* gba_strategy */
+  double load_factor;     /* HBM table target load (default 0.5) */
+  int64_t table_slots;    /* FIXED sizing */
+  int32_t preagg;         /* -1 auto, 0 off, 1 on */
+  int32_t smem_slots;     /* shared-memory table slots per CTA */
+  int32_t partition_bits; /* radix fan-out 2^bits */
+  int32_t blocks_per_sm;
+  int32_t block_threads;
+  int32_t tile_rows;
+  int32_t nstages;        /* TMA pipeline depth */
+  int32_t use_tma;        /* -1 auto, 0 off, 1 on */
+  int32_t coalesce;       /* -1 auto, 0 off, 1 on: __match_any_sync pre-combining */
+  int32_t probe_cap;      /* HBM table probe cap (0 = auto) */
+  int32_t smem_probe_cap; /* shared table probe cap (0 = auto) */
+  int32_t max_regrow;     /* regrow attempts before GBA_ERR_TABLE_OVERFLOW */
+  int32_t timing;         /* 1: time each kernel with CUDA events (gba_stats.kernel_ms) */
+} gba_knobs;
+
+/* What the last call on a context did. */
+typedef struct gba_stats {
+  int32_t strategy;         /* gba_strategy actually run */
+  int32_t preagg;           /* 1 if shared-memory pre-aggregation ran */
+  int64_t table_slots;      /* HBM table capacity of the final attempt */
+  int32_t partition_bits;
+  int32_t regrows;          /* overflow re-runs */
+  double predicted_groups;  /* estimator output (learned sizing), else -1 */
+  int64_t n_groups;
+  int32_t kernel_launches;  /* kernels launched by the call */
+  /* with gba_knobs.timing: device time of the call's kernels, by role:
+   * [0] table/partition setup, [1] the main aggregation kernel,
+   * [2] final reduce / compaction, [3] everything else */
+  double kernel_ms[4];
+} gba_stats;
+
+typedef struct gba_context gba_context;
+
+/* sizeof() of the ABI structs, for binding generators: which = 0 gba_query,
+ * 1 gba_output, 2 gba_knobs, 3 gba_stats, 4 gba_gen_spec. */
+int64_t gba_abi_struct_size(int32_t which);
+
+void gba_default_knobs(gba_knobs* k);
+const char* gba_status_string(gba_status s);
+
+/* Creates a context bound to CUDA device `device`.  The context owns a device
+ * workspace that grows on demand and is reused across calls. */
+gba_status gba_create(gba_context** out, int32_t device);
+gba_status gba_destroy(gba_context* ctx);
+const char* gba_last_error(const gba_context* ctx);
+gba_status gba_last_stats(const gba_context* ctx, gba_stats* out);
+
+/* Exact GROUP BY over device-resident columns, enqueued on `stream`; returns
+ * after the result is complete with *n_groups set (host pointer).  Replaces the
+ * two reference phases (lib_header.hpp:6-12 + groupby_agg_intra_partition.cuh:5-13)
+ * for data already in HBM. */
+gba_status gba_groupby(gba_context* ctx, const gba_query* q, const gba_output* out, const gba_knobs* knobs,
+                       void* stream, int64_t* n_groups);
+
+/* The same over HOST columns and HOST output buffers: rows are streamed to the
+ * device in chunks overlapped with aggregation (the reference's host-resident
+ * "coprocess" tiling, group_then_partition.cu:353-418), the result is copied
+ * back.  Pinned host memory gives full link speed. */
+gba_status gba_groupby_host(gba_context* ctx, const gba_query* q, const gba_output* out,
+                            const gba_knobs* knobs, void* stream, int64_t* n_groups);
+
+/* Many independent queries (device columns) in one persistent launch over a
+ * device work queue of (query, tile) items, replayed from a CUDA graph when the
+ * same shapes repeat.  n_groups: host array of n_queries counts.  No
+ * counterpart in the reference (its tile loop runs one query, one tile per
+ * host thread at a time: group_then_partition.cu:332-424). */
+gba_status gba_groupby_batch(gba_context* ctx, int32_t n_queries, const gba_query* qs, const gba_output* outs,
+                             const gba_knobs* knobs, void* stream, int64_t* n_groups);
+
+/* ---- learned cardinality estimator -------------------------------------- */
+#define GBA_EST_FEATURES 32
+#define GBA_EST_HIDDEN 64
+#define GBA_EST_SAMPLE 1024
+
+/* Features of a device key column: per tile of `tile_rows` rows, a strided
+ * 1024-row sample; out[GBA_EST_FEATURES] (host) gets the pooled features. */
+gba_status gba_estimator_features(gba_context* ctx, const gba_query* q, int64_t tile_rows, void* stream,
+                                  float* out);
+/* Loads MLP weights (host fp32 array laid out as gba_estimator_param_count()
+ * values) into the context; learned sizing uses them. */
+int64_t gba_estimator_param_count(void);
+gba_status gba_estimator_load(gba_context* ctx, const float* params);
+gba_status gba_estimator_get(gba_context* ctx, float* params);
+/* Predicts log2(groups) for n feature rows (host arrays). */
+gba_status gba_estimator_predict(gba_context* ctx, int32_t n, const float* feats, float* out_log2_groups);
+/* Trains on the GPU with the library's own forward/backward/Adam kernels:
+ * feats[n][GBA_EST_FEATURES], target log2(groups)[n]; returns the final mean
+ * squared error. */
+gba_status gba_estimator_train(gba_context* ctx, int32_t n, const float* feats, const float* target,
+                               int32_t epochs, int32_t batch, float lr, uint64_t seed, float* final_loss);
+/* One forward+backward pass on the GPU for a batch (gradient check):
+ * grads receives gba_estimator_param_count() values, *loss the MSE. */
+gba_status gba_estimator_grad(gba_context* ctx, int32_t n, const float* feats, const float* target,
+                              float* grads, float* loss);
+
+/* ---- seeded synthetic data ---------------------------------------------- */
+/* Host generator (any thread count); see csrc/datagen.h for the spec. */
+struct gba_gen_spec;
+gba_status gba_gen_host(const struct gba_gen_spec* spec, int64_t row0, int64_t n, void* keys, void* const* cols,
+                        int32_t nthreads);
+/* Device generator (same rows as the host generator up to libm rounding in the
+ * Zipf / normal draws). */
+gba_status gba_gen_device(const struct gba_gen_spec* spec, int64_t row0, int64_t n, void* keys, void* const* cols,
+                          void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GBA_H */

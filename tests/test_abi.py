@@ -1,0 +1,58 @@
+"""The C ABI library loads and exports every symbol include/*.h declares (CPU only)."""
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+from cpu_gpu_coprocess_groupby_agg_b200 import _abi as A
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def _declared_functions(header: Path) -> set[str]:
+    text = header.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return set(re.findall(r"\b(gba_[a-z0-9_]+)\s*\(", text)) - {"gba_gen_spec"}
+
+
+def test_library_exports_every_declared_function():
+    lib = A.lib()
+    declared = _declared_functions(ROOT / "include" / "gba.h")
+    assert len(declared) >= 19
+    missing = [f for f in declared if not hasattr(lib, f)]
+    assert not missing, missing
+    # and the binding covers every declared function
+    assert declared == set(A.SIGNATURES), declared ^ set(A.SIGNATURES)
+    out = subprocess.run(["nm", "-D", "--defined-only", str(A.LIB_PATH)], capture_output=True, text=True).stdout
+    for f in declared:
+        assert re.search(rf"\bT {f}\b", out), f
+
+
+def test_struct_layouts_match_binding():
+    lib = A.lib()
+    for which, cls in enumerate([A.Query, A.Output, A.Knobs, A.Stats, A.GenSpec]):
+        assert lib.gba_abi_struct_size(which) == C.sizeof(cls), cls.__name__
+
+
+def test_default_knobs_and_status_strings():
+    lib = A.lib()
+    k = A.Knobs()
+    lib.gba_default_knobs(C.byref(k))
+    assert k.load_factor == 0.5 and k.preagg == -1 and k.max_regrow == 4
+    for s in range(9):
+        assert lib.gba_status_string(s)
+
+
+def test_no_gpu_calls_fail_cleanly():
+    """Without a usable device gba_create reports an error instead of crashing."""
+    import torch
+    if torch.cuda.is_available():
+        return
+    h = C.c_void_p()
+    assert A.lib().gba_create(C.byref(h), 0) != A.OK
+
+
+def test_invalid_arguments_rejected_without_gpu():
+    lib = A.lib()
+    assert lib.gba_groupby(None, None, None, None, None, None) == A.ERR_INVALID_ARG
+    assert lib.gba_destroy(None) == A.ERR_INVALID_ARG
