@@ -114,13 +114,17 @@ class Context:
 
     # ---- device-resident ---------------------------------------------------
     def groupby(self, keys, cols: Sequence = (), aggs: Sequence = (("count", None),), knobs=None,
-                capacity: int | None = None, unsigned_keys: bool = False, stream=None, out=None) -> Result:
+                capacity: int | None = None, unsigned_keys: bool = False, stream=None, out=None,
+                unsigned_cols: Sequence[bool] = ()) -> Result:
+        """torch has no general uint32 dtype: pass uint32 data as int32 tensors
+        and mark them with unsigned_keys / unsigned_cols[i]."""
         import torch
         if not keys.is_cuda:
             raise ValueError("groupby() takes device tensors; use groupby_host() for host arrays")
         n = keys.numel()
         aggs_p = parse_aggs(aggs)
-        col_specs = [(c.data_ptr(), _torch_type(c)) for c in cols]
+        uc = list(unsigned_cols) + [False] * (len(cols) - len(unsigned_cols))
+        col_specs = [(c.data_ptr(), _torch_type(c, u)) for c, u in zip(cols, uc)]
         ktype = _torch_type(keys, unsigned_keys)
         q = build_query(n, keys.data_ptr(), ktype, col_specs, aggs_p)
         if out is None:

@@ -239,6 +239,12 @@ gba_status gba_build_qdesc(gba_context* ctx, const gba_query* q, QDesc* d) {
       return GBA_ERR_INVALID_ARG;
     }
   }
+  int w = 0;
+  for (int a = 0; a < q->n_aggs; ++a) {
+    d->acc_woff[a] = w;
+    w += gba_acc_smem_words(d->acc_op[a]);
+  }
+  d->nwords = w;
   return GBA_OK;
 }
 
@@ -248,11 +254,19 @@ static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 
 // Plan: everything the single-query driver decides before launching.
 void gba_make_plan(const gba_context* ctx, const QDesc& q, const gba_knobs& k, double predicted_groups,
                    GbaPlan* p) {
-  p->block = k.block_threads > 0 ? k.block_threads : 512;
-  p->block = std::min(512, std::max(128, p->block / 32 * 32));
-  p->tile_rows = k.tile_rows > 0 ? k.tile_rows : 2048;
+  p->block = k.block_threads > 0 ? k.block_threads : 1024;
+  p->block = std::min(1024, std::max(128, p->block / 32 * 32));
+  // TMA staging: about 96 KB of bulk copies in flight per SM reach the HBM read
+  // peak with one CTA per SM (measured: 2 x 32 KB -> 6.9 TB/s, 3 x 32 KB ->
+  // 7.3 TB/s, 2 x 16 KB -> 4.7 TB/s); tiles of at least 24 KB, 2-4 stages
+  size_t rb = q.key64 ? 8 : 4;
+  for (int c = 0; c < q.ncols; ++c) rb += q.col_type[c] == GBA_I64 ? 8 : 4;
+  int T = 1024;
+  while (T < 4096 && size_t(T) * rb < 24 * 1024) T *= 2;
+  p->tile_rows = k.tile_rows > 0 ? k.tile_rows : T;
   p->tile_rows = std::max(p->block, p->tile_rows / p->block * p->block);
-  p->nstages = k.nstages > 0 ? std::min(4, k.nstages) : 3;
+  const size_t stage = size_t(p->tile_rows) * rb;
+  p->nstages = k.nstages > 0 ? std::min(4, k.nstages) : int(std::min<size_t>(4, std::max<size_t>(2, (98304 + stage - 1) / stage)));
   const int64_t ntiles = (q.n + p->tile_rows - 1) / p->tile_rows;
   const int bps = k.blocks_per_sm > 0 ? k.blocks_per_sm : 1;
   p->grid = int(std::max<int64_t>(1, std::min<int64_t>(ntiles, int64_t(ctx->sms) * bps)));
@@ -260,16 +274,21 @@ void gba_make_plan(const gba_context* ctx, const QDesc& q, const gba_knobs& k, d
   bool tma_ok = aligned16(q.keys) && q.n >= p->tile_rows;
   for (int c = 0; c < q.ncols; ++c) tma_ok = tma_ok && aligned16(q.cols[c]);
   p->use_tma = k.use_tma == 0 ? 0 : (tma_ok ? 1 : 0);
-  p->coalesce = k.coalesce == 0 ? 0 : 1;
+  // measured: __match_any_sync pre-combining costs more than it saves unless a
+  // warp sees long runs of one key, so it is opt-in
+  p->coalesce = k.coalesce == 1 ? 1 : 0;
 
+  // HBM table capacity.  PLAIN: the only bound known without an estimate is the
+  // row count, at a fixed load factor (default 0.5), rounded to a power of two.
+  // LEARNED: 1.25x the predicted groups at load 0.7 (any size: slots are
+  // addressed by a multiply-shift of the hash), so tables of up to ~1.4M
+  // 48-byte slots stay L2-resident; an under-estimate overflows and regrows.
   const double lf = (k.load_factor > 0.05 && k.load_factor < 0.95) ? k.load_factor : 0.5;
-  double groups_bound;
-  if (k.sizing == GBA_SIZING_FIXED && k.table_slots > 0) groups_bound = double(k.table_slots) * lf;
+  uint64_t cap;
+  if (k.sizing == GBA_SIZING_FIXED && k.table_slots > 0) cap = uint64_t(k.table_slots);
   else if (k.sizing == GBA_SIZING_LEARNED && predicted_groups > 0)
-    groups_bound = std::min(double(std::max<int64_t>(q.n, 1)), predicted_groups * 1.5 + 64.0);
-  else groups_bound = double(std::max<int64_t>(q.n, 1));
-  uint64_t cap = (k.sizing == GBA_SIZING_FIXED && k.table_slots > 0) ? uint64_t(k.table_slots)
-                                                                      : gba_pow2_ceil(uint64_t(groups_bound / lf));
+    cap = uint64_t(std::min(double(std::max<int64_t>(q.n, 1)), predicted_groups * 1.25 + 64.0) / 0.7) + 1;
+  else cap = gba_pow2_ceil(uint64_t(double(std::max<int64_t>(q.n, 1)) / lf));
   p->table_slots = std::max<uint64_t>(cap, 64);
   p->probe_cap = k.probe_cap > 0 ? k.probe_cap : 256;
 
@@ -282,17 +301,24 @@ void gba_make_plan(const gba_context* ctx, const QDesc& q, const gba_knobs& k, d
       preagg = 0;  // nearly all keys distinct: pre-aggregation only costs time
   }
   p->preagg = preagg;
-  const size_t fixed = gba_preagg_smem_bytes(q, 0, p->tile_rows, p->nstages, p->use_tma);
-  const size_t slot_bytes = (q.key64 ? 8 : 4) + 8 * size_t(q.naccs);
-  int S = 0;
-  if (preagg) {
+  const size_t slot_bytes = (q.key64 ? 8 : 4) + 8 * size_t(q.nwords);
+  auto slots_with = [&](int use_tma) {
+    const size_t fixed = gba_preagg_smem_bytes(q, 0, p->tile_rows, p->nstages, use_tma);
     const size_t room = size_t(ctx->max_smem_optin) > fixed + 1024 ? size_t(ctx->max_smem_optin) - fixed - 1024 : 0;
-    S = int(std::min<size_t>(room / slot_bytes, 16384));
+    int S = int(std::min<size_t>(room / slot_bytes, 16384));
     if (k.smem_slots > 0) S = std::min(S, k.smem_slots);
-    if (S < 32) S = 0;
-  }
-  p->smem_slots = S;
-  p->smem_probe_cap = k.smem_probe_cap > 0 ? k.smem_probe_cap : 32;
+    return S < 32 ? 0 : S;
+  };
+  // The staging competes with the shared table.  When the groups are known to
+  // exceed what the table left beside the TMA stages can hold, drop TMA and
+  // give the table all of shared memory (rows are then loaded straight into
+  // registers, two per thread in flight).
+  if (p->use_tma && k.use_tma < 0 && preagg && predicted_groups > 0 &&
+      predicted_groups > 0.5 * slots_with(1))
+    p->use_tma = 0;
+  p->smem_slots = preagg ? slots_with(p->use_tma) : 0;
+  // a full table makes every miss walk the whole probe window: keep it short
+  p->smem_probe_cap = k.smem_probe_cap > 0 ? k.smem_probe_cap : 8;
   p->partition_bits = k.partition_bits;
 }
 

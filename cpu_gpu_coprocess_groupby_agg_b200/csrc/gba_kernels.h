@@ -29,7 +29,15 @@ struct QDesc {
   int acc_op[GBA_MAX_AGGS];
   int acc_col[GBA_MAX_AGGS];    // source column (0 for COUNT)
   int acc_ctype[GBA_MAX_AGGS];  // type of the source column
+  // shared-memory layout: accumulator a starts at word acc_woff[a] of a slot;
+  // fp32 SUM takes 3 words (128-bit exact fixed point + fp64 residual), the
+  // others 1; nwords = words per slot
+  int acc_woff[GBA_MAX_AGGS];
+  int nwords;
 };
+
+// 8-byte words one accumulator op occupies in a shared-memory slot
+inline int gba_acc_smem_words(int op) { return op == ACC_ADD_F ? 3 : 1; }
 
 // HBM hash table: array-of-structs slots [key | acc0 .. acc{A-1}], 8 bytes
 // each; slot `cap` is the side slot of the all-ones key (the empty marker),

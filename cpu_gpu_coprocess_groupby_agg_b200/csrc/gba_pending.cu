@@ -2,16 +2,6 @@
 #include "gba_context.h"
 #include "gba_plan.h"
 
-int gba_choose_strategy(const gba_context*, const QDesc&, const gba_knobs&, double, const GbaPlan&) {
-  return GBA_STRATEGY_TABLE;
-}
-
-gba_status gba_run_partition(gba_context* ctx, const QDesc&, const gba_output*, const gba_knobs&, const GbaPlan&,
-                             double, cudaStream_t, int64_t*) {
-  ctx->err = "partition strategy not built";
-  return GBA_ERR_UNSUPPORTED;
-}
-
 gba_status gba_predict_groups(gba_context* ctx, const QDesc&, cudaStream_t, double*) {
   ctx->err = "estimator not built";
   return GBA_ERR_UNSUPPORTED;

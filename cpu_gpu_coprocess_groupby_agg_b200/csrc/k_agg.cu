@@ -1,4 +1,4 @@
-// Tiled hash pre-aggregation + global table + final compaction (sm_100a).
+// Tiled hash pre-aggregation + HBM table + final compaction (sm_100a).
 //
 // Replaces the reference's per-tile aggregation chain (tiled_groupby_agg_partition/
 // src/kernel.cu:9-186 driven by group_then_partition.cu:24-246: a one-probe
@@ -15,7 +15,7 @@
 //   k_compact      - the final reduce: writes every occupied slot once to the
 //                    caller's output columns (warp-aggregated output cursor).
 #include "gba_internal.cuh"
-#include <type_traits>
+#include "smem_table.cuh"
 
 namespace {
 
@@ -45,101 +45,32 @@ __host__ __device__ inline size_t stage_bytes(const QDesc& q, int T) {
   return b;
 }
 
-// value bits of column c (selected without dynamic register indexing)
-__device__ __forceinline__ unsigned long long pick(int c, unsigned long long r0, unsigned long long r1,
-                                                   unsigned long long r2, unsigned long long r3) {
-  return c == 0 ? r0 : c == 1 ? r1 : c == 2 ? r2 : r3;
-}
-
-template <bool K64>
-struct SmemTable {
-  typedef typename std::conditional<K64, unsigned long long, unsigned>::type KeyW;
-  KeyW* keys;
-  unsigned long long* acc;  // [naccs][S]
-  unsigned long long* side; // [naccs]
-  unsigned* side_present;
-  int S;
-};
-
-template <bool K64>
-__device__ __forceinline__ int smem_find_or_insert(const SmemTable<K64>& t, uint64_t key, uint32_t h, int cap) {
-  typedef typename SmemTable<K64>::KeyW KeyW;
-  const KeyW kk = KeyW(key);
-  const KeyW empty = KeyW(K64 ? EMPTY64 : EMPTY32);
-  int s = int((uint64_t(h) * unsigned(t.S)) >> 32);
-  for (int p = 0; p < cap; ++p) {
-    KeyW cur = *(volatile KeyW*)&t.keys[s];
-    if (cur == kk) return s;
-    if (cur == empty) {
-      KeyW prev = atomicCAS(&t.keys[s], empty, kk);
-      if (prev == empty || prev == kk) return s;
-    }
-    s = (s + 1 == t.S) ? 0 : s + 1;
-  }
-  return -1;
-}
-
 // One warp-wide insertion step: every lane holds at most one row.
-template <bool K64>
+template <bool K64, int NA>
 __device__ __forceinline__ void warp_insert(const PreaggParams& P, const SmemTable<K64>& st, bool valid,
-                                            uint64_t key, unsigned long long (&v)[GBA_MAX_AGGS]) {
+                                            uint64_t key, unsigned long long (&v)[NA]) {
   const QDesc& q = P.q;
-  const unsigned lane = lane_id();
   const uint64_t emptyk = K64 ? EMPTY64 : uint64_t(EMPTY32);
   const bool sent = valid && key == emptyk;
-  if (__any_sync(GBA_FULL_MASK, sent) && sent) {
-    if (P.S > 0) {
-      if (*(volatile unsigned*)st.side_present == 0u) atomicExch(st.side_present, 1u);
-#pragma unroll
-      for (int a = 0; a < GBA_MAX_AGGS; ++a)
-        if (a < q.naccs) acc_atomic(q.acc_op[a], &st.side[a], v[a]);
-    } else {
-      gtable_insert<K64>(P.gt, q.naccs, q.acc_op, key, 0u, v, P.flags);
-    }
+  if (sent) {
+    if (P.S > 0) smem_apply_side<K64, NA>(st, q, v);
+    else gtable_insert<K64, NA>(P.gt, q.acc_op, key, 0u, v, P.flags);
   }
-  const bool live = valid && !sent;
-  const unsigned live_mask = __ballot_sync(GBA_FULL_MASK, live);
-  if (live_mask == 0) return;
-  if (!live) key = emptyk;
-  bool leader = live;
-  if (P.coalesce) {
-    unsigned peers;
-    if constexpr (K64) peers = __match_any_sync(GBA_FULL_MASK, (unsigned long long)key);
-    else peers = __match_any_sync(GBA_FULL_MASK, unsigned(key));
-    peers &= live_mask;
-    const unsigned gsize = live ? __popc(peers) : 0u;
-    const unsigned maxg = __reduce_max_sync(GBA_FULL_MASK, gsize);
-    if (maxg > 1) {
-      unsigned rem = live ? (peers & ~(1u << lane)) : 0u;
-      for (unsigned i = 1; i < maxg; ++i) {
-        const int src = rem ? __ffs(rem) - 1 : int(lane);
-#pragma unroll
-        for (int a = 0; a < GBA_MAX_AGGS; ++a) {
-          if (a < q.naccs) {
-            unsigned long long x = __shfl_sync(GBA_FULL_MASK, v[a], src);
-            if (rem) v[a] = acc_combine(q.acc_op[a], v[a], x);
-          }
-        }
-        rem &= rem - 1u;
-      }
-    }
-    leader = live && ((peers & ((1u << lane) - 1u)) == 0u);
+  bool leader = valid && !sent;
+  if (P.coalesce) {  // warp-synchronous: every lane of the warp is here
+    if (!leader) key = emptyk;
+    leader = warp_coalesce<K64, NA>(q, leader, key, v);
   }
   if (!leader) return;
-  const uint32_t h = key_hash<K64>(key, GBA_TABLE_SEED);
+  const uint32_t h = table_hash(key);
   int slot = -1;
   if (P.S > 0) slot = smem_find_or_insert<K64>(st, key, h, P.sprobe);
-  if (slot >= 0) {
-#pragma unroll
-    for (int a = 0; a < GBA_MAX_AGGS; ++a)
-      if (a < q.naccs) acc_atomic(q.acc_op[a], &st.acc[size_t(a) * st.S + slot], v[a]);
-  } else {
-    gtable_insert<K64>(P.gt, q.naccs, q.acc_op, key, h, v, P.flags);
-  }
+  if (slot >= 0) smem_apply<K64, NA>(st, q, slot, v);
+  else gtable_insert<K64, NA>(P.gt, q.acc_op, key, h, v, P.flags);
 }
 
-template <bool K64>
-__global__ void __launch_bounds__(512) k_preagg(PreaggParams P) {
+template <bool K64, int NA>
+__global__ void __launch_bounds__(1024, 1) k_preagg(PreaggParams P) {
   extern __shared__ __align__(128) unsigned char smem[];
   const QDesc& q = P.q;
   const int tid = threadIdx.x, nthr = blockDim.x;
@@ -155,15 +86,7 @@ __global__ void __launch_bounds__(512) k_preagg(PreaggParams P) {
   const size_t sb = stage_bytes(q, T);
   unsigned char* stage0 = smem + off;
   if (P.use_tma) off += sb * P.nstages;
-  SmemTable<K64> st;
-  st.S = P.S;
-  st.keys = reinterpret_cast<typename SmemTable<K64>::KeyW*>(smem + off);
-  off += align16(size_t(P.S) * kb);
-  st.acc = reinterpret_cast<unsigned long long*>(smem + off);
-  off += size_t(P.S) * q.naccs * 8;
-  st.side = reinterpret_cast<unsigned long long*>(smem + off);
-  off += GBA_MAX_AGGS * 8;
-  st.side_present = reinterpret_cast<unsigned*>(smem + off);
+  const SmemTable<K64> st = smem_table_carve<K64>(smem + off, P.S, q.nwords);
   __shared__ int s_abort;
 
   // column offsets inside a stage
@@ -177,16 +100,8 @@ __global__ void __launch_bounds__(512) k_preagg(PreaggParams P) {
     }
   }
 
-  for (int i = tid; i < P.S; i += nthr) {
-    st.keys[i] = typename SmemTable<K64>::KeyW(K64 ? EMPTY64 : EMPTY32);
-#pragma unroll
-    for (int a = 0; a < GBA_MAX_AGGS; ++a)
-      if (a < q.naccs) st.acc[size_t(a) * P.S + i] = acc_identity(q.acc_op[a]);
-  }
+  smem_table_init<K64, NA>(st, q);
   if (tid == 0) {
-#pragma unroll
-    for (int a = 0; a < GBA_MAX_AGGS; ++a) st.side[a] = a < q.naccs ? acc_identity(q.acc_op[a]) : 0ull;
-    *st.side_present = 0u;
     s_abort = 0;
     if (P.use_tma) {
       for (int s = 0; s < P.nstages; ++s) mbar_init(&bars[s], 1);
@@ -236,41 +151,46 @@ __global__ void __launch_bounds__(512) k_preagg(PreaggParams P) {
     __syncthreads();
     if (s_abort) break;
     const unsigned char* sbase = stage0 + size_t(s) * sb;
-    for (int j0 = 0; j0 < T; j0 += nthr) {
-      const int j = j0 + tid;
-      const bool valid = j < rows;
-      uint64_t key = 0;
-      unsigned long long r[GBA_MAX_COLS] = {0ull, 0ull, 0ull, 0ull};
-      if (valid) {
-        if (via_tma) {
-          key = K64 ? reinterpret_cast<const unsigned long long*>(sbase)[j]
-                    : reinterpret_cast<const unsigned*>(sbase)[j];
+    // two rows per thread per step, both loaded before either is processed
+    // (without TMA the loads are the memory-level parallelism)
+    constexpr int R = 2;
+    for (int j0 = 0; j0 < T; j0 += R * nthr) {
+      uint64_t key[R];
+      unsigned long long r[R][GBA_MAX_COLS];
 #pragma unroll
-          for (int c = 0; c < GBA_MAX_COLS; ++c)
-            if (c < q.ncols)
-              r[c] = col_bytes(q.col_type[c]) == 8
-                         ? reinterpret_cast<const unsigned long long*>(sbase + coff[c])[j]
-                         : reinterpret_cast<const unsigned*>(sbase + coff[c])[j];
-        } else {
-          key = load_key_g(q, r0 + j);
+      for (int u = 0; u < R; ++u) {
+        const int j = j0 + u * nthr + tid;
+        key[u] = 0;
 #pragma unroll
-          for (int c = 0; c < GBA_MAX_COLS; ++c)
-            if (c < q.ncols)
-              r[c] = col_bytes(q.col_type[c]) == 8
-                         ? __ldg(static_cast<const unsigned long long*>(q.cols[c]) + r0 + j)
-                         : __ldg(static_cast<const unsigned*>(q.cols[c]) + r0 + j);
+        for (int c = 0; c < GBA_MAX_COLS; ++c) r[u][c] = 0ull;
+        if (j < rows) {
+          if (via_tma) {
+            key[u] = K64 ? reinterpret_cast<const unsigned long long*>(sbase)[j]
+                         : reinterpret_cast<const unsigned*>(sbase)[j];
+#pragma unroll
+            for (int c = 0; c < GBA_MAX_COLS; ++c)
+              if (c < q.ncols)
+                r[u][c] = col_bytes(q.col_type[c]) == 8
+                              ? reinterpret_cast<const unsigned long long*>(sbase + coff[c])[j]
+                              : reinterpret_cast<const unsigned*>(sbase + coff[c])[j];
+          } else {
+            key[u] = load_key_g(q, r0 + j);
+#pragma unroll
+            for (int c = 0; c < GBA_MAX_COLS; ++c)
+              if (c < q.ncols)
+                r[u][c] = col_bytes(q.col_type[c]) == 8
+                              ? __ldg(static_cast<const unsigned long long*>(q.cols[c]) + r0 + j)
+                              : __ldg(static_cast<const unsigned*>(q.cols[c]) + r0 + j);
+          }
         }
       }
-      unsigned long long v[GBA_MAX_AGGS];
 #pragma unroll
-      for (int a = 0; a < GBA_MAX_AGGS; ++a) {
-        if (a < q.naccs) {
-          v[a] = acc_contrib(q.acc_op[a], q.acc_ctype[a], pick(q.acc_col[a], r[0], r[1], r[2], r[3]));
-        } else {
-          v[a] = 0ull;
-        }
+      for (int u = 0; u < R; ++u) {
+        const int j = j0 + u * nthr + tid;
+        unsigned long long v[NA];
+        row_contrib<NA>(q, r[u], v);
+        warp_insert<K64, NA>(P, st, j < rows, key[u], v);
       }
-      warp_insert<K64>(P, st, valid, key, v);
     }
     __syncthreads();  // stage s fully consumed
     if (via_tma && tid == 0) {
@@ -297,17 +217,17 @@ __global__ void __launch_bounds__(512) k_preagg(PreaggParams P) {
   __syncthreads();
   for (int i = tid; i < P.S; i += nthr) {
     const uint64_t k = st.keys[i];
-    if (k == (K64 ? EMPTY64 : uint64_t(EMPTY32))) continue;
-    unsigned long long v[GBA_MAX_AGGS];
+    if (k == uint64_t(smem_empty_key<K64>())) continue;
+    unsigned long long v[NA];
 #pragma unroll
-    for (int a = 0; a < GBA_MAX_AGGS; ++a) v[a] = a < q.naccs ? st.acc[size_t(a) * P.S + i] : 0ull;
-    gtable_insert<K64>(P.gt, q.naccs, q.acc_op, k, key_hash<K64>(k, GBA_TABLE_SEED), v, P.flags);
+    for (int a = 0; a < NA; ++a) v[a] = smem_acc_read<K64>(st, q, a, i);
+    gtable_insert<K64, NA>(P.gt, q.acc_op, k, table_hash(k), v, P.flags);
   }
   if (tid == 0 && P.S > 0 && *st.side_present) {
-    unsigned long long v[GBA_MAX_AGGS];
+    unsigned long long v[NA];
 #pragma unroll
-    for (int a = 0; a < GBA_MAX_AGGS; ++a) v[a] = st.side[a];
-    gtable_insert<K64>(P.gt, q.naccs, q.acc_op, K64 ? EMPTY64 : uint64_t(EMPTY32), 0u, v, P.flags);
+    for (int a = 0; a < NA; ++a) v[a] = smem_acc_read<K64>(st, q, a, -1);
+    gtable_insert<K64, NA>(P.gt, q.acc_op, K64 ? EMPTY64 : uint64_t(EMPTY32), 0u, v, P.flags);
   }
 }
 
@@ -379,9 +299,7 @@ __global__ void k_compact(GTable t, QDesc q, OutDesc o) {
 size_t gba_preagg_smem_bytes(const QDesc& q, int S, int T, int nstages, int use_tma) {
   size_t b = 128;
   if (use_tma) b += stage_bytes(q, T) * nstages;
-  b += align16(size_t(S) * key_bytes(q));
-  b += size_t(S) * q.naccs * 8;
-  b += GBA_MAX_AGGS * 8 + 16;
+  b += smem_table_bytes(S, q.key64, q.nwords);
   return b;
 }
 
@@ -403,17 +321,14 @@ cudaError_t gba_launch_preagg(const QDesc& q, const GTable& t, const PreaggCfg& 
   P.coalesce = c.coalesce;
   P.flags = flags;
   const size_t smem = gba_preagg_smem_bytes(q, P.S, P.T, P.nstages, P.use_tma);
-  cudaError_t e;
-  if (q.key64) {
-    e = cudaFuncSetAttribute(k_preagg<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  return gba_dispatch(q.key64 != 0, q.naccs, [&](auto K, auto N) -> cudaError_t {
+    constexpr bool k64 = decltype(K)::value;
+    constexpr int na = decltype(N)::value;
+    cudaError_t e = cudaFuncSetAttribute(k_preagg<k64, na>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
-    k_preagg<true><<<c.grid, c.block, smem, s>>>(P);
-  } else {
-    e = cudaFuncSetAttribute(k_preagg<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e != cudaSuccess) return e;
-    k_preagg<false><<<c.grid, c.block, smem, s>>>(P);
-  }
-  return cudaGetLastError();
+    k_preagg<k64, na><<<c.grid, c.block, smem, s>>>(P);
+    return cudaGetLastError();
+  });
 }
 
 cudaError_t gba_launch_compact(const GTable& t, const QDesc& q, const OutDesc& o, int grid, cudaStream_t s) {

@@ -1,0 +1,294 @@
+// Shared-memory open-addressing aggregation table, shared by the
+// pre-aggregation kernel and the per-partition aggregation kernel.
+//
+// Measured on B200 (sm_100a): shared-memory 32-bit atomicAdd runs at about
+// 3.4 T ops/s, 64-bit atomicAdd at about 0.5 T ops/s.  Accumulators are
+// therefore updated with 32-bit atomics wherever that stays exact:
+//   COUNT      32-bit add on the low word (a table lives for fewer than 2^32
+//              rows of one CTA)
+//   SUM int64  32-bit add on the low word; the add's own carry out of the
+//              low word is added to the high word with a second 32-bit add,
+//              issued only when nonzero.  The final 64-bit value is exactly
+//              the sum mod 2^64 because each carry is produced and accounted
+//              by the add that caused it.
+//   MIN / MAX  read first; the 64-bit atomic is issued only when the row
+//              improves on the value read (values only move one way, so a
+//              stale read can only cause an extra atomic, never a wrong skip).
+//   SUM fp32   fp64 atomicAdd.
+// NA (template) is the query's accumulator count.
+#pragma once
+#include <type_traits>
+
+#include "gba_internal.cuh"
+
+template <bool K64>
+struct SmemTable {
+  typedef typename std::conditional<K64, unsigned long long, unsigned>::type KeyW;
+  KeyW* keys;
+  unsigned long long* acc;   // [NA][S]
+  unsigned long long* side;  // [NA] accumulators of the all-ones key
+  unsigned* side_present;
+  int S;
+};
+
+template <bool K64>
+__device__ __forceinline__ typename SmemTable<K64>::KeyW smem_empty_key() {
+  return typename SmemTable<K64>::KeyW(K64 ? EMPTY64 : EMPTY32);
+}
+
+template <bool K64>
+__device__ __forceinline__ int smem_find_or_insert(const SmemTable<K64>& t, uint64_t key, uint32_t h, int cap) {
+  typedef typename SmemTable<K64>::KeyW KeyW;
+  const KeyW kk = KeyW(key);
+  const KeyW empty = smem_empty_key<K64>();
+  int s = int((uint64_t(h) * unsigned(t.S)) >> 32);
+  for (int p = 0; p < cap; ++p) {
+    KeyW cur = *(volatile KeyW*)&t.keys[s];
+    if (cur == kk) return s;
+    if (cur == empty) {
+      KeyW prev = atomicCAS(&t.keys[s], empty, kk);
+      if (prev == empty || prev == kk) return s;
+    }
+    s = (s + 1 == t.S) ? 0 : s + 1;
+  }
+  return -1;
+}
+
+// update one shared-memory accumulator
+__device__ __forceinline__ void smem_acc(int op, unsigned long long* p, unsigned long long v) {
+  switch (op) {
+    case ACC_CNT: atomicAdd(reinterpret_cast<unsigned*>(p), unsigned(v)); break;
+    case ACC_ADD_I: {
+      unsigned* w = reinterpret_cast<unsigned*>(p);
+      const unsigned lo = unsigned(v), hi = unsigned(v >> 32);
+      const unsigned old = atomicAdd(w, lo);
+      const unsigned add_hi = hi + ((old + lo) < old ? 1u : 0u);
+      if (add_hi) atomicAdd(w + 1, add_hi);
+      break;
+    }
+    case ACC_MIN_I:
+      if ((long long)v < *(volatile long long*)p) atomicMin(reinterpret_cast<long long*>(p), (long long)v);
+      break;
+    case ACC_MAX_I:
+      if ((long long)v > *(volatile long long*)p) atomicMax(reinterpret_cast<long long*>(p), (long long)v);
+      break;
+    default: break;  // ACC_ADD_F goes through smem_fsum
+  }
+}
+
+// fp32 SUM in shared memory: an exact 128-bit two's-complement fixed-point
+// accumulator with 64 fraction bits, held as four 32-bit limbs in words
+// fx[0..1], plus an fp64 residual in fx[2].  A contribution d (an fp32 value,
+// or an fp64 sum of a few of them after warp coalescing) is added exactly when
+// its binary expansion lies in [2^-64, 2^30): it is written as m * 2^shift with
+// a 53-bit integer m and added limb by limb with 32-bit atomics, each carry
+// forwarded by the add that produced it (so the limbs hold the exact sum mod
+// 2^128; sums of fewer than 2^32 such values stay below 2^62 in magnitude).
+// Anything else (NaN, infinities, |d| >= 2^30, bits below 2^-64) is added to
+// the fp64 residual.  32-bit shared atomics keep their rate when many threads
+// hit one hot key (measured 4.3 T/s on 8 slots, against 48 G/s for fp64
+// atomicAdd, which contends like a compare-and-swap loop).
+// The three words of one accumulator sit at w0[0], w0[stride], w0[2*stride]
+// (stride = table slots S in the slot arrays, 1 in the side slot).
+__device__ __forceinline__ void smem_fsum(unsigned long long* w0, size_t stride, double d) {
+  const unsigned long long bits = __double_as_longlong(d);
+  const int ex = int((bits >> 52) & 0x7ff);
+  unsigned long long m = bits & ((1ull << 52) - 1);
+  if (ex == 0 && m == 0) return;  // +-0
+  bool exact = ex != 0 && ex != 0x7ff;
+  int shift = ex - 1075 + 64;  // d = (m | 2^52) * 2^(ex-1075)
+  if (exact) {
+    m |= 1ull << 52;
+    if (shift < 0) {
+      const int r = -shift;
+      if (r >= 53 || (m & ((1ull << r) - 1))) exact = false;
+      else {
+        m >>= r;
+        shift = 0;
+      }
+    }
+    if (shift > 41) exact = false;  // |d| >= 2^30
+  }
+  if (!exact) {
+    atomicAdd(reinterpret_cast<double*>(w0 + 2 * stride), d);
+    return;
+  }
+  unsigned long long vlo = shift ? (m << shift) : m;
+  unsigned long long vhi = shift ? (m >> (64 - shift)) : 0ull;
+  if (bits >> 63) {  // negate (two's complement, 128 bits)
+    vlo = ~vlo + 1ull;
+    vhi = ~vhi + (vlo == 0ull ? 1ull : 0ull);
+  }
+  unsigned* const limb[4] = {reinterpret_cast<unsigned*>(w0), reinterpret_cast<unsigned*>(w0) + 1,
+                             reinterpret_cast<unsigned*>(w0 + stride), reinterpret_cast<unsigned*>(w0 + stride) + 1};
+  const unsigned v[4] = {unsigned(vlo), unsigned(vlo >> 32), unsigned(vhi), unsigned(vhi >> 32)};
+  unsigned carry = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const unsigned long long t = (unsigned long long)v[i] + carry;
+    const unsigned add = unsigned(t);
+    const unsigned k = unsigned(t >> 32);
+    if (add == 0u) {
+      carry = k;
+    } else if (i < 3) {
+      const unsigned old = atomicAdd(limb[i], add);
+      carry = k + ((old + add) < old ? 1u : 0u);
+    } else {
+      atomicAdd(limb[3], add);  // carries out of bit 127 are discarded (mod 2^128)
+    }
+  }
+}
+
+// value of an fp32-SUM accumulator as fp64 bits (one rounding of the exact
+// fixed-point sum, plus the residual)
+__device__ __forceinline__ unsigned long long smem_fsum_read(const unsigned long long* w0, size_t stride) {
+  const long long hi = (long long)w0[stride];
+  const unsigned long long lo = w0[0];
+  const double d = double(hi) + double(lo) * 0x1p-64 + __longlong_as_double(w0[2 * stride]);
+  return __double_as_longlong(d);
+}
+
+// accumulator a of slot i (or of the side slot when i < 0) as its 8-byte
+// result value
+template <bool K64>
+__device__ __forceinline__ unsigned long long smem_acc_read(const SmemTable<K64>& t, const QDesc& q, int a, int i) {
+  const unsigned long long* w0 = i >= 0 ? t.acc + size_t(q.acc_woff[a]) * t.S + i : t.side + q.acc_woff[a];
+  const size_t stride = i >= 0 ? size_t(t.S) : 1;
+  return q.acc_op[a] == ACC_ADD_F ? smem_fsum_read(w0, stride) : w0[0];
+}
+
+// init all slots (called by the whole CTA; caller syncs): every accumulator
+// word starts at its op's identity (fixed-point words and residual at 0)
+template <bool K64, int NA>
+__device__ __forceinline__ void smem_table_init(const SmemTable<K64>& t, const QDesc& q) {
+  for (int i = threadIdx.x; i < t.S; i += blockDim.x) {
+    t.keys[i] = smem_empty_key<K64>();
+#pragma unroll
+    for (int a = 0; a < NA; ++a) {
+      const unsigned long long id = acc_identity(q.acc_op[a]);
+      unsigned long long* w = t.acc + size_t(q.acc_woff[a]) * t.S + i;
+      w[0] = id;
+      if (q.acc_op[a] == ACC_ADD_F) {
+        w[t.S] = 0ull;
+        w[2 * size_t(t.S)] = 0ull;
+      }
+    }
+  }
+  if (threadIdx.x == 0) {
+    for (int w = 0; w < q.nwords; ++w) t.side[w] = 0ull;
+#pragma unroll
+    for (int a = 0; a < NA; ++a)
+      if (q.acc_op[a] != ACC_ADD_F) t.side[q.acc_woff[a]] = acc_identity(q.acc_op[a]);
+    *t.side_present = 0u;
+  }
+}
+
+// Warp-cooperative coalescing of equal keys (all 32 lanes call it).  Lanes
+// holding the same key combine their contributions and only the group's
+// lowest lane (returned true) applies the combined update:
+//   - every live lane holds the same key (the hot-key case): xor-butterfly
+//     reduction, 5 shuffle rounds per accumulator;
+//   - largest group <= 4 lanes: each lane walks its (small) group;
+//   - otherwise: no combining; each lane applies its own row (atomics to the
+//     same address are serialised by the hardware, but the walk would cost
+//     more than that).
+template <bool K64, int NA>
+__device__ __forceinline__ bool warp_coalesce(const QDesc& q, bool live, uint64_t key,
+                                              unsigned long long (&v)[NA]) {
+  const unsigned lane = lane_id();
+  const unsigned live_mask = __ballot_sync(GBA_FULL_MASK, live);
+  unsigned peers;
+  if constexpr (K64) peers = __match_any_sync(GBA_FULL_MASK, (unsigned long long)key);
+  else peers = __match_any_sync(GBA_FULL_MASK, unsigned(key));
+  peers &= live_mask;
+  const unsigned gsize = live ? __popc(peers) : 0u;
+  const unsigned maxg = __reduce_max_sync(GBA_FULL_MASK, gsize);
+  if (maxg <= 1) return live;
+  if (maxg == unsigned(__popc(live_mask))) {
+    // one key across all live lanes: dead lanes contribute identities
+    if (!live) {
+#pragma unroll
+      for (int a = 0; a < NA; ++a) v[a] = acc_identity(q.acc_op[a]);
+    }
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+#pragma unroll
+      for (int a = 0; a < NA; ++a) v[a] = acc_combine(q.acc_op[a], v[a], __shfl_xor_sync(GBA_FULL_MASK, v[a], o));
+    }
+    return live && lane == unsigned(__ffs(live_mask) - 1);
+  }
+  if (maxg > 4) return live;
+  // small groups: each lane sums its own peer group from the peers' ORIGINAL values
+  unsigned long long own[NA];
+#pragma unroll
+  for (int a = 0; a < NA; ++a) own[a] = v[a];
+  unsigned rem = live ? (peers & ~(1u << lane)) : 0u;
+#pragma unroll 1
+  for (unsigned i = 1; i < maxg; ++i) {
+    const int src = rem ? __ffs(rem) - 1 : int(lane);
+#pragma unroll
+    for (int a = 0; a < NA; ++a) {
+      unsigned long long x = __shfl_sync(GBA_FULL_MASK, own[a], src);
+      if (rem) v[a] = acc_combine(q.acc_op[a], v[a], x);
+    }
+    rem &= rem - 1u;
+  }
+  return live && ((peers & ((1u << lane) - 1u)) == 0u);
+}
+
+// apply a row (or coalesced partial) to shared slot `slot`
+template <bool K64, int NA>
+__device__ __forceinline__ void smem_apply(const SmemTable<K64>& t, const QDesc& q, int slot,
+                                           const unsigned long long (&v)[NA]) {
+#pragma unroll
+  for (int a = 0; a < NA; ++a) {
+    unsigned long long* w0 = t.acc + size_t(q.acc_woff[a]) * t.S + slot;
+    if (q.acc_op[a] == ACC_ADD_F) smem_fsum(w0, size_t(t.S), __longlong_as_double(v[a]));
+    else smem_acc(q.acc_op[a], w0, v[a]);
+  }
+}
+
+template <bool K64, int NA>
+__device__ __forceinline__ void smem_apply_side(const SmemTable<K64>& t, const QDesc& q,
+                                                const unsigned long long (&v)[NA]) {
+  if (*(volatile unsigned*)t.side_present == 0u) atomicExch(t.side_present, 1u);
+#pragma unroll
+  for (int a = 0; a < NA; ++a) {
+    unsigned long long* w0 = t.side + q.acc_woff[a];
+    if (q.acc_op[a] == ACC_ADD_F) smem_fsum(w0, 1, __longlong_as_double(v[a]));
+    else smem_acc(q.acc_op[a], w0, v[a]);
+  }
+}
+
+// smem bytes of a table with S slots of `nwords` accumulator words
+__host__ __device__ inline size_t smem_table_bytes(int S, int key64, int nwords) {
+  const size_t kb = key64 ? 8 : 4;
+  return ((size_t(S) * kb + 15) & ~size_t(15)) + size_t(S) * nwords * 8 + 3 * GBA_MAX_AGGS * 8 + 16;
+}
+
+// carve a table at `base` (16-byte aligned)
+template <bool K64>
+__device__ __forceinline__ SmemTable<K64> smem_table_carve(unsigned char* base, int S, int nwords) {
+  SmemTable<K64> t;
+  t.S = S;
+  size_t off = 0;
+  t.keys = reinterpret_cast<typename SmemTable<K64>::KeyW*>(base + off);
+  off += (size_t(S) * (K64 ? 8 : 4) + 15) & ~size_t(15);
+  t.acc = reinterpret_cast<unsigned long long*>(base + off);
+  off += size_t(S) * nwords * 8;
+  t.side = reinterpret_cast<unsigned long long*>(base + off);
+  off += 3 * GBA_MAX_AGGS * 8;
+  t.side_present = reinterpret_cast<unsigned*>(base + off);
+  return t;
+}
+
+// contribution of a row's raw column bits to each accumulator
+__device__ __forceinline__ unsigned long long pick_col(int c, const unsigned long long (&r)[GBA_MAX_COLS]) {
+  return c == 0 ? r[0] : c == 1 ? r[1] : c == 2 ? r[2] : r[3];
+}
+template <int NA>
+__device__ __forceinline__ void row_contrib(const QDesc& q, const unsigned long long (&raw)[GBA_MAX_COLS],
+                                            unsigned long long (&v)[NA]) {
+#pragma unroll
+  for (int a = 0; a < NA; ++a) v[a] = acc_contrib(q.acc_op[a], q.acc_ctype[a], pick_col(q.acc_col[a], raw));
+}

@@ -44,6 +44,8 @@ def lib() -> C.CDLL:
         L.orc_tile_partition_counts.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_void_p]
         L.orc_partition_of_u32.restype = C.c_uint32
         L.orc_partition_of_u32.argtypes = [C.c_uint32, C.c_uint32]
+        L.orc_partition_u32_array.restype = None
+        L.orc_partition_u32_array.argtypes = [C.c_void_p, C.c_int64, C.c_uint32, C.c_void_p]
         L.orc_merge_partitions.restype = C.c_int64
         L.orc_merge_partitions.argtypes = [C.c_void_p, C.c_int64, C.c_uint64, C.c_void_p, C.c_void_p]
         _lib = L
@@ -97,8 +99,11 @@ def tile_partition_counts(keys_u32: np.ndarray, tile_len: int, P: int) -> np.nda
 
 
 def partition_of_u32(keys_u32: np.ndarray, P: int) -> np.ndarray:
-    f = lib().orc_partition_of_u32
-    return np.array([f(int(k), P) for k in keys_u32], dtype=np.uint32)
+    """murmur3(key, seed 0) % P for every key (the reference's partition id)."""
+    keys_u32 = np.ascontiguousarray(keys_u32, dtype=np.uint32)
+    out = np.empty(keys_u32.shape[0], dtype=np.uint32)
+    lib().orc_partition_u32_array(keys_u32.ctypes.data, keys_u32.shape[0], P, out.ctypes.data)
+    return out
 
 
 def merge_partitions(sizes: np.ndarray, K: int):
@@ -110,15 +115,20 @@ def merge_partitions(sizes: np.ndarray, K: int):
     return merged_of, merged_sizes[:m]
 
 
-def fnv_pairs(keys: np.ndarray, vals: np.ndarray) -> str:
-    """FNV-1a 64 over (u32 key, u32 value) pairs sorted by (key, value) — the
-    digest the reference driver writes for each phase-1 partition."""
-    order = np.lexsort((vals.astype(np.uint32), keys.astype(np.uint32)))
-    b = np.empty((len(keys), 2), dtype=np.uint32)
-    b[:, 0] = keys.astype(np.uint32)[order]
-    b[:, 1] = vals.astype(np.uint32)[order]
-    h = 1469598103934665603
-    for byte in b.tobytes():
-        h ^= byte
-        h = (h * 1099511628211) & 0xFFFFFFFFFFFFFFFF
-    return f"{h:016x}"
+def _mix64(z: np.ndarray) -> np.ndarray:
+    z = z.astype(np.uint64)
+    with np.errstate(over="ignore"):
+        z ^= z >> np.uint64(31)
+        z *= np.uint64(0x7FB5D329728EA185)
+        z ^= z >> np.uint64(27)
+        z *= np.uint64(0x81DADEF4BC2DD44D)
+        z ^= z >> np.uint64(33)
+    return z
+
+
+def digest_pairs(keys: np.ndarray, vals: np.ndarray) -> str:
+    """Order-independent digest of (u32 key, u32 value) pairs: sum of
+    mix64(key << 32 | value) mod 2^64 - the digest oracle/ref_driver.cu writes."""
+    z = (keys.astype(np.uint32).astype(np.uint64) << np.uint64(32)) | vals.astype(np.uint32).astype(np.uint64)
+    with np.errstate(over="ignore"):
+        return f"{int(_mix64(z).sum(dtype=np.uint64)):016x}"

@@ -355,6 +355,9 @@ void orc_tile_partition_counts(const uint32_t* keys, int64_t n, int64_t tile_len
 
 // Partition of u32 keys as the reference's partitioner places them (seed 0).
 uint32_t orc_partition_of_u32(uint32_t key, uint32_t P) { return orc_murmur3_32(&key, 4, 0) % P; }
+void orc_partition_u32_array(const uint32_t* keys, int64_t n, uint32_t P, uint32_t* out) {
+  for (int64_t i = 0; i < n; ++i) out[i] = orc_murmur3_32(&keys[i], 4, 0) % P;
+}
 
 // Greedy merge of partitions (min-heap by size, merge while the sum stays <= K),
 // restating groupby_agg_intra_partition.cu:13-48 with the same container

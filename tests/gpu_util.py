@@ -49,7 +49,8 @@ def compare(gk, gaggs, keys, cols, aggs, label=""):
 def run_gpu(ctx, keys, cols, aggs, knobs=None, capacity=None):
     dk = to_device(keys)
     dcols = [to_device(c) for c in cols]
-    res = ctx.groupby(dk, dcols, aggs, knobs=knobs, capacity=capacity, unsigned_keys=keys.dtype == np.uint32)
+    res = ctx.groupby(dk, dcols, aggs, knobs=knobs, capacity=capacity, unsigned_keys=keys.dtype == np.uint32,
+                      unsigned_cols=[c.dtype == np.uint32 for c in cols])
     gk = res.keys.cpu().numpy()
     if keys.dtype == np.uint32:
         gk = gk.view(np.uint32)

@@ -40,7 +40,7 @@ def test_types_and_cardinalities(ctx, kdt, ndv):
 
 
 @pytest.mark.parametrize("knobs", [
-    dict(use_tma=0), dict(use_tma=1), dict(coalesce=0), dict(preagg=0), dict(smem_slots=64),
+    dict(use_tma=0), dict(use_tma=1), dict(coalesce=0), dict(coalesce=1), dict(preagg=0), dict(smem_slots=64),
     dict(smem_probe_cap=1), dict(tile_rows=512, block_threads=128), dict(nstages=1), dict(blocks_per_sm=2),
     dict(strategy="table"),
 ])
@@ -62,8 +62,9 @@ def test_misaligned_columns_fall_back_from_tma(ctx):
     import torch
     keys, cols = _data(100_001, np.int64, 999, seed=9)
     dk = torch.from_numpy(np.concatenate([[0], keys])).cuda()[1:]  # 8-byte but not 16-byte aligned
-    dcols = [torch.from_numpy(np.concatenate([c[:1], c])).cuda()[1:] for c in cols]
-    res = ctx.groupby(dk, dcols, AGGS_ALL)
+    dcols = [torch.from_numpy(np.concatenate([c[:1], c]).view(np.int32 if c.dtype == np.uint32 else c.dtype)).cuda()[1:]
+             for c in cols]
+    res = ctx.groupby(dk, dcols, AGGS_ALL, unsigned_cols=[False, False, False, True])
     compare(res.keys.cpu().numpy(), [a.cpu().numpy() for a in res.aggs], keys, cols, AGGS_ALL, "misaligned")
 
 
@@ -88,7 +89,8 @@ def test_sentinel_and_extreme_keys(ctx):
 
 def test_regrow_on_overflow(ctx):
     keys, cols = _data(200_000, np.int64, 150_000, seed=4)
-    gk, ga, res = run_gpu(ctx, keys, cols, AGGS_ALL, knobs=dict(sizing="fixed", table_slots=1024, probe_cap=16))
+    gk, ga, res = run_gpu(ctx, keys, cols, AGGS_ALL,
+                          knobs=dict(sizing="fixed", table_slots=1024, probe_cap=32, max_regrow=6, strategy="table"))
     assert res.stats["regrows"] >= 1
     compare(gk, ga, keys, cols, AGGS_ALL, "regrow")
 
