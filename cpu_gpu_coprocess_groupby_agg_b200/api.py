@@ -149,6 +149,61 @@ class Context:
         g = ng.value
         return Result(okeys[:g], [t[:g] for t in oaggs], g, self.stats())
 
+    # ---- learned cardinality estimator ---------------------------------------
+    def est_param_count(self) -> int:
+        return int(self._lib.gba_estimator_param_count())
+
+    def est_load(self, params: np.ndarray) -> None:
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        assert p.shape == (self.est_param_count(),)
+        A.check(self._lib.gba_estimator_load(self._h, p.ctypes.data_as(C.POINTER(C.c_float))), self._h)
+
+    def est_get(self) -> np.ndarray:
+        p = np.empty(self.est_param_count(), dtype=np.float32)
+        A.check(self._lib.gba_estimator_get(self._h, p.ctypes.data_as(C.POINTER(C.c_float))), self._h)
+        return p
+
+    def est_predict(self, feats: np.ndarray) -> np.ndarray:
+        """log2(groups) predicted for each feature row."""
+        X = np.ascontiguousarray(feats, dtype=np.float32).reshape(-1, A.GBA_EST_FEATURES)
+        out = np.empty(X.shape[0], dtype=np.float32)
+        A.check(self._lib.gba_estimator_predict(self._h, X.shape[0], X.ctypes.data_as(C.POINTER(C.c_float)),
+                                                out.ctypes.data_as(C.POINTER(C.c_float))), self._h)
+        return out
+
+    def est_features(self, keys, unsigned: bool = False, tile_rows: int = 0, stream=None) -> np.ndarray:
+        """The 32 estimator features of a device key column."""
+        import torch
+        q = build_query(keys.numel(), keys.data_ptr(), _torch_type(keys, unsigned), [], [(A.COUNT, 0)])
+        out = np.empty(A.GBA_EST_FEATURES, dtype=np.float32)
+        s = stream if stream is not None else torch.cuda.current_stream(keys.device)
+        A.check(self._lib.gba_estimator_features(self._h, C.byref(q), tile_rows, C.c_void_p(s.cuda_stream),
+                                                 out.ctypes.data_as(C.POINTER(C.c_float))), self._h)
+        return out
+
+    def est_train(self, X: np.ndarray, log2_groups: np.ndarray, epochs: int = 100, batch: int = 128,
+                  lr: float = 1e-3, seed: int = 0) -> float:
+        """Trains the loaded weights on the GPU; returns the final MSE in (log2)^2."""
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        y = np.ascontiguousarray(log2_groups, dtype=np.float32)
+        loss = C.c_float(0)
+        A.check(self._lib.gba_estimator_train(self._h, X.shape[0], X.ctypes.data_as(C.POINTER(C.c_float)),
+                                              y.ctypes.data_as(C.POINTER(C.c_float)), epochs, batch, lr, seed,
+                                              C.byref(loss)), self._h)
+        return float(loss.value)
+
+    def est_grad(self, X: np.ndarray, log2_groups: np.ndarray):
+        """One forward/backward pass on the GPU: (gradients, loss) with the
+        target scaled as t = log2(groups) / 32."""
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        y = np.ascontiguousarray(log2_groups, dtype=np.float32)
+        g = np.empty(self.est_param_count(), dtype=np.float32)
+        loss = C.c_float(0)
+        A.check(self._lib.gba_estimator_grad(self._h, X.shape[0], X.ctypes.data_as(C.POINTER(C.c_float)),
+                                             y.ctypes.data_as(C.POINTER(C.c_float)),
+                                             g.ctypes.data_as(C.POINTER(C.c_float)), C.byref(loss)), self._h)
+        return g, float(loss.value)
+
     # ---- host-resident -----------------------------------------------------
     def groupby_host(self, keys: np.ndarray, cols: Sequence[np.ndarray] = (), aggs: Sequence = (("count", None),),
                      knobs=None, capacity: int | None = None, stream=None, out=None) -> Result:

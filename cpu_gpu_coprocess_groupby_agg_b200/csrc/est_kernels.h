@@ -1,0 +1,26 @@
+// Host-visible interface of the cardinality estimator kernels (k_est.cu).
+#pragma once
+#include "gba_kernels.h"
+
+#define GBA_EST_MAX_TILES 256
+
+// One query's sampling job and its scratch (all device pointers).
+struct EstQuery {
+  const void* keys;
+  int64_t n;
+  int64_t tile_rows;
+  int64_t tile_step;    // sample every tile_step-th tile
+  int sampled_tiles;
+  int key64;
+  unsigned long long* table;  // cap x {key, count}
+  uint64_t cap;
+  unsigned* hll;              // 64 registers
+  float* feat;                // 32 features
+  unsigned long long* stats;  // [0] distinct sampled keys, [1] max count, [2] sampled rows, [3] all-ones key count
+};
+
+void gba_est_plan(EstQuery* e, int64_t n, int64_t tile_rows);
+int64_t gba_est_nparam();
+cudaError_t gba_launch_est_sample(const EstQuery* d_qs, int nq, int64_t max_items, cudaStream_t s);
+cudaError_t gba_launch_est_reduce(const EstQuery* d_qs, int nq, cudaStream_t s);
+cudaError_t gba_launch_mlp_forward(const float* W, const float* X, int n, float* out, cudaStream_t s);

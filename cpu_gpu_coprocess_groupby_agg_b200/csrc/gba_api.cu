@@ -81,6 +81,7 @@ extern "C" gba_status gba_destroy(gba_context* ctx) {
   if (ctx->d_small) cudaFree(ctx->d_small);
   if (ctx->h_small) cudaFreeHost(ctx->h_small);
   if (ctx->d_est) cudaFree(ctx->d_est);
+  if (ctx->est_ws) cudaFree(ctx->est_ws);
   for (auto& e : ctx->ev)
     if (e) cudaEventDestroy(e);
   for (auto& e : ctx->tev)
@@ -137,6 +138,21 @@ gba_status gba_stage_reserve(gba_context* ctx, size_t bytes, cudaStream_t s) {
     return GBA_ERR_OOM;
   }
   ctx->stage_bytes = want;
+  return GBA_OK;
+}
+
+gba_status gba_est_reserve(gba_context* ctx, size_t bytes, cudaStream_t s) {
+  if (bytes <= ctx->est_ws_bytes) return GBA_OK;
+  if (ctx->est_ws) {
+    GBA_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    GBA_CUDA_TRY(ctx, cudaDeviceSynchronize());
+    cudaFree(ctx->est_ws);
+    ctx->est_ws = nullptr;
+    ctx->est_ws_bytes = 0;
+  }
+  const size_t want = gba_round_up(std::max(bytes, size_t(1) << 22), size_t(1) << 21);
+  GBA_CUDA_TRY(ctx, cudaMalloc(&ctx->est_ws, want));
+  ctx->est_ws_bytes = want;
   return GBA_OK;
 }
 
@@ -250,6 +266,27 @@ gba_status gba_build_qdesc(gba_context* ctx, const gba_query* q, QDesc* d) {
 
 static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
+// Drops value columns no aggregate reads (they are never streamed) and remaps
+// the aggregates' column indices; aggregate order is unchanged.
+void gba_compact_query(const gba_query* in, gba_query* out) {
+  *out = *in;
+  int remap[GBA_MAX_COLS];
+  int nc = 0;
+  for (int c = 0; c < in->n_cols && c < GBA_MAX_COLS; ++c) {
+    bool used = false;
+    for (int a = 0; a < in->n_aggs && a < GBA_MAX_AGGS; ++a)
+      used = used || (in->aggs[a].op != GBA_COUNT && in->aggs[a].col == c);
+    remap[c] = used ? nc : -1;
+    if (used) out->cols[nc++] = in->cols[c];
+  }
+  out->n_cols = nc;
+  for (int a = 0; a < in->n_aggs && a < GBA_MAX_AGGS; ++a) {
+    const int c = in->aggs[a].col;
+    if (in->aggs[a].op == GBA_COUNT) out->aggs[a].col = 0;
+    else out->aggs[a].col = (c >= 0 && c < in->n_cols && c < GBA_MAX_COLS) ? remap[c] : c;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Plan: everything the single-query driver decides before launching.
 void gba_make_plan(const gba_context* ctx, const QDesc& q, const gba_knobs& k, double predicted_groups,
@@ -296,9 +333,15 @@ void gba_make_plan(const gba_context* ctx, const QDesc& q, const gba_knobs& k, d
   int preagg = k.preagg;
   if (preagg < 0) {
     preagg = 1;
-    if (k.sizing == GBA_SIZING_LEARNED && predicted_groups > 0 && q.n > 0 &&
-        predicted_groups > 0.5 * double(q.n))
-      preagg = 0;  // nearly all keys distinct: pre-aggregation only costs time
+    if (k.sizing == GBA_SIZING_LEARNED && predicted_groups > 0 && q.n > 0) {
+      // A CTA's shared table catches a row when its key is among the few
+      // thousand the table holds: worth it when the groups fit a handful of
+      // tables, or when the sample shows hot keys (the top key alone holds
+      // >= 0.1% of the rows); otherwise every row pays a lookup and a miss.
+      const double slots = double(ctx->max_smem_optin) / double((q.key64 ? 8 : 4) + 8 * q.nwords);
+      if (predicted_groups > 4.0 * slots && ctx->est_skew < 1e-3) preagg = 0;
+      if (predicted_groups > 0.5 * double(q.n)) preagg = 0;  // nearly all keys distinct
+    }
   }
   p->preagg = preagg;
   const size_t slot_bytes = (q.key64 ? 8 : 4) + 8 * size_t(q.nwords);
@@ -431,6 +474,9 @@ extern "C" gba_status gba_groupby(gba_context* ctx, const gba_query* q, const gb
   gba_knobs k;
   if (knobs) k = *knobs;
   else gba_default_knobs(&k);
+  gba_query qc;
+  gba_compact_query(q, &qc);
+  q = &qc;
   QDesc qd;
   gba_status st = gba_build_qdesc(ctx, q, &qd);
   if (st != GBA_OK) return st;

@@ -27,9 +27,14 @@ struct gba_context {
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev[8] = {};
   cudaEvent_t tev[16] = {};  // timing events (gba_knobs.timing)
-  // estimator (device weights + Adam state)
+  // estimator (device weights + Adam state + gradient scratch)
   float* d_est = nullptr;
   bool est_loaded = false;
+  // estimator sampling scratch (count tables, HLL registers, features)
+  void* est_ws = nullptr;
+  size_t est_ws_bytes = 0;
+  // share of the last estimator sample taken by its most frequent key
+  double est_skew = 0.0;
   std::string err;
   gba_stats stats{};
 };
@@ -59,6 +64,11 @@ struct GbaTimer {
 
 gba_status gba_ws_reserve(gba_context* ctx, size_t bytes, cudaStream_t s);
 gba_status gba_small_reserve(gba_context* ctx, size_t bytes);
+gba_status gba_est_reserve(gba_context* ctx, size_t bytes, cudaStream_t s);
+// estimator features of nq device queries into ctx->est_ws (device pointers)
+gba_status gba_est_features_device(gba_context* ctx, const QDesc* qs, int nq, int64_t tile_rows, cudaStream_t s,
+                                   float** feats_out, unsigned long long** stats_out);
 gba_status gba_build_qdesc(gba_context* ctx, const gba_query* q, QDesc* d);
+void gba_compact_query(const gba_query* in, gba_query* out);
 size_t gba_round_up(size_t x, size_t a);
 uint64_t gba_pow2_ceil(uint64_t x);

@@ -25,6 +25,9 @@ extern "C" gba_status gba_groupby_host(gba_context* ctx, const gba_query* q, con
   gba_knobs k;
   if (knobs) k = *knobs;
   else gba_default_knobs(&k);
+  gba_query qc;
+  gba_compact_query(q, &qc);
+  q = &qc;
   QDesc hq;
   gba_status st = gba_build_qdesc(ctx, q, &hq);
   if (st != GBA_OK) return st;

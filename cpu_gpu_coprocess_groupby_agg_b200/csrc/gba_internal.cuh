@@ -168,6 +168,36 @@ __device__ __forceinline__ void gtable_insert(const GTable& t, const int* ops, u
   for (int a = 0; a < NA; ++a) global_acc(ops[a], slotp + 1 + a, vals[a]);
 }
 
+// The same insert split in two so a thread can have several first probes in
+// flight: gtable_first_slot() gives the home slot; the caller loads its key
+// word with __ldcg for each pending insert, then finishes each one.
+__device__ __forceinline__ uint64_t gtable_home(const GTable& t, uint32_t h) { return (uint64_t(h) * t.cap) >> 32; }
+
+template <bool K64, int NA>
+__device__ __forceinline__ void gtable_finish(const GTable& t, const int* ops, uint64_t key, uint64_t s,
+                                              unsigned long long cur, const unsigned long long* vals,
+                                              unsigned* flags) {
+  constexpr int stride = 1 + NA;
+  unsigned long long* slotp = t.base + s * stride;
+  int p = 0;
+  for (;;) {
+    if (cur == key) break;
+    if (cur == EMPTY64) {
+      unsigned long long prev = atomicCAS(slotp, EMPTY64, key);
+      if (prev == EMPTY64 || prev == key) break;
+    }
+    if (++p >= t.probe_cap) {
+      atomicOr(flags, GBA_FLAG_TABLE_OVERFLOW);
+      return;
+    }
+    s = (s + 1 == t.cap) ? 0 : s + 1;
+    slotp = t.base + s * stride;
+    cur = __ldcg(slotp);
+  }
+#pragma unroll
+  for (int a = 0; a < NA; ++a) global_acc(ops[a], slotp + 1 + a, vals[a]);
+}
+
 // Compile-time dispatch over (key width, accumulator count): f(K64, NA) is
 // called with std::integral_constant arguments.
 #include <type_traits>

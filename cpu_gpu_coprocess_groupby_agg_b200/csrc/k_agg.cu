@@ -45,30 +45,40 @@ __host__ __device__ inline size_t stage_bytes(const QDesc& q, int T) {
   return b;
 }
 
-// One warp-wide insertion step: every lane holds at most one row.
-template <bool K64, int NA>
-__device__ __forceinline__ void warp_insert(const PreaggParams& P, const SmemTable<K64>& st, bool valid,
-                                            uint64_t key, unsigned long long (&v)[NA]) {
-  const QDesc& q = P.q;
-  const uint64_t emptyk = K64 ? EMPTY64 : uint64_t(EMPTY32);
-  const bool sent = valid && key == emptyk;
-  if (sent) {
-    if (P.S > 0) smem_apply_side<K64, NA>(st, q, v);
-    else gtable_insert<K64, NA>(P.gt, q.acc_op, key, 0u, v, P.flags);
+// Row j of the current tile: from the TMA stage or straight from HBM.
+template <bool K64>
+__device__ __forceinline__ void load_row(const QDesc& q, bool via_tma, const unsigned char* sbase,
+                                         const size_t (&coff)[GBA_MAX_COLS], int64_t r0, int j, uint64_t& key,
+                                         unsigned long long (&r)[GBA_MAX_COLS]) {
+#pragma unroll
+  for (int c = 0; c < GBA_MAX_COLS; ++c) r[c] = 0ull;
+  if (via_tma) {
+    key = K64 ? reinterpret_cast<const unsigned long long*>(sbase)[j] : reinterpret_cast<const unsigned*>(sbase)[j];
+#pragma unroll
+    for (int c = 0; c < GBA_MAX_COLS; ++c)
+      if (c < q.ncols)
+        r[c] = col_bytes(q.col_type[c]) == 8 ? reinterpret_cast<const unsigned long long*>(sbase + coff[c])[j]
+                                             : reinterpret_cast<const unsigned*>(sbase + coff[c])[j];
+  } else {
+    key = load_key_g(q, r0 + j);
+#pragma unroll
+    for (int c = 0; c < GBA_MAX_COLS; ++c)
+      if (c < q.ncols)
+        r[c] = col_bytes(q.col_type[c]) == 8 ? __ldg(static_cast<const unsigned long long*>(q.cols[c]) + r0 + j)
+                                             : __ldg(static_cast<const unsigned*>(q.cols[c]) + r0 + j);
   }
-  bool leader = valid && !sent;
-  if (P.coalesce) {  // warp-synchronous: every lane of the warp is here
-    if (!leader) key = emptyk;
-    leader = warp_coalesce<K64, NA>(q, leader, key, v);
-  }
-  if (!leader) return;
-  const uint32_t h = table_hash(key);
-  int slot = -1;
-  if (P.S > 0) slot = smem_find_or_insert<K64>(st, key, h, P.sprobe);
-  if (slot >= 0) smem_apply<K64, NA>(st, q, slot, v);
-  else gtable_insert<K64, NA>(P.gt, q.acc_op, key, h, v, P.flags);
 }
 
+// Each tile is processed in two phases.
+//  A: every row probes the CTA's shared table (capped probes) and updates it
+//     with 32-bit atomics; a row whose key is not there and cannot enter only
+//     records its index in the tile's miss list (warp-aggregated append).
+//  B: the CTA walks the miss list with two independent HBM-table inserts per
+//     thread in flight, so their L2 round trips overlap (the reference's
+//     kernels do one dependent probe chain per thread,
+//     kernel.cu:116-158).
+// With warp coalescing enabled the leaders' combined contributions cannot be
+// re-read from the tile, so their misses are inserted in phase A instead.
 template <bool K64, int NA>
 __global__ void __launch_bounds__(1024, 1) k_preagg(PreaggParams P) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -79,6 +89,7 @@ __global__ void __launch_bounds__(1024, 1) k_preagg(PreaggParams P) {
   const int64_t ntiles = (n + T - 1) / T;
   const int64_t nfull = n / T;
   const int kb = K64 ? 8 : 4;
+  const uint64_t emptyk = K64 ? EMPTY64 : uint64_t(EMPTY32);
 
   // ---- carve shared memory ------------------------------------------------------
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
@@ -86,8 +97,11 @@ __global__ void __launch_bounds__(1024, 1) k_preagg(PreaggParams P) {
   const size_t sb = stage_bytes(q, T);
   unsigned char* stage0 = smem + off;
   if (P.use_tma) off += sb * P.nstages;
+  unsigned short* miss = reinterpret_cast<unsigned short*>(smem + off);
+  off += align16(size_t(T) * 2);
   const SmemTable<K64> st = smem_table_carve<K64>(smem + off, P.S, q.nwords);
   __shared__ int s_abort;
+  __shared__ unsigned s_nmiss;
 
   // column offsets inside a stage
   size_t coff[GBA_MAX_COLS];
@@ -103,6 +117,7 @@ __global__ void __launch_bounds__(1024, 1) k_preagg(PreaggParams P) {
   smem_table_init<K64, NA>(st, q);
   if (tid == 0) {
     s_abort = 0;
+    s_nmiss = 0;
     if (P.use_tma) {
       for (int s = 0; s < P.nstages; ++s) mbar_init(&bars[s], 1);
       mbar_fence_init();
@@ -137,6 +152,7 @@ __global__ void __launch_bounds__(1024, 1) k_preagg(PreaggParams P) {
     }
   }
 
+  const unsigned lane = lane_id();
   unsigned phase = 0;  // bit s = parity to wait for on stage s
   int64_t it = 0;
   for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
@@ -151,8 +167,8 @@ __global__ void __launch_bounds__(1024, 1) k_preagg(PreaggParams P) {
     __syncthreads();
     if (s_abort) break;
     const unsigned char* sbase = stage0 + size_t(s) * sb;
-    // two rows per thread per step, both loaded before either is processed
-    // (without TMA the loads are the memory-level parallelism)
+
+    // ---- phase A: shared-table pass (two rows per thread loaded up front) ----
     constexpr int R = 2;
     for (int j0 = 0; j0 < T; j0 += R * nthr) {
       uint64_t key[R];
@@ -160,44 +176,87 @@ __global__ void __launch_bounds__(1024, 1) k_preagg(PreaggParams P) {
 #pragma unroll
       for (int u = 0; u < R; ++u) {
         const int j = j0 + u * nthr + tid;
-        key[u] = 0;
+        key[u] = emptyk;
+        if (j < rows) load_row<K64>(q, via_tma, sbase, coff, r0, j, key[u], r[u]);
+        else {
 #pragma unroll
-        for (int c = 0; c < GBA_MAX_COLS; ++c) r[u][c] = 0ull;
-        if (j < rows) {
-          if (via_tma) {
-            key[u] = K64 ? reinterpret_cast<const unsigned long long*>(sbase)[j]
-                         : reinterpret_cast<const unsigned*>(sbase)[j];
-#pragma unroll
-            for (int c = 0; c < GBA_MAX_COLS; ++c)
-              if (c < q.ncols)
-                r[u][c] = col_bytes(q.col_type[c]) == 8
-                              ? reinterpret_cast<const unsigned long long*>(sbase + coff[c])[j]
-                              : reinterpret_cast<const unsigned*>(sbase + coff[c])[j];
-          } else {
-            key[u] = load_key_g(q, r0 + j);
-#pragma unroll
-            for (int c = 0; c < GBA_MAX_COLS; ++c)
-              if (c < q.ncols)
-                r[u][c] = col_bytes(q.col_type[c]) == 8
-                              ? __ldg(static_cast<const unsigned long long*>(q.cols[c]) + r0 + j)
-                              : __ldg(static_cast<const unsigned*>(q.cols[c]) + r0 + j);
-          }
+          for (int c = 0; c < GBA_MAX_COLS; ++c) r[u][c] = 0ull;
         }
       }
 #pragma unroll
       for (int u = 0; u < R; ++u) {
         const int j = j0 + u * nthr + tid;
+        const bool valid = j < rows;
         unsigned long long v[NA];
         row_contrib<NA>(q, r[u], v);
-        warp_insert<K64, NA>(P, st, j < rows, key[u], v);
+        uint64_t k = key[u];
+        const bool sent = valid && k == emptyk;
+        if (sent) {
+          if (P.S > 0) smem_apply_side<K64, NA>(st, q, v);
+          else gtable_insert<K64, NA>(P.gt, q.acc_op, k, 0u, v, P.flags);
+        }
+        bool live = valid && !sent;
+        if (P.coalesce) {  // warp-synchronous: every lane of the warp is here
+          if (!live) k = emptyk;
+          live = warp_coalesce<K64, NA>(q, live, k, v);
+        }
+        bool missed = false;
+        if (live) {
+          int slot = -1;
+          const uint32_t h = table_hash(k);
+          if (P.S > 0) slot = smem_find_or_insert<K64>(st, k, h, P.sprobe);
+          if (slot >= 0) smem_apply<K64, NA>(st, q, slot, v);
+          else if (P.coalesce) gtable_insert<K64, NA>(P.gt, q.acc_op, k, h, v, P.flags);
+          else missed = true;
+        }
+        // warp-aggregated append of the misses to the tile's miss list
+        const unsigned mm = __ballot_sync(GBA_FULL_MASK, missed);
+        if (mm) {
+          unsigned base = 0;
+          if (lane == 0) base = atomicAdd(&s_nmiss, unsigned(__popc(mm)));
+          base = __shfl_sync(GBA_FULL_MASK, base, 0);
+          if (missed) miss[base + __popc(mm & ((1u << lane) - 1u))] = (unsigned short)j;
+        }
       }
     }
-    __syncthreads();  // stage s fully consumed
-    if (via_tma && tid == 0) {
-      const int64_t nxt = tile + int64_t(P.nstages) * gridDim.x;
-      if (nxt < nfull) {
-        fence_proxy_async_smem();
-        issue(nxt, s);
+    __syncthreads();
+
+    // ---- phase B: HBM-table inserts of the misses, two in flight per thread ----
+    const int nm = int(s_nmiss);
+    for (int i0 = 0; i0 < nm; i0 += 2 * nthr) {
+      uint64_t k[2];
+      uint64_t slot[2];
+      unsigned long long cur[2];
+      unsigned long long v[2][NA];
+      bool act[2];
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int i = i0 + u * nthr + tid;
+        act[u] = i < nm;
+        k[u] = 0;
+        slot[u] = 0;
+        unsigned long long rr[GBA_MAX_COLS] = {0ull, 0ull, 0ull, 0ull};
+        if (act[u]) {
+          load_row<K64>(q, via_tma, sbase, coff, r0, int(miss[i]), k[u], rr);
+          slot[u] = gtable_home(P.gt, table_hash(k[u]));
+        }
+        row_contrib<NA>(q, rr, v[u]);
+      }
+#pragma unroll
+      for (int u = 0; u < 2; ++u) cur[u] = act[u] ? __ldcg(P.gt.base + slot[u] * (1 + NA)) : 0ull;
+#pragma unroll
+      for (int u = 0; u < 2; ++u)
+        if (act[u]) gtable_finish<K64, NA>(P.gt, q.acc_op, k[u], slot[u], cur[u], v[u], P.flags);
+    }
+    __syncthreads();  // stage s and the miss list fully consumed
+    if (tid == 0) {
+      s_nmiss = 0;
+      if (via_tma) {
+        const int64_t nxt = tile + int64_t(P.nstages) * gridDim.x;
+        if (nxt < nfull) {
+          fence_proxy_async_smem();
+          issue(nxt, s);
+        }
       }
     }
   }
@@ -299,6 +358,7 @@ __global__ void k_compact(GTable t, QDesc q, OutDesc o) {
 size_t gba_preagg_smem_bytes(const QDesc& q, int S, int T, int nstages, int use_tma) {
   size_t b = 128;
   if (use_tma) b += stage_bytes(q, T) * nstages;
+  b += align16(size_t(T) * 2);  // miss list
   b += smem_table_bytes(S, q.key64, q.nwords);
   return b;
 }
