@@ -151,7 +151,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="skewed", choices=["skewed", "small", "highcard"])
-    ap.add_argument("--sizing", default="plain", choices=["plain", "learned"])
+    ap.add_argument("--sizing", default="learned", choices=["plain", "learned"])
+    ap.add_argument("--no-plain-compare", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--knob", action="append", default=[], help="name=value knob override")
@@ -172,8 +173,11 @@ def main():
         pg = dist
 
     from cpu_gpu_coprocess_groupby_agg_b200 import Context, gen_device, make_knobs
+    from cpu_gpu_coprocess_groupby_agg_b200 import estimator as E
     w = get_workload(args.workload)
     ctx = Context(local)
+    if args.sizing == "learned" and not E.load_default(ctx):
+        raise SystemExit(f"learned sizing needs trained weights at {E.WEIGHTS}")
     keys, cols = gen_device(w.spec, w.n, device=local)
     torch.cuda.synchronize()
     kn = {"sizing": args.sizing, "timing": 1}
@@ -243,6 +247,26 @@ def main():
         "gpu_launches": launches,
     }
     line["clocks"] = clk.summary()
+    line["config"]["predicted_groups"] = round(res.stats["predicted_groups"], 1)
+
+    if args.sizing == "learned" and not args.no_plain_compare:
+        # the same workload with plain (estimator-free) sizing, for comparison
+        pk = make_knobs(sizing="plain", timing=1)
+        for _ in range(2):
+            ctx.groupby(keys, cols, w.aggs, knobs=pk, out=(out_keys, out_aggs), stream=stream)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = max(2, min(args.steps, 5))
+        e0.record(stream)
+        for _ in range(reps):
+            pres = ctx.groupby(keys, cols, w.aggs, knobs=pk, out=(out_keys, out_aggs), stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        pms = e0.elapsed_time(e1) / reps
+        line["plain_sizing"] = {"value": round(w.n / (pms / 1e3) / 1e9, 4), "unit": "G rows/s",
+                                "ms_per_step": round(pms, 4), "strategy": pres.stats["strategy"],
+                                "table_slots": pres.stats["table_slots"],
+                                "partition_bits": pres.stats["partition_bits"]}
 
     if not args.no_e2e and rank == 0:
         line["e2e"] = e2e(ctx, w, keys, cols, knobs, args, ws)

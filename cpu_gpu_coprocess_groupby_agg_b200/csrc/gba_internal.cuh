@@ -138,9 +138,10 @@ __device__ __forceinline__ void global_acc(int op, unsigned long long* p, unsign
 // NA is the number of accumulators of the query (the table's slot stride is
 // 1 + NA words); kernels are instantiated per NA so no dead accumulator code
 // is emitted.
-template <bool K64, int NA>
-__device__ __forceinline__ void gtable_insert(const GTable& t, const int* ops, uint64_t key, uint32_t h,
+template <bool K64, typename Sig>
+__device__ __forceinline__ void gtable_insert(const GTable& t, const QDesc& q, uint64_t key, uint32_t h,
                                               const unsigned long long* vals, unsigned* flags) {
+  constexpr int NA = Sig::NA;
   constexpr int stride = 1 + NA;
   unsigned long long* slotp;
   if (key == (K64 ? EMPTY64 : uint64_t(EMPTY32))) {
@@ -165,7 +166,7 @@ __device__ __forceinline__ void gtable_insert(const GTable& t, const int* ops, u
     }
   }
 #pragma unroll
-  for (int a = 0; a < NA; ++a) global_acc(ops[a], slotp + 1 + a, vals[a]);
+  for (int a = 0; a < NA; ++a) global_acc(Sig::op(q, a), slotp + 1 + a, vals[a]);
 }
 
 // The same insert split in two so a thread can have several first probes in
@@ -173,10 +174,11 @@ __device__ __forceinline__ void gtable_insert(const GTable& t, const int* ops, u
 // word with __ldcg for each pending insert, then finishes each one.
 __device__ __forceinline__ uint64_t gtable_home(const GTable& t, uint32_t h) { return (uint64_t(h) * t.cap) >> 32; }
 
-template <bool K64, int NA>
-__device__ __forceinline__ void gtable_finish(const GTable& t, const int* ops, uint64_t key, uint64_t s,
+template <bool K64, typename Sig>
+__device__ __forceinline__ void gtable_finish(const GTable& t, const QDesc& q, uint64_t key, uint64_t s,
                                               unsigned long long cur, const unsigned long long* vals,
                                               unsigned* flags) {
+  constexpr int NA = Sig::NA;
   constexpr int stride = 1 + NA;
   unsigned long long* slotp = t.base + s * stride;
   int p = 0;
@@ -195,7 +197,7 @@ __device__ __forceinline__ void gtable_finish(const GTable& t, const int* ops, u
     cur = __ldcg(slotp);
   }
 #pragma unroll
-  for (int a = 0; a < NA; ++a) global_acc(ops[a], slotp + 1 + a, vals[a]);
+  for (int a = 0; a < NA; ++a) global_acc(Sig::op(q, a), slotp + 1 + a, vals[a]);
 }
 
 // Compile-time dispatch over (key width, accumulator count): f(K64, NA) is

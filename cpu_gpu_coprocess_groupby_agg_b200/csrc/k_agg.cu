@@ -16,6 +16,7 @@
 //                    caller's output columns (warp-aggregated output cursor).
 #include "gba_internal.cuh"
 #include "smem_table.cuh"
+#include "batch_kernels.h"
 
 namespace {
 
@@ -45,8 +46,9 @@ __host__ __device__ inline size_t stage_bytes(const QDesc& q, int T) {
   return b;
 }
 
-// Row j of the current tile: from the TMA stage or straight from HBM.
-template <bool K64>
+// Row j of the current tile: from the TMA stage or straight from HBM.  The
+// column count and types come from the signature (constants when compiled in).
+template <bool K64, typename Sig>
 __device__ __forceinline__ void load_row(const QDesc& q, bool via_tma, const unsigned char* sbase,
                                          const size_t (&coff)[GBA_MAX_COLS], int64_t r0, int j, uint64_t& key,
                                          unsigned long long (&r)[GBA_MAX_COLS]) {
@@ -56,16 +58,129 @@ __device__ __forceinline__ void load_row(const QDesc& q, bool via_tma, const uns
     key = K64 ? reinterpret_cast<const unsigned long long*>(sbase)[j] : reinterpret_cast<const unsigned*>(sbase)[j];
 #pragma unroll
     for (int c = 0; c < GBA_MAX_COLS; ++c)
-      if (c < q.ncols)
-        r[c] = col_bytes(q.col_type[c]) == 8 ? reinterpret_cast<const unsigned long long*>(sbase + coff[c])[j]
-                                             : reinterpret_cast<const unsigned*>(sbase + coff[c])[j];
+      if (c < Sig::ncols(q))
+        r[c] = col_bytes(Sig::coltype(q, c)) == 8 ? reinterpret_cast<const unsigned long long*>(sbase + coff[c])[j]
+                                                  : reinterpret_cast<const unsigned*>(sbase + coff[c])[j];
   } else {
-    key = load_key_g(q, r0 + j);
+    key = K64 ? __ldg(static_cast<const unsigned long long*>(q.keys) + r0 + j)
+              : __ldg(static_cast<const unsigned*>(q.keys) + r0 + j);
 #pragma unroll
     for (int c = 0; c < GBA_MAX_COLS; ++c)
-      if (c < q.ncols)
-        r[c] = col_bytes(q.col_type[c]) == 8 ? __ldg(static_cast<const unsigned long long*>(q.cols[c]) + r0 + j)
-                                             : __ldg(static_cast<const unsigned*>(q.cols[c]) + r0 + j);
+      if (c < Sig::ncols(q))
+        r[c] = col_bytes(Sig::coltype(q, c)) == 8 ? __ldg(static_cast<const unsigned long long*>(q.cols[c]) + r0 + j)
+                                                  : __ldg(static_cast<const unsigned*>(q.cols[c]) + r0 + j);
+  }
+}
+
+// Phases A and B of one tile (every thread of the CTA calls it; it syncs
+// between the phases, the caller syncs after it).
+template <bool K64, typename Sig>
+__device__ __forceinline__ void tile_two_phase(const QDesc& q, const GTable& gt, const SmemTable<K64>& st, int S,
+                                               int sprobe, int coalesce, bool via_tma, const unsigned char* sbase,
+                                               const size_t (&coff)[GBA_MAX_COLS], int64_t r0, int rows, int T,
+                                               unsigned short* miss, unsigned* s_nmiss, unsigned* flags) {
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const unsigned lane = lane_id();
+  const uint64_t emptyk = K64 ? EMPTY64 : uint64_t(EMPTY32);
+    // ---- phase A: shared-table pass (two rows per thread loaded up front) ----
+    constexpr int R = 2;
+    for (int j0 = 0; j0 < T; j0 += R * nthr) {
+      uint64_t key[R];
+      unsigned long long r[R][GBA_MAX_COLS];
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int j = j0 + u * nthr + tid;
+        key[u] = emptyk;
+        if (j < rows) load_row<K64, Sig>(q, via_tma, sbase, coff, r0, j, key[u], r[u]);
+        else {
+#pragma unroll
+          for (int c = 0; c < GBA_MAX_COLS; ++c) r[u][c] = 0ull;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int j = j0 + u * nthr + tid;
+        const bool valid = j < rows;
+        unsigned long long v[Sig::NA];
+        row_contrib<Sig>(q, r[u], v);
+        uint64_t k = key[u];
+        const bool sent = valid && k == emptyk;
+        if (sent) {
+          if (S > 0) smem_apply_side<K64, Sig>(st, q, v);
+          else gtable_insert<K64, Sig>(gt, q, k, 0u, v, flags);
+        }
+        bool live = valid && !sent;
+        if (coalesce) {  // warp-synchronous: every lane of the warp is here
+          if (!live) k = emptyk;
+          live = warp_coalesce<K64, Sig>(q, live, k, v);
+        }
+        bool missed = false;
+        if (live) {
+          int slot = -1;
+          const uint32_t h = table_hash(k);
+          if (S > 0) slot = smem_find_or_insert<K64>(st, k, h, sprobe);
+          if (slot >= 0) smem_apply<K64, Sig>(st, q, slot, v);
+          else if (coalesce) gtable_insert<K64, Sig>(gt, q, k, h, v, flags);
+          else missed = true;
+        }
+        // warp-aggregated append of the misses to the tile's miss list
+        const unsigned mm = __ballot_sync(GBA_FULL_MASK, missed);
+        if (mm) {
+          unsigned base = 0;
+          if (lane == 0) base = atomicAdd(s_nmiss, unsigned(__popc(mm)));
+          base = __shfl_sync(GBA_FULL_MASK, base, 0);
+          if (missed) miss[base + __popc(mm & ((1u << lane) - 1u))] = (unsigned short)j;
+        }
+      }
+    }
+    __syncthreads();
+
+    // ---- phase B: HBM-table inserts of the misses, two in flight per thread ----
+    const int nm = int(*s_nmiss);
+    for (int i0 = 0; i0 < nm; i0 += 2 * nthr) {
+      uint64_t k[2];
+      uint64_t slot[2];
+      unsigned long long cur[2];
+      unsigned long long v[2][Sig::NA];
+      bool act[2];
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int i = i0 + u * nthr + tid;
+        act[u] = i < nm;
+        k[u] = 0;
+        slot[u] = 0;
+        unsigned long long rr[GBA_MAX_COLS] = {0ull, 0ull, 0ull, 0ull};
+        if (act[u]) {
+          load_row<K64, Sig>(q, via_tma, sbase, coff, r0, int(miss[i]), k[u], rr);
+          slot[u] = gtable_home(gt, table_hash(k[u]));
+        }
+        row_contrib<Sig>(q, rr, v[u]);
+      }
+#pragma unroll
+      for (int u = 0; u < 2; ++u) cur[u] = act[u] ? __ldcg(gt.base + slot[u] * (1 + Sig::NA)) : 0ull;
+#pragma unroll
+      for (int u = 0; u < 2; ++u)
+        if (act[u]) gtable_finish<K64, Sig>(gt, q, k[u], slot[u], cur[u], v[u], flags);
+    }
+}
+
+// Merges a CTA's shared table into the HBM table (caller synced first).
+template <bool K64, typename Sig>
+__device__ __forceinline__ void flush_table(const QDesc& q, const GTable& gt, const SmemTable<K64>& st,
+                                            unsigned* flags) {
+  for (int i = threadIdx.x; i < st.S; i += blockDim.x) {
+    const uint64_t k = st.keys[i];
+    if (k == uint64_t(smem_empty_key<K64>())) continue;
+    unsigned long long v[Sig::NA];
+#pragma unroll
+    for (int a = 0; a < Sig::NA; ++a) v[a] = smem_acc_read<K64, Sig>(st, q, a, i);
+    gtable_insert<K64, Sig>(gt, q, k, table_hash(k), v, flags);
+  }
+  if (threadIdx.x == 0 && st.S > 0 && *st.side_present) {
+    unsigned long long v[Sig::NA];
+#pragma unroll
+    for (int a = 0; a < Sig::NA; ++a) v[a] = smem_acc_read<K64, Sig>(st, q, a, -1);
+    gtable_insert<K64, Sig>(gt, q, K64 ? EMPTY64 : uint64_t(EMPTY32), 0u, v, flags);
   }
 }
 
@@ -79,7 +194,7 @@ __device__ __forceinline__ void load_row(const QDesc& q, bool via_tma, const uns
 //     kernel.cu:116-158).
 // With warp coalescing enabled the leaders' combined contributions cannot be
 // re-read from the tile, so their misses are inserted in phase A instead.
-template <bool K64, int NA>
+template <bool K64, typename Sig>
 __global__ void __launch_bounds__(1024, 1) k_preagg(PreaggParams P) {
   extern __shared__ __align__(128) unsigned char smem[];
   const QDesc& q = P.q;
@@ -114,7 +229,7 @@ __global__ void __launch_bounds__(1024, 1) k_preagg(PreaggParams P) {
     }
   }
 
-  smem_table_init<K64, NA>(st, q);
+  smem_table_init<K64, Sig>(st, q);
   if (tid == 0) {
     s_abort = 0;
     s_nmiss = 0;
@@ -168,86 +283,8 @@ __global__ void __launch_bounds__(1024, 1) k_preagg(PreaggParams P) {
     if (s_abort) break;
     const unsigned char* sbase = stage0 + size_t(s) * sb;
 
-    // ---- phase A: shared-table pass (two rows per thread loaded up front) ----
-    constexpr int R = 2;
-    for (int j0 = 0; j0 < T; j0 += R * nthr) {
-      uint64_t key[R];
-      unsigned long long r[R][GBA_MAX_COLS];
-#pragma unroll
-      for (int u = 0; u < R; ++u) {
-        const int j = j0 + u * nthr + tid;
-        key[u] = emptyk;
-        if (j < rows) load_row<K64>(q, via_tma, sbase, coff, r0, j, key[u], r[u]);
-        else {
-#pragma unroll
-          for (int c = 0; c < GBA_MAX_COLS; ++c) r[u][c] = 0ull;
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < R; ++u) {
-        const int j = j0 + u * nthr + tid;
-        const bool valid = j < rows;
-        unsigned long long v[NA];
-        row_contrib<NA>(q, r[u], v);
-        uint64_t k = key[u];
-        const bool sent = valid && k == emptyk;
-        if (sent) {
-          if (P.S > 0) smem_apply_side<K64, NA>(st, q, v);
-          else gtable_insert<K64, NA>(P.gt, q.acc_op, k, 0u, v, P.flags);
-        }
-        bool live = valid && !sent;
-        if (P.coalesce) {  // warp-synchronous: every lane of the warp is here
-          if (!live) k = emptyk;
-          live = warp_coalesce<K64, NA>(q, live, k, v);
-        }
-        bool missed = false;
-        if (live) {
-          int slot = -1;
-          const uint32_t h = table_hash(k);
-          if (P.S > 0) slot = smem_find_or_insert<K64>(st, k, h, P.sprobe);
-          if (slot >= 0) smem_apply<K64, NA>(st, q, slot, v);
-          else if (P.coalesce) gtable_insert<K64, NA>(P.gt, q.acc_op, k, h, v, P.flags);
-          else missed = true;
-        }
-        // warp-aggregated append of the misses to the tile's miss list
-        const unsigned mm = __ballot_sync(GBA_FULL_MASK, missed);
-        if (mm) {
-          unsigned base = 0;
-          if (lane == 0) base = atomicAdd(&s_nmiss, unsigned(__popc(mm)));
-          base = __shfl_sync(GBA_FULL_MASK, base, 0);
-          if (missed) miss[base + __popc(mm & ((1u << lane) - 1u))] = (unsigned short)j;
-        }
-      }
-    }
-    __syncthreads();
-
-    // ---- phase B: HBM-table inserts of the misses, two in flight per thread ----
-    const int nm = int(s_nmiss);
-    for (int i0 = 0; i0 < nm; i0 += 2 * nthr) {
-      uint64_t k[2];
-      uint64_t slot[2];
-      unsigned long long cur[2];
-      unsigned long long v[2][NA];
-      bool act[2];
-#pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        const int i = i0 + u * nthr + tid;
-        act[u] = i < nm;
-        k[u] = 0;
-        slot[u] = 0;
-        unsigned long long rr[GBA_MAX_COLS] = {0ull, 0ull, 0ull, 0ull};
-        if (act[u]) {
-          load_row<K64>(q, via_tma, sbase, coff, r0, int(miss[i]), k[u], rr);
-          slot[u] = gtable_home(P.gt, table_hash(k[u]));
-        }
-        row_contrib<NA>(q, rr, v[u]);
-      }
-#pragma unroll
-      for (int u = 0; u < 2; ++u) cur[u] = act[u] ? __ldcg(P.gt.base + slot[u] * (1 + NA)) : 0ull;
-#pragma unroll
-      for (int u = 0; u < 2; ++u)
-        if (act[u]) gtable_finish<K64, NA>(P.gt, q.acc_op, k[u], slot[u], cur[u], v[u], P.flags);
-    }
+    tile_two_phase<K64, Sig>(q, P.gt, st, P.S, P.sprobe, P.coalesce, via_tma, sbase, coff, r0, rows, T, miss,
+                             &s_nmiss, P.flags);
     __syncthreads();  // stage s and the miss list fully consumed
     if (tid == 0) {
       s_nmiss = 0;
@@ -272,22 +309,8 @@ __global__ void __launch_bounds__(1024, 1) k_preagg(PreaggParams P) {
     return;
   }
 
-  // ---- flush the shared table into the HBM table -------------------------------
   __syncthreads();
-  for (int i = tid; i < P.S; i += nthr) {
-    const uint64_t k = st.keys[i];
-    if (k == uint64_t(smem_empty_key<K64>())) continue;
-    unsigned long long v[NA];
-#pragma unroll
-    for (int a = 0; a < NA; ++a) v[a] = smem_acc_read<K64>(st, q, a, i);
-    gtable_insert<K64, NA>(P.gt, q.acc_op, k, table_hash(k), v, P.flags);
-  }
-  if (tid == 0 && P.S > 0 && *st.side_present) {
-    unsigned long long v[NA];
-#pragma unroll
-    for (int a = 0; a < NA; ++a) v[a] = smem_acc_read<K64>(st, q, a, -1);
-    gtable_insert<K64, NA>(P.gt, q.acc_op, K64 ? EMPTY64 : uint64_t(EMPTY32), 0u, v, P.flags);
-  }
+  flush_table<K64, Sig>(q, P.gt, st, P.flags);
 }
 
 __global__ void k_table_init(GTable t, int naccs, QDesc q) {
@@ -351,6 +374,133 @@ __global__ void k_compact(GTable t, QDesc q, OutDesc o) {
   }
 }
 
+// ---- batched queries ----------------------------------------------------------------
+// One persistent launch per aggregate signature of a batch (both key widths):
+// CTAs pop (query, row range) items from a device work queue; each item is
+// aggregated through the CTA's shared table (sized per query, possibly empty)
+// and flushed into that query's HBM table, then the CTA takes the next item.
+template <bool K64, typename Sig>
+__device__ __forceinline__ void batch_item(const BatchQ& bq, const BatchItem& item, unsigned char* tbase,
+                                           unsigned short* miss, unsigned* s_nmiss, int sprobe, int T) {
+  const QDesc& q = bq.q;
+  const size_t coff[GBA_MAX_COLS] = {0, 0, 0, 0};
+  const SmemTable<K64> st = smem_table_carve<K64>(tbase, bq.S, q.nwords);
+  smem_table_init<K64, Sig>(st, q);
+  __syncthreads();
+  for (int64_t r0 = item.row_begin; r0 < item.row_end; r0 += T) {
+    const int rows = int(item.row_end - r0 < int64_t(T) ? item.row_end - r0 : int64_t(T));
+    tile_two_phase<K64, Sig>(q, bq.gt, st, bq.S, sprobe, 0, false, nullptr, coff, r0, rows, T, miss, s_nmiss,
+                             bq.flags);
+    __syncthreads();
+    if (threadIdx.x == 0) *s_nmiss = 0;
+    __syncthreads();
+  }
+  flush_table<K64, Sig>(q, bq.gt, st, bq.flags);
+}
+
+template <typename Sig>
+__global__ void __launch_bounds__(1024, 1) k_batch_preagg(const BatchQ* qs, const BatchItem* items, int nitems,
+                                                          unsigned* item_ctr, int sprobe, int T) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  unsigned short* miss = reinterpret_cast<unsigned short*>(smem);
+  unsigned char* tbase = smem + align16(size_t(T) * 2);
+  __shared__ int s_item;
+  __shared__ unsigned s_nmiss;
+  __shared__ __align__(16) BatchQ s_q;
+  const int tid = threadIdx.x;
+  for (;;) {
+    if (tid == 0) {
+      s_item = int(atomicAdd(item_ctr, 1u));
+      s_nmiss = 0;
+    }
+    __syncthreads();
+    const int it = s_item;
+    if (it >= nitems) break;
+    const BatchItem item = items[it];
+    {
+      const unsigned* src = reinterpret_cast<const unsigned*>(qs + item.qi);
+      unsigned* dst = reinterpret_cast<unsigned*>(&s_q);
+      for (int w = tid; w < int(sizeof(BatchQ) / 4); w += blockDim.x) dst[w] = src[w];
+    }
+    __syncthreads();
+    if (s_q.q.key64) batch_item<true, Sig>(s_q, item, tbase, miss, &s_nmiss, sprobe, T);
+    else batch_item<false, Sig>(s_q, item, tbase, miss, &s_nmiss, sprobe, T);
+    __syncthreads();  // s_q and the tables are rewritten by the next item
+  }
+}
+
+// table init for every query of a group (blockIdx.y = query)
+__global__ void k_batch_init(const BatchQ* qs, int nq) {
+  for (int qi = blockIdx.y; qi < nq; qi += gridDim.y) {
+    const GTable t = qs[qi].gt;
+    const QDesc& q = qs[qi].q;
+    const int stride = 1 + q.naccs;
+    const uint64_t total = (t.cap + 1) * stride;
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < total;
+         i += uint64_t(gridDim.x) * blockDim.x) {
+      const uint64_t slot = i / stride;
+      const int w = int(i - slot * stride);
+      unsigned long long v;
+      if (w == 0) v = slot == t.cap ? 0ull : EMPTY64;
+      else {
+        v = 0ull;
+#pragma unroll
+        for (int a = 0; a < GBA_MAX_AGGS; ++a)
+          if (a == w - 1) v = acc_identity(q.acc_op[a]);
+      }
+      t.base[i] = v;
+    }
+  }
+}
+
+// compaction of every query of a group (blockIdx.y = query)
+__global__ void k_batch_compact(const BatchQ* qs, int nq) {
+  for (int qi = blockIdx.y; qi < nq; qi += gridDim.y) {
+    const GTable t = qs[qi].gt;
+    const QDesc& q = qs[qi].q;
+    const OutDesc o = qs[qi].out;
+    const bool K64 = q.key64 != 0;
+    const int stride = 1 + q.naccs;
+    const unsigned lane = lane_id();
+    const uint64_t warp = (blockIdx.x * uint64_t(blockDim.x) + threadIdx.x) >> 5;
+    const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+    for (uint64_t base = warp * 32; base < t.cap; base += nwarps * 32) {
+      const uint64_t i = base + lane;
+      unsigned long long k = EMPTY64;
+      if (i < t.cap) k = t.base[i * stride];
+      const bool occ = k != EMPTY64;
+      const unsigned m = __ballot_sync(GBA_FULL_MASK, occ);
+      if (m == 0) continue;
+      unsigned long long pos0 = 0;
+      if (lane == 0) pos0 = atomicAdd(o.count, (unsigned long long)__popc(m));
+      pos0 = __shfl_sync(GBA_FULL_MASK, pos0, 0);
+      if (occ) {
+        const unsigned long long pos = pos0 + __popc(m & ((1u << lane) - 1u));
+        if (pos < (unsigned long long)o.capacity) {
+          if (K64) static_cast<unsigned long long*>(o.keys)[pos] = k;
+          else static_cast<unsigned*>(o.keys)[pos] = unsigned(k);
+#pragma unroll
+          for (int a = 0; a < GBA_MAX_AGGS; ++a)
+            if (a < q.naccs) o.accs[a][pos] = t.base[i * stride + 1 + a];
+        }
+      }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      const unsigned long long* side = t.base + t.cap * stride;
+      if (side[0] != 0ull) {
+        const unsigned long long pos = atomicAdd(o.count, 1ull);
+        if (pos < (unsigned long long)o.capacity) {
+          if (K64) static_cast<unsigned long long*>(o.keys)[pos] = EMPTY64;
+          else static_cast<unsigned*>(o.keys)[pos] = EMPTY32;
+#pragma unroll
+          for (int a = 0; a < GBA_MAX_AGGS; ++a)
+            if (a < q.naccs) o.accs[a][pos] = side[1 + a];
+        }
+      }
+    }
+  }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -381,12 +531,12 @@ cudaError_t gba_launch_preagg(const QDesc& q, const GTable& t, const PreaggCfg& 
   P.coalesce = c.coalesce;
   P.flags = flags;
   const size_t smem = gba_preagg_smem_bytes(q, P.S, P.T, P.nstages, P.use_tma);
-  return gba_dispatch(q.key64 != 0, q.naccs, [&](auto K, auto N) -> cudaError_t {
+  return gba_dispatch_sig(q, [&](auto K, auto sig) -> cudaError_t {
     constexpr bool k64 = decltype(K)::value;
-    constexpr int na = decltype(N)::value;
-    cudaError_t e = cudaFuncSetAttribute(k_preagg<k64, na>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    using Sig = decltype(sig);
+    cudaError_t e = cudaFuncSetAttribute(k_preagg<k64, Sig>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
-    k_preagg<k64, na><<<c.grid, c.block, smem, s>>>(P);
+    k_preagg<k64, Sig><<<c.grid, c.block, smem, s>>>(P);
     return cudaGetLastError();
   });
 }
@@ -394,5 +544,36 @@ cudaError_t gba_launch_preagg(const QDesc& q, const GTable& t, const PreaggCfg& 
 cudaError_t gba_launch_compact(const GTable& t, const QDesc& q, const OutDesc& o, int grid, cudaStream_t s) {
   if (q.key64) k_compact<true><<<grid, 256, 0, s>>>(t, q, o);
   else k_compact<false><<<grid, 256, 0, s>>>(t, q, o);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+size_t gba_batch_smem_bytes(const QDesc& q, int S, int T) {
+  // sized for 64-bit keys: one launch serves both key widths
+  return align16(size_t(T) * 2) + smem_table_bytes(S, 1, q.nwords) + 64;
+}
+size_t gba_batch_static_smem() { return sizeof(BatchQ) + 64; }
+
+cudaError_t gba_launch_batch_preagg(const QDesc& proto, const BatchQ* d_qs, const BatchItem* d_items, int nitems,
+                                    unsigned* item_ctr, int S_max, int sprobe, int T, int grid, cudaStream_t s) {
+  const size_t smem = gba_batch_smem_bytes(proto, S_max, T);
+  return gba_dispatch_sig(proto, [&](auto, auto sig) -> cudaError_t {
+    using Sig = decltype(sig);
+    cudaError_t e = cudaFuncSetAttribute(k_batch_preagg<Sig>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    k_batch_preagg<Sig><<<grid, 1024, smem, s>>>(d_qs, d_items, nitems, item_ctr, sprobe, T);
+    return cudaGetLastError();
+  });
+}
+
+cudaError_t gba_launch_batch_init(const BatchQ* d_qs, int nq, int gx, cudaStream_t s) {
+  dim3 g(gx, nq < 65535 ? nq : 65535);
+  k_batch_init<<<g, 256, 0, s>>>(d_qs, nq);
+  return cudaGetLastError();
+}
+
+cudaError_t gba_launch_batch_compact(const BatchQ* d_qs, int nq, int gx, cudaStream_t s) {
+  dim3 g(gx, nq < 65535 ? nq : 65535);
+  k_batch_compact<<<g, 256, 0, s>>>(d_qs, nq);
   return cudaGetLastError();
 }

@@ -268,7 +268,7 @@ __global__ void __launch_bounds__(512) k_part_scatter(PartPass p, int T) {
 }
 
 // ---- per-partition aggregation ------------------------------------------------------
-template <bool K64, int NA>
+template <bool K64, typename Sig>
 __global__ void __launch_bounds__(1024, 1) k_part_agg(PartAgg a) {
   extern __shared__ __align__(16) unsigned char sm[];
   const QDesc& q = a.rows;
@@ -285,7 +285,7 @@ __global__ void __launch_bounds__(1024, 1) k_part_agg(PartAgg a) {
     // rows (load <= 0.7) when that is smaller than the shared budget
     const int64_t want = (e - b) * 10 / 7 + 32;
     const SmemTable<K64> st = smem_table_carve<K64>(sm, int(want < a.S ? want : a.S), q.nwords);
-    smem_table_init<K64, NA>(st, q);
+    smem_table_init<K64, Sig>(st, q);
     __syncthreads();
     // a partition with many more rows than table slots repeats keys heavily
     // (skew): pre-combine equal keys inside each warp there
@@ -305,8 +305,8 @@ __global__ void __launch_bounds__(1024, 1) k_part_agg(PartAgg a) {
                         : __ldg(static_cast<const unsigned*>(q.keys) + r);
 #pragma unroll
           for (int c = 0; c < GBA_MAX_COLS; ++c)
-            if (c < q.ncols)
-              raw[u][c] = col_bytes_t(q.col_type[c]) == 8
+            if (c < Sig::ncols(q))
+              raw[u][c] = col_bytes_t(Sig::coltype(q, c)) == 8
                               ? __ldg(static_cast<const unsigned long long*>(q.cols[c]) + r)
                               : __ldg(static_cast<const unsigned*>(q.cols[c]) + r);
         }
@@ -319,21 +319,21 @@ __global__ void __launch_bounds__(1024, 1) k_part_agg(PartAgg a) {
         unsigned long long rr[GBA_MAX_COLS];
 #pragma unroll
         for (int c = 0; c < GBA_MAX_COLS; ++c) rr[c] = raw[u][c];
-        unsigned long long v[NA];
-        row_contrib<NA>(q, rr, v);
+        unsigned long long v[Sig::NA];
+        row_contrib<Sig>(q, rr, v);
         const bool sent = valid && key == emptyk;
-        if (sent) smem_apply_side<K64, NA>(st, q, v);
+        if (sent) smem_apply_side<K64, Sig>(st, q, v);
         bool leader = valid && !sent;
         if (coal) {  // CTA-uniform, so every lane of the warp is here
           if (!leader) key = emptyk;
-          leader = warp_coalesce<K64, NA>(q, leader, key, v);
+          leader = warp_coalesce<K64, Sig>(q, leader, key, v);
         }
         if (leader) {
           const uint32_t h = table_hash(key);
           const int slot = smem_find_or_insert<K64>(st, key, h, a.sprobe);
-          if (slot >= 0) smem_apply<K64, NA>(st, q, slot, v);
+          if (slot >= 0) smem_apply<K64, Sig>(st, q, slot, v);
           else {
-            gtable_insert<K64, NA>(a.fallback, q.acc_op, key, h, v, a.flags);
+            gtable_insert<K64, Sig>(a.fallback, q, key, h, v, a.flags);
             atomicOr(a.flags, GBA_FLAG_PART_OVERFLOW);
           }
         }
@@ -357,7 +357,7 @@ __global__ void __launch_bounds__(1024, 1) k_part_agg(PartAgg a) {
         if (K64) static_cast<unsigned long long*>(a.out.keys)[pos] = k;
         else static_cast<unsigned*>(a.out.keys)[pos] = unsigned(k);
 #pragma unroll
-        for (int x = 0; x < NA; ++x) a.out.accs[x][pos] = smem_acc_read<K64>(st, q, x, i);
+        for (int x = 0; x < Sig::NA; ++x) a.out.accs[x][pos] = smem_acc_read<K64, Sig>(st, q, x, i);
       }
       ++pos;
     }
@@ -367,7 +367,7 @@ __global__ void __launch_bounds__(1024, 1) k_part_agg(PartAgg a) {
         if (K64) static_cast<unsigned long long*>(a.out.keys)[sp] = EMPTY64;
         else static_cast<unsigned*>(a.out.keys)[sp] = EMPTY32;
 #pragma unroll
-        for (int x = 0; x < NA; ++x) a.out.accs[x][sp] = smem_acc_read<K64>(st, q, x, -1);
+        for (int x = 0; x < Sig::NA; ++x) a.out.accs[x][sp] = smem_acc_read<K64, Sig>(st, q, x, -1);
       }
     }
     __syncthreads();
@@ -444,12 +444,12 @@ cudaError_t gba_launch_part_scatter(const PartPass& p, int grid, int T, cudaStre
 
 cudaError_t gba_launch_part_agg(const PartAgg& a, int grid, cudaStream_t s) {
   const size_t smem = smem_table_bytes(a.S, a.rows.key64, a.rows.nwords) + 64;
-  return gba_dispatch(a.rows.key64 != 0, a.rows.naccs, [&](auto K, auto N) -> cudaError_t {
+  return gba_dispatch_sig(a.rows, [&](auto K, auto sig) -> cudaError_t {
     constexpr bool k64 = decltype(K)::value;
-    constexpr int na = decltype(N)::value;
-    cudaError_t e = cudaFuncSetAttribute(k_part_agg<k64, na>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    using Sig = decltype(sig);
+    cudaError_t e = cudaFuncSetAttribute(k_part_agg<k64, Sig>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
-    k_part_agg<k64, na><<<grid, 1024, smem, s>>>(a);
+    k_part_agg<k64, Sig><<<grid, 1024, smem, s>>>(a);
     return cudaGetLastError();
   });
 }

@@ -15,11 +15,12 @@
 //              improves on the value read (values only move one way, so a
 //              stale read can only cause an extra atomic, never a wrong skip).
 //   SUM fp32   fp64 atomicAdd.
-// NA (template) is the query's accumulator count.
+// Sig (template) is the query's aggregate signature (sig.cuh).
 #pragma once
 #include <type_traits>
 
 #include "gba_internal.cuh"
+#include "sig.cuh"
 
 template <bool K64>
 struct SmemTable {
@@ -150,35 +151,35 @@ __device__ __forceinline__ unsigned long long smem_fsum_read(const unsigned long
 
 // accumulator a of slot i (or of the side slot when i < 0) as its 8-byte
 // result value
-template <bool K64>
+template <bool K64, typename Sig>
 __device__ __forceinline__ unsigned long long smem_acc_read(const SmemTable<K64>& t, const QDesc& q, int a, int i) {
-  const unsigned long long* w0 = i >= 0 ? t.acc + size_t(q.acc_woff[a]) * t.S + i : t.side + q.acc_woff[a];
+  const unsigned long long* w0 = i >= 0 ? t.acc + size_t(Sig::woff(q, a)) * t.S + i : t.side + Sig::woff(q, a);
   const size_t stride = i >= 0 ? size_t(t.S) : 1;
-  return q.acc_op[a] == ACC_ADD_F ? smem_fsum_read(w0, stride) : w0[0];
+  return Sig::op(q, a) == ACC_ADD_F ? smem_fsum_read(w0, stride) : w0[0];
 }
 
 // init all slots (called by the whole CTA; caller syncs): every accumulator
 // word starts at its op's identity (fixed-point words and residual at 0)
-template <bool K64, int NA>
+template <bool K64, typename Sig>
 __device__ __forceinline__ void smem_table_init(const SmemTable<K64>& t, const QDesc& q) {
   for (int i = threadIdx.x; i < t.S; i += blockDim.x) {
     t.keys[i] = smem_empty_key<K64>();
 #pragma unroll
-    for (int a = 0; a < NA; ++a) {
-      const unsigned long long id = acc_identity(q.acc_op[a]);
-      unsigned long long* w = t.acc + size_t(q.acc_woff[a]) * t.S + i;
+    for (int a = 0; a < Sig::NA; ++a) {
+      const unsigned long long id = acc_identity(Sig::op(q, a));
+      unsigned long long* w = t.acc + size_t(Sig::woff(q, a)) * t.S + i;
       w[0] = id;
-      if (q.acc_op[a] == ACC_ADD_F) {
+      if (Sig::op(q, a) == ACC_ADD_F) {
         w[t.S] = 0ull;
         w[2 * size_t(t.S)] = 0ull;
       }
     }
   }
   if (threadIdx.x == 0) {
-    for (int w = 0; w < q.nwords; ++w) t.side[w] = 0ull;
+    for (int w = 0; w < Sig::nwords(q); ++w) t.side[w] = 0ull;
 #pragma unroll
-    for (int a = 0; a < NA; ++a)
-      if (q.acc_op[a] != ACC_ADD_F) t.side[q.acc_woff[a]] = acc_identity(q.acc_op[a]);
+    for (int a = 0; a < Sig::NA; ++a)
+      if (Sig::op(q, a) != ACC_ADD_F) t.side[Sig::woff(q, a)] = acc_identity(Sig::op(q, a));
     *t.side_present = 0u;
   }
 }
@@ -192,9 +193,10 @@ __device__ __forceinline__ void smem_table_init(const SmemTable<K64>& t, const Q
 //   - otherwise: no combining; each lane applies its own row (atomics to the
 //     same address are serialised by the hardware, but the walk would cost
 //     more than that).
-template <bool K64, int NA>
+template <bool K64, typename Sig>
 __device__ __forceinline__ bool warp_coalesce(const QDesc& q, bool live, uint64_t key,
-                                              unsigned long long (&v)[NA]) {
+                                              unsigned long long (&v)[Sig::NA]) {
+  constexpr int NA = Sig::NA;
   const unsigned lane = lane_id();
   const unsigned live_mask = __ballot_sync(GBA_FULL_MASK, live);
   unsigned peers;
@@ -208,12 +210,12 @@ __device__ __forceinline__ bool warp_coalesce(const QDesc& q, bool live, uint64_
     // one key across all live lanes: dead lanes contribute identities
     if (!live) {
 #pragma unroll
-      for (int a = 0; a < NA; ++a) v[a] = acc_identity(q.acc_op[a]);
+      for (int a = 0; a < NA; ++a) v[a] = acc_identity(Sig::op(q, a));
     }
 #pragma unroll
     for (int o = 16; o >= 1; o >>= 1) {
 #pragma unroll
-      for (int a = 0; a < NA; ++a) v[a] = acc_combine(q.acc_op[a], v[a], __shfl_xor_sync(GBA_FULL_MASK, v[a], o));
+      for (int a = 0; a < NA; ++a) v[a] = acc_combine(Sig::op(q, a), v[a], __shfl_xor_sync(GBA_FULL_MASK, v[a], o));
     }
     return live && lane == unsigned(__ffs(live_mask) - 1);
   }
@@ -229,7 +231,7 @@ __device__ __forceinline__ bool warp_coalesce(const QDesc& q, bool live, uint64_
 #pragma unroll
     for (int a = 0; a < NA; ++a) {
       unsigned long long x = __shfl_sync(GBA_FULL_MASK, own[a], src);
-      if (rem) v[a] = acc_combine(q.acc_op[a], v[a], x);
+      if (rem) v[a] = acc_combine(Sig::op(q, a), v[a], x);
     }
     rem &= rem - 1u;
   }
@@ -237,26 +239,26 @@ __device__ __forceinline__ bool warp_coalesce(const QDesc& q, bool live, uint64_
 }
 
 // apply a row (or coalesced partial) to shared slot `slot`
-template <bool K64, int NA>
+template <bool K64, typename Sig>
 __device__ __forceinline__ void smem_apply(const SmemTable<K64>& t, const QDesc& q, int slot,
-                                           const unsigned long long (&v)[NA]) {
+                                           const unsigned long long (&v)[Sig::NA]) {
 #pragma unroll
-  for (int a = 0; a < NA; ++a) {
-    unsigned long long* w0 = t.acc + size_t(q.acc_woff[a]) * t.S + slot;
-    if (q.acc_op[a] == ACC_ADD_F) smem_fsum(w0, size_t(t.S), __longlong_as_double(v[a]));
-    else smem_acc(q.acc_op[a], w0, v[a]);
+  for (int a = 0; a < Sig::NA; ++a) {
+    unsigned long long* w0 = t.acc + size_t(Sig::woff(q, a)) * t.S + slot;
+    if (Sig::op(q, a) == ACC_ADD_F) smem_fsum(w0, size_t(t.S), __longlong_as_double(v[a]));
+    else smem_acc(Sig::op(q, a), w0, v[a]);
   }
 }
 
-template <bool K64, int NA>
+template <bool K64, typename Sig>
 __device__ __forceinline__ void smem_apply_side(const SmemTable<K64>& t, const QDesc& q,
-                                                const unsigned long long (&v)[NA]) {
+                                                const unsigned long long (&v)[Sig::NA]) {
   if (*(volatile unsigned*)t.side_present == 0u) atomicExch(t.side_present, 1u);
 #pragma unroll
-  for (int a = 0; a < NA; ++a) {
-    unsigned long long* w0 = t.side + q.acc_woff[a];
-    if (q.acc_op[a] == ACC_ADD_F) smem_fsum(w0, 1, __longlong_as_double(v[a]));
-    else smem_acc(q.acc_op[a], w0, v[a]);
+  for (int a = 0; a < Sig::NA; ++a) {
+    unsigned long long* w0 = t.side + Sig::woff(q, a);
+    if (Sig::op(q, a) == ACC_ADD_F) smem_fsum(w0, 1, __longlong_as_double(v[a]));
+    else smem_acc(Sig::op(q, a), w0, v[a]);
   }
 }
 
@@ -286,9 +288,10 @@ __device__ __forceinline__ SmemTable<K64> smem_table_carve(unsigned char* base, 
 __device__ __forceinline__ unsigned long long pick_col(int c, const unsigned long long (&r)[GBA_MAX_COLS]) {
   return c == 0 ? r[0] : c == 1 ? r[1] : c == 2 ? r[2] : r[3];
 }
-template <int NA>
+template <typename Sig>
 __device__ __forceinline__ void row_contrib(const QDesc& q, const unsigned long long (&raw)[GBA_MAX_COLS],
-                                            unsigned long long (&v)[NA]) {
+                                            unsigned long long (&v)[Sig::NA]) {
 #pragma unroll
-  for (int a = 0; a < NA; ++a) v[a] = acc_contrib(q.acc_op[a], q.acc_ctype[a], pick_col(q.acc_col[a], raw));
+  for (int a = 0; a < Sig::NA; ++a)
+    v[a] = acc_contrib(Sig::op(q, a), Sig::ctype(q, a), pick_col(Sig::col(q, a), raw));
 }
