@@ -122,6 +122,7 @@ SIGNATURES = {
                                    C.POINTER(C.c_int64)]),
     "gba_groupby_batch": (C.c_int, [_P, C.c_int32, C.POINTER(Query), C.POINTER(Output), C.POINTER(Knobs), _P,
                                     C.POINTER(C.c_int64)]),
+    "gba_groupby_noalloc": (C.c_int, [_P, C.POINTER(Query), C.POINTER(Output), _P, C.POINTER(C.c_int64)]),
     "gba_estimator_features": (C.c_int, [_P, C.POINTER(Query), C.c_int64, _P, C.POINTER(C.c_float)]),
     "gba_estimator_param_count": (C.c_int64, []),
     "gba_estimator_load": (C.c_int, [_P, C.POINTER(C.c_float)]),

@@ -165,6 +165,27 @@ gba_status gba_groupby_host(gba_context* ctx, const gba_query* q, const gba_outp
 gba_status gba_groupby_batch(gba_context* ctx, int32_t n_queries, const gba_query* qs, const gba_output* outs,
                              const gba_knobs* knobs, void* stream, int64_t* n_groups);
 
+/* gba_groupby without any device allocation: the table strategy (plain
+ * sizing, 2 n + 64 slots) over a fixed 16 MiB scratch that is a static device
+ * array of the library, not the context's workspace.  No counterpart in the
+ * reference.
+ *
+ * For callers that must not allocate device memory per call: a process whose
+ * device memory a pool allocator already reserved (a fresh cudaMalloc can fail
+ * there), or a latency-sensitive thread whose device also runs other streams
+ * (cudaFree synchronises the whole device).
+ *
+ * Limit: (2 n_rows + 65) * (1 + n_aggs) * 8 + 256 bytes must fit in 16 MiB
+ * (about 349,000 rows with 2 aggregates); larger queries return
+ * GBA_ERR_INVALID_ARG with the limit in gba_last_error and launch nothing.
+ * The first call on a device looks up the scratch's address, which may load
+ * the library's device code: make it before any stream capture begins.  Every
+ * call clears the scratch's status and counter words and initialises its table
+ * itself.  All calls on one device share the scratch: calls that overlap in
+ * time on one device race; serialise them.  Synchronises `stream`. */
+gba_status gba_groupby_noalloc(gba_context* ctx, const gba_query* q, const gba_output* out, void* stream,
+                               int64_t* n_groups);
+
 /* ---- learned cardinality estimator -------------------------------------- */
 #define GBA_EST_FEATURES 32
 #define GBA_EST_HIDDEN 64
