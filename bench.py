@@ -1,14 +1,19 @@
 #!/usr/bin/env python
 """Benchmark of the hash GROUP BY path on B200 (one JSON line on stdout).
 
-Default workload: the skewed single query (2^26 rows, int64 keys Zipf s=1.0
-over 2^20 ids; SUM/COUNT/MIN/MAX of an int64 column and SUM of an fp32
-column).  A step is one exact GROUP BY of the whole table.
+Default workload (--workload batch): the 256-query mixed batch (rows
+log-uniform in [2^12, 2^24], distinct keys log-uniform in [16, rows/2], Zipf
+s in [0, 1.5], int32/int64 keys 50/50, SUM + COUNT of an int64 column).  A step
+is one gba_groupby_batch call over all 256 queries with learned sizing; the
+same batch with plain sizing is timed beside it (plain_sizing).  Single-query
+workloads: skewed (2^26 rows, int64 keys Zipf s=1.0 over 2^20 ids;
+SUM/COUNT/MIN/MAX of an int64 column and SUM of an fp32 column), small,
+highcard.
 
-  value  rows / s over K steps, inputs resident in HBM (1.34 GB > L2, so no
+  value  rows / s over K steps, inputs resident in HBM (several GB > L2, so no
          flush is needed between steps), device-timed with CUDA events.
-  e2e    the same through the host-buffer entry point (gba_groupby_host):
-         pinned host inputs copied H2D inside every step, results read back.
+  e2e    the same through the public API with host buffers: pinned host
+         inputs copied H2D inside every step, results read back.
   --impl reference
          the CPU restatement of the reference's algorithm (the reference has
          no CPU aggregation path) on all host cores, bounded sample per step.
@@ -105,6 +110,20 @@ def get_workload(name: str):
     return {"skewed": W.skewed, "small": W.small, "highcard": W.high_card}[name]()
 
 
+BATCH_NAME = "batch_256q_rows2^12-2^24_logu_ndv16-rows/2_zipf0-1.5_sum+count"
+
+
+def batch_cpu_sample(ws_list, limit=1 << 24):
+    """Leading queries of the batch whose rows add up to about `limit`."""
+    out, tot = [], 0
+    for w in ws_list:
+        if tot >= limit:
+            break
+        out.append(w)
+        tot += w.n
+    return out, tot
+
+
 def cpu_sample_rows(w) -> int:
     # about 10-30 s of single-pass CPU work over the steps of the reference arm
     return min(w.n, 1 << 24)
@@ -118,15 +137,32 @@ def run_reference(args, ws, rank):
     import numpy as np
     import cpu_oracle as O
     from cpu_gpu_coprocess_groupby_agg_b200 import gen_host
-    w = get_workload(args.workload)
     cores = os.cpu_count() or 1
-    m = cpu_sample_rows(w)
-    keys, cols = gen_host(w.spec, m, nthreads=cores)
+    if args.workload == "batch":
+        from cpu_gpu_coprocess_groupby_agg_b200 import workloads as W
+        allq = W.batch_queries()
+        sample, m = batch_cpu_sample(allq)
+        data = [gen_host(q.spec, q.n, nthreads=cores) for q in sample]
+        name, total_rows, aggs = BATCH_NAME, sum(q.n for q in allq), sample[0].aggs
+
+        def one():
+            for q, (k, c) in zip(sample, data):
+                O.groupby(k, c, q.aggs, nthreads=cores, sort=False)
+        what = f"the first {len(sample)} of the 256 queries ({m} rows) per step"
+    else:
+        w = get_workload(args.workload)
+        m = cpu_sample_rows(w)
+        keys, cols = gen_host(w.spec, m, nthreads=cores)
+        name, total_rows, aggs = w.name, w.n, w.aggs
+
+        def one():
+            O.groupby(keys, cols, w.aggs, nthreads=cores, sort=False)
+        what = f"first {m} rows of the workload per step"
     for _ in range(args.warmup):
-        O.groupby(keys, cols, w.aggs, nthreads=cores, sort=False)
+        one()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        O.groupby(keys, cols, w.aggs, nthreads=cores, sort=False)
+        one()
     dt = (time.perf_counter() - t0) / args.steps
     value = m / dt / 1e9
     line = {
@@ -134,10 +170,11 @@ def run_reference(args, ws, rank):
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
         "data": "synthetic (seeded PCG32 generator)",
-        "config": {"workload": w.name, "rows": w.n, "sample_rows_per_step": m, "aggs": [list(map(str, a)) for a in w.aggs]},
+        "config": {"workload": name, "rows": total_rows, "sample_rows_per_step": m,
+                   "aggs": [list(map(str, a)) for a in aggs]},
         "cpu_baseline": {"value": round(value, 6), "unit": "G rows/s", "cores": cores, "kind": "port",
-                         "sample": f"first {m} rows of the workload per step (partitioned hash aggregation, "
-                                   f"{cores} threads); the reference itself has no CPU aggregation path"},
+                         "sample": f"{what} (partitioned hash aggregation, {cores} threads); the reference "
+                                   f"itself has no CPU aggregation path"},
         "e2e": {"value": round(value, 6), "unit": "G rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -150,7 +187,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="skewed", choices=["skewed", "small", "highcard"])
+    ap.add_argument("--workload", default="batch", choices=["batch", "skewed", "small", "highcard"])
     ap.add_argument("--sizing", default="learned", choices=["plain", "learned"])
     ap.add_argument("--no-plain-compare", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -174,6 +211,8 @@ def main():
 
     from cpu_gpu_coprocess_groupby_agg_b200 import Context, gen_device, make_knobs
     from cpu_gpu_coprocess_groupby_agg_b200 import estimator as E
+    if args.workload == "batch":
+        return run_batch(args, ws, rank, local, pg)
     w = get_workload(args.workload)
     ctx = Context(local)
     if args.sizing == "learned" and not E.load_default(ctx):
@@ -279,6 +318,169 @@ def main():
         pg.barrier()
         pg.destroy_process_group()
     return 0
+
+
+def _knob_overrides(args) -> dict:
+    kn = {}
+    for kv in args.knob:
+        name, val = kv.split("=")
+        kn[name] = float(val) if "." in val else int(val)
+    return kn
+
+
+def run_batch(args, ws, rank, local, pg):
+    """The 256-query mixed batch in one gba_groupby_batch call per step."""
+    import torch
+    from cpu_gpu_coprocess_groupby_agg_b200 import Context, gen_device, make_knobs
+    from cpu_gpu_coprocess_groupby_agg_b200 import estimator as E
+    from cpu_gpu_coprocess_groupby_agg_b200 import workloads as W
+    allq = W.batch_queries()
+    ctx = Context(local)
+    if args.sizing == "learned" and not E.load_default(ctx):
+        raise SystemExit(f"learned sizing needs trained weights at {E.WEIGHTS}")
+    dq = []
+    for q in allq:
+        k, c = gen_device(q.spec, q.n, device=local)
+        dq.append((k, c, q.aggs))
+    torch.cuda.synchronize()
+    total_rows = sum(q.n for q in allq)
+    in_bytes = sum(q.n * q.row_bytes() for q in allq)
+    outs = ctx.batch_outputs(dq)
+    stream = torch.cuda.current_stream()
+    base = {"timing": 1}
+    base.update(_knob_overrides(args))
+
+    def timed(sizing, steps, clocks=False):
+        knobs = make_knobs(**dict(base, sizing=sizing))
+        for _ in range(args.warmup):
+            res = ctx.groupby_batch(dq, knobs=knobs, outs=outs, stream=stream)
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        main_ms, main_bytes, launches = 0.0, 0, 0
+        with ClockSampler(local) as clk:
+            e0.record(stream)
+            for _ in range(steps):
+                res = ctx.groupby_batch(dq, knobs=knobs, outs=outs, stream=stream)
+                st = res[0].stats
+                main_ms += st["kernel_ms"][1]
+                main_bytes += st["main_bytes"]
+                launches += st["kernel_launches"]
+            e1.record(stream)
+            torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        el = e0.elapsed_time(e1)
+        if pg:
+            t = torch.tensor([el], device="cuda")
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            el = float(t.item())
+        return el / steps, main_ms / steps, main_bytes / steps, launches, res, clk.summary()
+
+    ms_step, main_ms, main_bytes, launches, res, clocks = timed(args.sizing, args.steps)
+    value = ws * total_rows / (ms_step / 1e3) / 1e9
+    st = res[0].stats
+    groups = sum(r.n_groups for r in res)
+    peak, peak_kind = peaks()
+    achieved = main_bytes / (main_ms / 1e3) / 1e9 if main_ms > 0 else None
+    traffic = None
+    tfile = ROOT / "profiles" / "traffic.json"
+    if tfile.exists():
+        traffic = json.loads(tfile.read_text()).get(f"{BATCH_NAME}:k_batch_preagg")
+    line = {
+        "metric": "groupby_rows_per_s", "value": round(value, 4), "unit": "G rows/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "data": "synthetic (seeded PCG32 generator, generated on device)",
+        "config": {"workload": BATCH_NAME, "queries": len(allq), "rows": total_rows, "input_bytes": in_bytes,
+                   "groups": groups, "aggs": ["sum(0)", "count(*)"], "sizing": args.sizing,
+                   "strategy_mix": st["strategy"], "table_slots_total": st["table_slots"],
+                   "predicted_groups_total": round(st["predicted_groups"], 1),
+                   "l2": "inputs larger than L2 (no flush needed)", "parallelism": f"replicas x{ws}",
+                   "launch": "one gba_groupby_batch call per step (CUDA graph replay)"},
+        "whole_step_hbm_gbs": round(in_bytes / (ms_step / 1e3) / 1e9, 1),
+        "roofline": {"bound": "hbm", "kernel": "k_batch_preagg (+ k_part_agg of partition-strategy queries)",
+                     "achieved": round(achieved, 1) if achieved else None, "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4) if achieved else None, "peak_kind": peak_kind,
+                     "traffic": traffic, "alg_bytes_per_step": int(main_bytes), "launch_ms": round(main_ms, 4)},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if args.sizing == "learned" and not args.no_plain_compare:
+        pms, pmain, pbytes, _, pres, _ = timed("plain", max(3, min(args.steps, 5)))
+        line["plain_sizing"] = {"value": round(ws * total_rows / (pms / 1e3) / 1e9, 4), "unit": "G rows/s",
+                                "ms_per_step": round(pms, 4), "strategy_mix": pres[0].stats["strategy"],
+                                "table_slots_total": pres[0].stats["table_slots"],
+                                "learned_speedup": round(pms / ms_step, 3)}
+    if not args.no_e2e and rank == 0:
+        line["e2e"] = batch_e2e(ctx, allq, dq, outs, make_knobs(**dict(base, sizing=args.sizing)), args)
+    if not args.no_cpu_baseline and rank == 0 and ws == 1:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import cpu_oracle as O
+        sample, m = batch_cpu_sample(allq)
+        host = [(dq[i][0].cpu().numpy(), [c.cpu().numpy() for c in dq[i][1]]) for i in range(len(sample))]
+        cores = os.cpu_count() or 1
+        for (k, c), q in zip(host, sample):
+            O.groupby(k, c, q.aggs, nthreads=cores, sort=False)
+        t0 = time.perf_counter()
+        for (k, c), q in zip(host, sample):
+            O.groupby(k, c, q.aggs, nthreads=cores, sort=False)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": round(m / dt / 1e9, 6), "unit": "G rows/s", "cores": cores, "kind": "port",
+                                "sample": f"the first {len(sample)} of the 256 queries ({m} rows), partitioned "
+                                          f"hash aggregation on {cores} threads"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    del outs, dq
+    ctx.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+def batch_e2e(ctx, allq, dq, outs, knobs, args):
+    """The batch through the public API with host buffers: every step copies
+    each query's pinned host columns to the device, runs the batch, and copies
+    every query's groups back to pinned host memory."""
+    import torch
+    stream = torch.cuda.current_stream()
+    hin = [(k.cpu().pin_memory(), [c.cpu().pin_memory() for c in cs]) for k, cs, _ in dq]
+    first = ctx.groupby_batch(dq, knobs=knobs, outs=outs, stream=stream)
+    hout = [(torch.empty(r.n_groups + 1, dtype=ok.dtype).pin_memory(),
+             [torch.empty(r.n_groups + 1, dtype=a.dtype).pin_memory() for a in oa])
+            for r, (ok, oa) in zip(first, outs)]
+    h2d = sum(k.numel() * k.element_size() + sum(c.numel() * c.element_size() for c in cs) for k, cs in hin)
+
+    def step():
+        for (hk, hc), (k, cs, _) in zip(hin, dq):
+            k.copy_(hk, non_blocking=True)
+            for a, b in zip(cs, hc):
+                a.copy_(b, non_blocking=True)
+        res = ctx.groupby_batch(dq, knobs=knobs, outs=outs, stream=stream)
+        d2h = 0
+        for r, (ok, oa) in zip(res, hout):
+            g = r.n_groups
+            ok[:g].copy_(r.keys, non_blocking=True)
+            d2h += g * r.keys.element_size()
+            for a, b in zip(oa, r.aggs):
+                a[:g].copy_(b, non_blocking=True)
+                d2h += g * 8
+        torch.cuda.synchronize()
+        return d2h
+
+    for _ in range(2):
+        step()
+    steps = max(3, min(args.steps, 5))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        d2h = step()
+    dt = (time.perf_counter() - t0) / steps
+    total = sum(q.n for q in allq)
+    return {"value": round(total / dt / 1e9, 4), "unit": "G rows/s", "ms_per_step": round(dt * 1e3, 3),
+            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "pinned": True,
+            "timer": "host wall clock around the step (copies in, batch call, copies out, sync)"}
 
 
 def e2e(ctx, w, keys, cols, knobs, args, ws):

@@ -74,6 +74,8 @@ class Knobs(C.Structure):
         ("smem_probe_cap", C.c_int32),
         ("max_regrow", C.c_int32),
         ("timing", C.c_int32),
+        ("use_graph", C.c_int32),
+        ("item_rows", C.c_int32),
     ]
 
 
@@ -88,6 +90,8 @@ class Stats(C.Structure):
         ("n_groups", C.c_int64),
         ("kernel_launches", C.c_int32),
         ("kernel_ms", C.c_double * 4),
+        ("main_rows", C.c_int64),
+        ("main_bytes", C.c_int64),
     ]
 
 

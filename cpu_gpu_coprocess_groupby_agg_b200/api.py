@@ -149,6 +149,64 @@ class Context:
         g = ng.value
         return Result(okeys[:g], [t[:g] for t in oaggs], g, self.stats())
 
+    def batch_outputs(self, queries: Sequence, capacity: Sequence[int] | None = None) -> list:
+        """Device output buffers (keys, aggs) for each query of a batch; reusable
+        across calls with the same shapes."""
+        import torch
+        outs = []
+        for i, q in enumerate(queries):
+            keys, cols, aggs = q[0], q[1], q[2]
+            aggs_p = parse_aggs(aggs)
+            uc = list(q[4]) if len(q) > 4 else []
+            uc += [False] * (len(cols) - len(uc))
+            ctypes_ = [_torch_type(c, u) for c, u in zip(cols, uc)]
+            cap = capacity[i] if capacity is not None else max(keys.numel(), 1) + 1
+            okeys = torch.empty(cap, dtype=keys.dtype, device=keys.device)
+            oaggs = [torch.empty(cap, dtype=torch.float64 if agg_is_fp(op, ctypes_[col] if op != A.COUNT else 0)
+                                 else torch.int64, device=keys.device) for op, col in aggs_p]
+            outs.append((okeys, oaggs))
+        return outs
+
+    def groupby_batch(self, queries: Sequence, knobs=None, stream=None, outs=None) -> list:
+        """Many independent queries in one call (gba_groupby_batch).
+
+        queries: sequence of (keys, cols, aggs[, unsigned_keys[, unsigned_cols]])
+        with device tensors; outs: batch_outputs() buffers (allocated when None).
+        Returns one Result per query (views into the output buffers)."""
+        import torch
+        nq = len(queries)
+        if outs is None:
+            outs = self.batch_outputs(queries)
+        qarr = (A.Query * max(nq, 1))()
+        oarr = (A.Output * max(nq, 1))()
+        for i, q in enumerate(queries):
+            keys, cols, aggs = q[0], q[1], q[2]
+            uk = bool(q[3]) if len(q) > 3 else False
+            uc = list(q[4]) if len(q) > 4 else []
+            uc += [False] * (len(cols) - len(uc))
+            if not keys.is_cuda:
+                raise ValueError("groupby_batch() takes device tensors")
+            col_specs = [(c.data_ptr(), _torch_type(c, u)) for c, u in zip(cols, uc)]
+            qarr[i] = build_query(keys.numel(), keys.data_ptr(), _torch_type(keys, uk), col_specs, parse_aggs(aggs))
+            okeys, oaggs = outs[i]
+            oarr[i].keys = okeys.data_ptr()
+            for a, t in enumerate(oaggs):
+                oarr[i].aggs[a] = t.data_ptr()
+            oarr[i].capacity = okeys.numel()
+        kn = knobs if isinstance(knobs, A.Knobs) else make_knobs(**(knobs or {}))
+        ng = (C.c_int64 * max(nq, 1))()
+        dev = queries[0][0].device if nq else torch.device("cuda", 0)
+        s = stream if stream is not None else torch.cuda.current_stream(dev)
+        A.check(self._lib.gba_groupby_batch(self._h, nq, qarr, oarr, C.byref(kn), C.c_void_p(s.cuda_stream), ng),
+                self._h)
+        st = self.stats()
+        res = []
+        for i in range(nq):
+            g = ng[i]
+            okeys, oaggs = outs[i]
+            res.append(Result(okeys[:g], [t[:g] for t in oaggs], g, st))
+        return res
+
     # ---- learned cardinality estimator ---------------------------------------
     def est_param_count(self) -> int:
         return int(self._lib.gba_estimator_param_count())

@@ -21,6 +21,7 @@ struct EstQuery {
 
 void gba_est_plan(EstQuery* e, int64_t n, int64_t tile_rows);
 int64_t gba_est_nparam();
+cudaError_t gba_launch_est_init(const EstQuery* d_qs, int nq, cudaStream_t s);
 cudaError_t gba_launch_est_sample(const EstQuery* d_qs, int nq, int64_t max_items, cudaStream_t s);
 cudaError_t gba_launch_est_reduce(const EstQuery* d_qs, int nq, cudaStream_t s);
 cudaError_t gba_launch_mlp_forward(const float* W, const float* X, int n, float* out, cudaStream_t s);

@@ -30,6 +30,7 @@ extern "C" void gba_default_knobs(gba_knobs* k) {
   k->use_tma = -1;
   k->coalesce = -1;
   k->max_regrow = 4;
+  k->use_graph = -1;
 }
 
 extern "C" const char* gba_status_string(gba_status s) {
@@ -87,6 +88,9 @@ extern "C" gba_status gba_destroy(gba_context* ctx) {
   for (auto& e : ctx->tev)
     if (e) cudaEventDestroy(e);
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+  if (ctx->batch_exec) cudaGraphExecDestroy(ctx->batch_exec);
+  if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
+  if (ctx->h_batch) cudaFreeHost(ctx->h_batch);
   delete ctx;
   return GBA_OK;
 }
@@ -153,6 +157,17 @@ gba_status gba_est_reserve(gba_context* ctx, size_t bytes, cudaStream_t s) {
   const size_t want = gba_round_up(std::max(bytes, size_t(1) << 22), size_t(1) << 21);
   GBA_CUDA_TRY(ctx, cudaMalloc(&ctx->est_ws, want));
   ctx->est_ws_bytes = want;
+  return GBA_OK;
+}
+
+gba_status gba_batch_host_reserve(gba_context* ctx, size_t bytes) {
+  if (bytes <= ctx->h_batch_bytes) return GBA_OK;
+  if (ctx->h_batch) cudaFreeHost(ctx->h_batch);
+  ctx->h_batch = nullptr;
+  ctx->h_batch_bytes = 0;
+  const size_t want = gba_round_up(std::max(bytes, size_t(1) << 20), size_t(1) << 16);
+  GBA_CUDA_TRY(ctx, cudaMallocHost(&ctx->h_batch, want));
+  ctx->h_batch_bytes = want;
   return GBA_OK;
 }
 
@@ -408,6 +423,8 @@ static gba_status run_table_once(gba_context* ctx, const QDesc& q, const gba_out
     GBA_CUDA_TRY(ctx, gba_launch_preagg(q, t, c, d_flags, s));
     tm.end();
     ++launches;
+    ctx->stats.main_rows += q.n;
+    ctx->stats.main_bytes += q.n * int64_t(gba_row_bytes(q));
   }
   OutDesc o;
   o.keys = out->keys;

@@ -1,0 +1,416 @@
+// gba_groupby_batch: many independent device queries in a few launches.
+//
+// Every query is planned as gba_groupby would plan it (learned sizing runs the
+// estimator once for the whole batch).  Queries on the table strategy share
+// one launch sequence:
+//   k_batch_init      every query's HBM table (blocks dealt by table size)
+//   k_batch_preagg    one persistent launch per aggregate signature; CTAs pop
+//                     (query, row range) items from a device work queue,
+//                     longest first
+//   k_batch_compact   every query's groups into its own output
+// replayed from a CUDA graph while the batch's launch shapes repeat (the
+// per-query descriptors are copied from pinned host memory by the graph's
+// first node, so new queries of the same shapes reuse it).  Queries on the
+// partition strategy run one after another behind it.  A query whose table
+// overflowed is rerun alone with a larger table.
+//
+// No counterpart in the reference: its host loop runs one query, one tile per
+// stream at a time (group_then_partition.cu:332-424).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "batch_kernels.h"
+#include "est_kernels.h"
+#include "gba_context.h"
+#include "gba_plan.h"
+
+namespace {
+
+struct QInfo {
+  QDesc q;
+  GbaPlan p;
+  double pred = -1;
+  int strategy = GBA_STRATEGY_TABLE;
+  int S = 0;         // shared-table slots in the batch kernel
+  int slot = -1;     // index among the table-strategy queries
+};
+
+struct Group {
+  int sig;
+  QDesc proto;
+  std::vector<int> members;  // indices into the batch's queries
+  size_t smem = 0;           // dynamic shared memory of the group's launch
+  int64_t item_begin = 0, nitems = 0;
+  int grid = 0;
+};
+
+size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// Estimator predictions for every query of the batch: one sampling pass, one
+// MLP launch, one copy back.
+gba_status batch_predict(gba_context* ctx, const std::vector<QDesc>& qs, cudaStream_t s, std::vector<double>* pred,
+                         std::vector<double>* skew) {
+  const int n = int(qs.size());
+  float* f;
+  unsigned long long* stats;
+  gba_status st = gba_est_features_device(ctx, qs.data(), n, 0, s, &f, &stats);
+  if (st != GBA_OK) return st;
+  const size_t y_off = 4096, s_off = round_up(y_off + 4 * size_t(n), 256);
+  st = gba_small_reserve(ctx, std::max<size_t>(ctx->d_small_bytes, s_off + 32 * size_t(n)));
+  if (st != GBA_OK) return st;
+  float* y = reinterpret_cast<float*>(ctx->d_small + y_off);
+  GBA_CUDA_TRY(ctx, gba_launch_mlp_forward(ctx->d_est, f, n, y, s));
+  GBA_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_small + y_off, y, 4 * size_t(n), cudaMemcpyDeviceToHost, s));
+  GBA_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_small + s_off, stats, 32 * size_t(n), cudaMemcpyDeviceToHost, s));
+  GBA_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+  ctx->stats.kernel_launches += 1;
+  const float* yh = reinterpret_cast<const float*>(ctx->h_small + y_off);
+  const unsigned long long* sh = reinterpret_cast<const unsigned long long*>(ctx->h_small + s_off);
+  pred->resize(n);
+  skew->resize(n);
+  for (int i = 0; i < n; ++i) {
+    double g = exp2(double(yh[i]) * 32.0);
+    g = std::max(g, double(sh[4 * i + 0]));
+    g = std::min(g, double(std::max<int64_t>(qs[i].n, 1)));
+    (*pred)[i] = g;
+    (*skew)[i] = double(sh[4 * i + 1]) / double(std::max<unsigned long long>(1, sh[4 * i + 2]));
+  }
+  return GBA_OK;
+}
+
+// Shared-table slots a batch CTA can hold for signature `proto` with tiles of
+// T rows and `bps` CTAs per SM.
+int batch_smem_slots(const gba_context* ctx, const QDesc& proto, int T, int bps) {
+  const size_t budget = size_t(ctx->max_smem_optin) / size_t(bps);
+  const size_t fixed = gba_batch_smem_bytes(proto, 0, T) + gba_batch_static_smem() + 1024;
+  if (budget <= fixed) return 0;
+  const size_t slot = 8 + 8 * size_t(proto.nwords);
+  const int S = int(std::min<size_t>(16384, (budget - fixed) / slot));
+  return S < 32 ? 0 : S;
+}
+
+}  // namespace
+
+extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_query* qs, const gba_output* outs,
+                                        const gba_knobs* knobs, void* stream, int64_t* n_groups) {
+  if (!ctx || nq < 0 || (nq > 0 && (!qs || !outs || !n_groups))) return GBA_ERR_INVALID_ARG;
+  GBA_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  ctx->stats = gba_stats{};
+  ctx->stats.predicted_groups = -1;
+  if (nq == 0) return GBA_OK;
+  gba_knobs k;
+  if (knobs) k = *knobs;
+  else gba_default_knobs(&k);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+
+  // ---- validate and describe every query ----
+  std::vector<QInfo> qi(nq);
+  std::vector<QDesc> qd(nq);
+  for (int i = 0; i < nq; ++i) {
+    gba_query qc;
+    gba_compact_query(&qs[i], &qc);
+    gba_status st = gba_build_qdesc(ctx, &qc, &qd[i]);
+    if (st != GBA_OK) {
+      ctx->err = "query " + std::to_string(i) + ": " + ctx->err;
+      return st;
+    }
+    const gba_output& o = outs[i];
+    bool bad = o.capacity < 0 || (o.capacity > 0 && !o.keys);
+    for (int a = 0; a < qc.n_aggs; ++a) bad = bad || (o.capacity > 0 && !o.aggs[a]);
+    if (bad) {
+      ctx->err = "query " + std::to_string(i) + ": bad output descriptor";
+      return GBA_ERR_INVALID_ARG;
+    }
+    qi[i].q = qd[i];
+    n_groups[i] = 0;
+  }
+
+  // ---- sizing: one estimator pass for the batch ----
+  std::vector<double> pred(nq, -1.0), skew(nq, 0.0);
+  if (k.sizing == GBA_SIZING_LEARNED) {
+    if (!ctx->est_loaded) {
+      ctx->err = "learned sizing requested but no estimator weights are loaded";
+      return GBA_ERR_INVALID_ARG;
+    }
+    gba_status st = batch_predict(ctx, qd, s, &pred, &skew);
+    if (st != GBA_OK) return st;
+    ctx->stats.predicted_groups = std::accumulate(pred.begin(), pred.end(), 0.0);
+  }
+  const int bps = k.blocks_per_sm == 2 ? 2 : 1;
+  const int block = 1024 / bps;
+  int T = k.tile_rows > 0 ? k.tile_rows : 8192;
+  T = std::min(32768, std::max(block, T / block * block));
+  const int sprobe = k.smem_probe_cap > 0 ? k.smem_probe_cap : 8;
+  for (int i = 0; i < nq; ++i) {
+    ctx->est_skew = skew[i];
+    gba_make_plan(ctx, qd[i], k, pred[i], &qi[i].p);
+    qi[i].pred = pred[i];
+    qi[i].strategy = k.strategy != GBA_STRATEGY_AUTO ? k.strategy
+                                                     : gba_choose_strategy(ctx, qd[i], k, pred[i], qi[i].p);
+  }
+
+  // ---- group the table-strategy queries by aggregate signature ----
+  std::vector<Group> groups;
+  std::vector<int> tq;  // table-strategy queries, group by group
+  for (int i = 0; i < nq; ++i) {
+    if (qi[i].strategy != GBA_STRATEGY_TABLE) continue;
+    const int sig = gba_batch_sig_id(qd[i]);
+    auto it = std::find_if(groups.begin(), groups.end(), [&](const Group& g) { return g.sig == sig; });
+    if (it == groups.end()) {
+      groups.push_back(Group{sig, qd[i], {}});
+      it = groups.end() - 1;
+    }
+    it->members.push_back(i);
+  }
+  for (auto& g : groups) {
+    g.smem = gba_batch_smem_bytes(g.proto, 0, T);
+    for (int i : g.members) {
+      // run-time signatures may differ in accumulator words per member
+      int S = qi[i].p.preagg ? batch_smem_slots(ctx, qd[i], T, bps) : 0;
+      if (k.smem_slots > 0) S = std::min(S, k.smem_slots);
+      // a known-small group count needs only a small shared table (cheaper
+      // to clear and flush per work item)
+      if (S > 0 && qi[i].pred > 0) S = std::min<int64_t>(S, std::max<int64_t>(256, int64_t(qi[i].pred * 2.0 + 31) / 32 * 32));
+      qi[i].S = S;
+      g.smem = std::max(g.smem, gba_batch_smem_bytes(qd[i], S, T));
+      qi[i].slot = int(tq.size());
+      tq.push_back(i);
+    }
+  }
+  const int nt = int(tq.size());
+
+  // ---- work items ----
+  int64_t total_rows = 0;
+  for (int i : tq) total_rows += qd[i].n;
+  const int grid_max = ctx->sms * bps;
+  int64_t item_rows = k.item_rows > 0 ? int64_t(k.item_rows)
+                                      : std::min<int64_t>(int64_t(1) << 20,
+                                                          std::max<int64_t>(4 * int64_t(T), total_rows / (4 * grid_max)));
+  item_rows = std::max<int64_t>(T, (item_rows + T - 1) / T * T);
+  std::vector<BatchItem> items;
+  for (auto& g : groups) {
+    g.item_begin = int64_t(items.size());
+    for (int i : g.members)
+      for (int64_t r = 0; r < qd[i].n; r += item_rows)
+        items.push_back(BatchItem{qi[i].slot, 0, r, std::min(qd[i].n, r + item_rows)});
+    g.nitems = int64_t(items.size()) - g.item_begin;
+    std::stable_sort(items.begin() + g.item_begin, items.end(), [](const BatchItem& a, const BatchItem& b) {
+      return a.row_end - a.row_begin > b.row_end - b.row_begin;
+    });
+    g.grid = int(std::max<int64_t>(1, std::min<int64_t>(g.nitems, grid_max)));
+  }
+  const int ng = int(groups.size());
+
+  // ---- device layout: descriptors | items | block prefixes | status | counters | tables ----
+  size_t off = 0;
+  auto take = [&](size_t b) {
+    const size_t o = off;
+    off = round_up(off + b, 256);
+    return o;
+  };
+  const size_t o_q = take(sizeof(BatchQ) * size_t(nt));
+  const size_t o_items = take(sizeof(BatchItem) * items.size());
+  const size_t o_ipre = take(8 * size_t(nt + 1));
+  const size_t o_cpre = take(8 * size_t(nt + 1));
+  const size_t desc_bytes = off;
+  const size_t o_stat = take(16 * size_t(nt) + 4 * size_t(ng));
+  const size_t stat_bytes = 16 * size_t(nt) + 4 * size_t(ng);
+  std::vector<size_t> o_tab(nt);
+  std::vector<int64_t> ipre(nt + 1, 0), cpre(nt + 1, 0);
+  for (int j = 0; j < nt; ++j) {
+    const QInfo& x = qi[tq[j]];
+    const size_t words = (x.p.table_slots + 1) * (1 + size_t(x.q.naccs));
+    o_tab[j] = take(words * 8);
+    ipre[j + 1] = ipre[j] + int64_t(std::max<size_t>(1, (words + 256 * 16 - 1) / (256 * 16)));
+    cpre[j + 1] = cpre[j] + int64_t(std::max<uint64_t>(1, (x.p.table_slots + 2047) / 2048));
+  }
+  if (nt > 0) {
+    gba_status st = gba_ws_reserve(ctx, off, s);
+    if (st != GBA_OK) return st;
+    st = gba_batch_host_reserve(ctx, desc_bytes + stat_bytes + 256);
+    if (st != GBA_OK) return st;
+  }
+  unsigned char* d = static_cast<unsigned char*>(ctx->ws);
+  unsigned char* h = ctx->h_batch;
+  const size_t h_stat = round_up(desc_bytes, 256);
+  if (nt > 0) {
+    BatchQ* hq = reinterpret_cast<BatchQ*>(h + o_q);
+    for (int j = 0; j < nt; ++j) {
+      const int i = tq[j];
+      BatchQ b;
+      std::memset(&b, 0, sizeof(b));
+      b.q = qd[i];
+      b.gt.base = reinterpret_cast<unsigned long long*>(d + o_tab[j]);
+      b.gt.cap = qi[i].p.table_slots;
+      b.gt.probe_cap = qi[i].p.probe_cap;
+      b.out.keys = outs[i].keys;
+      for (int a = 0; a < GBA_MAX_AGGS; ++a) b.out.accs[a] = static_cast<unsigned long long*>(outs[i].aggs[a]);
+      b.out.capacity = outs[i].capacity;
+      b.out.count = reinterpret_cast<unsigned long long*>(d + o_stat + 16 * size_t(j) + 8);
+      b.flags = reinterpret_cast<unsigned*>(d + o_stat + 16 * size_t(j));
+      b.S = qi[i].S;
+      hq[j] = b;
+    }
+    if (!items.empty()) std::memcpy(h + o_items, items.data(), sizeof(BatchItem) * items.size());
+    std::memcpy(h + o_ipre, ipre.data(), 8 * size_t(nt + 1));
+    std::memcpy(h + o_cpre, cpre.data(), 8 * size_t(nt + 1));
+  }
+
+  // ---- the launch sequence (direct or as a replayed graph) ----
+  const BatchQ* d_qs = reinterpret_cast<const BatchQ*>(d + o_q);
+  const BatchItem* d_items = reinterpret_cast<const BatchItem*>(d + o_items);
+  unsigned* d_ctr = reinterpret_cast<unsigned*>(d + o_stat + 16 * size_t(nt));
+  // with timing on, events around the three kernel roles (recorded as graph
+  // nodes when captured): [0] table init, [1] pre-aggregation, [2] compaction
+  const bool timing = k.timing != 0;
+  auto mark = [&](int i, cudaStream_t cs) -> cudaError_t {
+    return timing ? cudaEventRecordWithFlags(ctx->tev[i], cs, cudaEventRecordExternal) : cudaSuccess;
+  };
+  auto enqueue = [&](cudaStream_t cs) -> cudaError_t {
+    cudaError_t e = cudaMemcpyAsync(d, h, desc_bytes, cudaMemcpyHostToDevice, cs);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d + o_stat, 0, stat_bytes, cs);
+    if (e == cudaSuccess) e = mark(0, cs);
+    if (e == cudaSuccess)
+      e = gba_launch_batch_init(d_qs, reinterpret_cast<const int64_t*>(d + o_ipre), nt, ipre[nt], cs);
+    if (e == cudaSuccess) e = mark(1, cs);
+    for (int g = 0; g < ng && e == cudaSuccess; ++g)
+      e = gba_launch_batch_preagg(groups[g].proto, d_qs, d_items + groups[g].item_begin, int(groups[g].nitems),
+                                  d_ctr + g, groups[g].smem, sprobe, T, groups[g].grid, block, cs);
+    if (e == cudaSuccess) e = mark(2, cs);
+    if (e == cudaSuccess)
+      e = gba_launch_batch_compact(d_qs, reinterpret_cast<const int64_t*>(d + o_cpre), nt, cpre[nt], cs);
+    if (e == cudaSuccess) e = mark(3, cs);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h + h_stat, d + o_stat, stat_bytes, cudaMemcpyDeviceToHost, cs);
+    return e;
+  };
+  if (nt > 0) {
+    for (int g = 0; g < ng; ++g)
+      GBA_CUDA_TRY(ctx, gba_prepare_batch_preagg(groups[g].proto, groups[g].smem));
+    if (k.use_graph != 0) {
+      // the graph depends only on launch shapes and buffer addresses
+      std::vector<int64_t> key = {nt,
+                                  int64_t(items.size()),
+                                  ipre[nt],
+                                  cpre[nt],
+                                  int64_t(desc_bytes),
+                                  int64_t(stat_bytes),
+                                  int64_t(reinterpret_cast<uintptr_t>(d)),
+                                  int64_t(reinterpret_cast<uintptr_t>(h)),
+                                  T,
+                                  sprobe,
+                                  block,
+                                  timing ? 1 : 0};
+      for (const auto& g : groups) {
+        key.push_back(g.sig);
+        key.push_back(int64_t(g.smem));
+        key.push_back(g.item_begin);
+        key.push_back(g.nitems);
+        key.push_back(g.grid);
+      }
+      if (!ctx->batch_exec || key != ctx->batch_key) {
+        if (ctx->batch_exec) {
+          cudaGraphExecDestroy(ctx->batch_exec);
+          ctx->batch_exec = nullptr;
+        }
+        if (!ctx->cap_stream) GBA_CUDA_TRY(ctx, cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
+        GBA_CUDA_TRY(ctx, cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal));
+        const cudaError_t e = enqueue(ctx->cap_stream);
+        cudaGraph_t graph = nullptr;
+        const cudaError_t e2 = cudaStreamEndCapture(ctx->cap_stream, &graph);
+        GBA_CUDA_TRY(ctx, e);
+        GBA_CUDA_TRY(ctx, e2);
+        const cudaError_t e3 = cudaGraphInstantiate(&ctx->batch_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        GBA_CUDA_TRY(ctx, e3);
+        ctx->batch_key = key;
+      }
+      GBA_CUDA_TRY(ctx, cudaGraphLaunch(ctx->batch_exec, s));
+    } else {
+      GBA_CUDA_TRY(ctx, enqueue(s));
+    }
+    GBA_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    for (int r = 0; timing && r < 3; ++r) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, ctx->tev[r], ctx->tev[r + 1]) == cudaSuccess) ctx->stats.kernel_ms[r] += ms;
+    }
+    ctx->stats.kernel_launches += 2 + ng;
+    for (int i : tq) {
+      ctx->stats.main_rows += qd[i].n;
+      ctx->stats.main_bytes += qd[i].n * int64_t(gba_row_bytes(qd[i]));
+    }
+  }
+
+  // ---- results; reruns of overflowed queries; partition-strategy queries ----
+  gba_status result = GBA_OK;
+  gba_stats acc = ctx->stats;
+  std::vector<int> rerun;
+  for (int j = 0; j < nt; ++j) {
+    const int i = tq[j];
+    const unsigned flags = *reinterpret_cast<const unsigned*>(h + h_stat + 16 * size_t(j));
+    const unsigned long long cnt = *reinterpret_cast<const unsigned long long*>(h + h_stat + 16 * size_t(j) + 8);
+    acc.table_slots += int64_t(qi[i].p.table_slots);
+    if (flags & GBA_FLAG_WAIT_TIMEOUT) {
+      ctx->err = "query " + std::to_string(i) + ": a bounded device wait timed out";
+      return GBA_ERR_TIMEOUT;
+    }
+    if (flags & GBA_FLAG_TABLE_OVERFLOW) {
+      rerun.push_back(i);
+      continue;
+    }
+    n_groups[i] = int64_t(cnt);
+    if (int64_t(cnt) > outs[i].capacity && result == GBA_OK) {
+      ctx->err = "query " + std::to_string(i) + ": output capacity " + std::to_string(outs[i].capacity) + " < " +
+                 std::to_string(cnt) + " groups";
+      result = GBA_ERR_OUTPUT_CAPACITY;
+    }
+  }
+  auto run_alone = [&](int i) -> gba_status {
+    GbaPlan p = qi[i].p;
+    gba_status st;
+    if (qi[i].strategy == GBA_STRATEGY_TABLE) {
+      p.table_slots *= 4;
+      acc.regrows++;
+      st = gba_run_table(ctx, qd[i], &outs[i], k, p, s, &n_groups[i]);
+    } else {
+      st = gba_run_partition(ctx, qd[i], &outs[i], k, p, qi[i].pred, s, &n_groups[i]);
+    }
+    acc.regrows += ctx->stats.regrows;
+    acc.kernel_launches += ctx->stats.kernel_launches;
+    acc.main_rows += ctx->stats.main_rows;
+    acc.main_bytes += ctx->stats.main_bytes;
+    for (int r = 0; r < 4; ++r) acc.kernel_ms[r] += ctx->stats.kernel_ms[r];
+    acc.partition_bits = std::max(acc.partition_bits, ctx->stats.partition_bits);
+    ctx->stats = gba_stats{};
+    return st;
+  };
+  for (int i : rerun) {
+    ctx->stats = gba_stats{};
+    const gba_status st = run_alone(i);
+    if (st != GBA_OK) {
+      ctx->stats = acc;
+      ctx->err = "query " + std::to_string(i) + ": " + ctx->err;
+      return st;
+    }
+  }
+  for (int i = 0; i < nq; ++i) {
+    if (qi[i].strategy == GBA_STRATEGY_TABLE) continue;
+    ctx->stats = gba_stats{};
+    const gba_status st = run_alone(i);
+    if (st != GBA_OK) {
+      ctx->stats = acc;
+      ctx->err = "query " + std::to_string(i) + ": " + ctx->err;
+      return st;
+    }
+  }
+  acc.strategy = nt == nq ? GBA_STRATEGY_TABLE : (nt == 0 ? GBA_STRATEGY_PARTITION : GBA_STRATEGY_AUTO);
+  acc.preagg = 0;
+  for (int j = 0; j < nt; ++j) acc.preagg += qi[tq[j]].S > 0;
+  acc.n_groups = 0;
+  for (int i = 0; i < nq; ++i) acc.n_groups += n_groups[i];
+  ctx->stats = acc;
+  return result;
+}

@@ -35,6 +35,13 @@ struct gba_context {
   size_t est_ws_bytes = 0;
   // share of the last estimator sample taken by its most frequent key
   double est_skew = 0.0;
+  // batch path: pinned descriptor/status staging, capture stream, and the
+  // instantiated graph of the last batch shape with its key
+  unsigned char* h_batch = nullptr;
+  size_t h_batch_bytes = 0;
+  cudaStream_t cap_stream = nullptr;
+  cudaGraphExec_t batch_exec = nullptr;
+  std::vector<int64_t> batch_key;
   std::string err;
   gba_stats stats{};
 };
@@ -64,6 +71,7 @@ struct GbaTimer {
 
 gba_status gba_ws_reserve(gba_context* ctx, size_t bytes, cudaStream_t s);
 gba_status gba_small_reserve(gba_context* ctx, size_t bytes);
+gba_status gba_batch_host_reserve(gba_context* ctx, size_t bytes);
 gba_status gba_est_reserve(gba_context* ctx, size_t bytes, cudaStream_t s);
 // estimator features of nq device queries into ctx->est_ws (device pointers)
 gba_status gba_est_features_device(gba_context* ctx, const QDesc* qs, int nq, int64_t tile_rows, cudaStream_t s,

@@ -157,6 +157,8 @@ extern "C" gba_status gba_groupby_host(gba_context* ctx, const gba_query* q, con
       c.coalesce = cp.coalesce;
       GBA_CUDA_TRY(ctx, gba_launch_preagg(cq, t, c, d_flags, s));
       ++launches;
+      ctx->stats.main_rows += cq.n;
+      ctx->stats.main_bytes += cq.n * int64_t(gba_row_bytes(cq));
     }
     OutDesc o;
     o.keys = dout.keys;

@@ -105,7 +105,14 @@ gba_status gba_run_partition(gba_context* ctx, const QDesc& q, const gba_output*
     const size_t o_cbase = cv.take(8 * size_t(max_nseg_in));
     const size_t o_snch = cv.take(4 * size_t(max_nseg_in));
     const size_t o_segs = cv.take(8 * size_t(nseg_final + 1) * 2);
-    const size_t o_fb = cv.take((fb_cap + 1) * (1 + size_t(q.naccs)) * 8);
+    // final work items: whole partitions packed up to Lp rows, partitions of
+    // more than 2 Lp rows (hot keys) split into pieces of Lp rows
+    const int64_t Lp = std::max<int64_t>(32768, n / (int64_t(ctx->sms) * 4));
+    const int64_t max_split = n / (2 * Lp) + 1;
+    const size_t o_work = cv.take(sizeof(PartWork) * size_t(nseg_final + n / Lp + 2));
+    // the fallback table goes last: its final size is known after partitioning
+    const size_t fb_slot_bytes = (1 + size_t(q.naccs)) * 8;
+    const size_t o_fb = cv.take((fb_cap + 1 + uint64_t(max_split) * uint64_t(S) * 2) * fb_slot_bytes);
     gba_status st = gba_ws_reserve(ctx, cv.off, s);
     if (st != GBA_OK) return st;
     unsigned char* W = static_cast<unsigned char*>(ctx->ws);
@@ -190,16 +197,44 @@ gba_status gba_run_partition(gba_context* ctx, const QDesc& q, const gba_output*
       }
     }
 
+    // plan the final work items from the partition bounds
+    std::vector<long long> sb(size_t(nseg_final) + 1);
+    GBA_CUDA_TRY(ctx, cudaMemcpyAsync(sb.data(), d_seg, 8 * sb.size(), cudaMemcpyDeviceToHost, s));
+    GBA_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    std::vector<PartWork> work;
+    int64_t nsplit = 0;
+    for (int64_t sg = 0; sg < nseg_final;) {
+      const int64_t rows = sb[sg + 1] - sb[sg];
+      if (rows > 2 * Lp) {
+        ++nsplit;
+        for (int64_t r = sb[sg]; r < sb[sg + 1]; r += Lp)
+          work.push_back(PartWork{int(sg), int(sg) + 1, 1, 0, r, std::min<int64_t>(sb[sg + 1], r + Lp)});
+        ++sg;
+        continue;
+      }
+      int64_t e = sg + 1;
+      while (e < nseg_final && sb[e + 1] - sb[sg] <= Lp && sb[e + 1] - sb[e] <= 2 * Lp) ++e;
+      work.push_back(PartWork{int(sg), int(e), 0, 0, sb[sg], sb[e]});
+      sg = e;
+    }
+    std::stable_sort(work.begin(), work.end(), [](const PartWork& x, const PartWork& y) {
+      return x.row_end - x.row_begin > y.row_end - y.row_begin;
+    });
+    GBA_CUDA_TRY(ctx, cudaMemcpyAsync(W + o_work, work.data(), sizeof(PartWork) * work.size(),
+                                      cudaMemcpyHostToDevice, s));
+
     // final aggregation over the 2^B partitions, then the fallback table
     GTable fb;
     fb.base = reinterpret_cast<unsigned long long*>(W + o_fb);
-    fb.cap = fb_cap;
+    fb.cap = fb_cap + uint64_t(nsplit) * uint64_t(S) * 2;
     fb.probe_cap = 256;
     GBA_CUDA_TRY(ctx, gba_launch_table_init(fb, q, ctx->sms * 4, s));
     PartAgg pa;
     pa.rows = in;
     pa.seg_begin = d_seg;
     pa.nsegs = int(nseg_final);
+    pa.work = reinterpret_cast<const PartWork*>(W + o_work);
+    pa.nwork = int(work.size());
     pa.seg_ctr = d_seg_ctr;
     pa.S = S;
     pa.sprobe = p.smem_probe_cap > 0 ? std::max(p.smem_probe_cap, 64) : 64;
@@ -211,10 +246,13 @@ gba_status gba_run_partition(gba_context* ctx, const QDesc& q, const gba_output*
     pa.out.capacity = out->capacity;
     pa.out.count = d_count;
     tm.begin(1);
-    GBA_CUDA_TRY(ctx, gba_launch_part_agg(pa, std::min<int>(pa.nsegs, ctx->sms), s));
+    GBA_CUDA_TRY(ctx, gba_launch_part_agg(pa, std::min<int>(pa.nwork, ctx->sms), s));
     tm.end();
+    ctx->stats.main_rows += n;
+    ctx->stats.main_bytes += n * int64_t(rb);
     tm.begin(2);
-    GBA_CUDA_TRY(ctx, gba_launch_compact(fb, q, pa.out, ctx->sms * 2, s));
+    GBA_CUDA_TRY(ctx, gba_launch_compact(
+                          fb, q, pa.out, int(std::max<uint64_t>(1, std::min<uint64_t>(ctx->sms * 8, fb.cap / 256))), s));
     tm.end();
     launches += 3;
     GBA_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_small, ctx->d_small, 16, cudaMemcpyDeviceToHost, s));

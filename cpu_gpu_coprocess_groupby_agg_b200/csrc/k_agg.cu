@@ -165,25 +165,6 @@ __device__ __forceinline__ void tile_two_phase(const QDesc& q, const GTable& gt,
 }
 
 // Merges a CTA's shared table into the HBM table (caller synced first).
-template <bool K64, typename Sig>
-__device__ __forceinline__ void flush_table(const QDesc& q, const GTable& gt, const SmemTable<K64>& st,
-                                            unsigned* flags) {
-  for (int i = threadIdx.x; i < st.S; i += blockDim.x) {
-    const uint64_t k = st.keys[i];
-    if (k == uint64_t(smem_empty_key<K64>())) continue;
-    unsigned long long v[Sig::NA];
-#pragma unroll
-    for (int a = 0; a < Sig::NA; ++a) v[a] = smem_acc_read<K64, Sig>(st, q, a, i);
-    gtable_insert<K64, Sig>(gt, q, k, table_hash(k), v, flags);
-  }
-  if (threadIdx.x == 0 && st.S > 0 && *st.side_present) {
-    unsigned long long v[Sig::NA];
-#pragma unroll
-    for (int a = 0; a < Sig::NA; ++a) v[a] = smem_acc_read<K64, Sig>(st, q, a, -1);
-    gtable_insert<K64, Sig>(gt, q, K64 ? EMPTY64 : uint64_t(EMPTY32), 0u, v, flags);
-  }
-}
-
 // Each tile is processed in two phases.
 //  A: every row probes the CTA's shared table (capped probes) and updates it
 //     with 32-bit atomics; a row whose key is not there and cannot enter only
@@ -310,7 +291,7 @@ __global__ void __launch_bounds__(1024, 1) k_preagg(PreaggParams P) {
   }
 
   __syncthreads();
-  flush_table<K64, Sig>(q, P.gt, st, P.flags);
+  smem_flush_to_gtable<K64, Sig>(q, P.gt, st, P.flags);
 }
 
 __global__ void k_table_init(GTable t, int naccs, QDesc q) {
@@ -395,7 +376,7 @@ __device__ __forceinline__ void batch_item(const BatchQ& bq, const BatchItem& it
     if (threadIdx.x == 0) *s_nmiss = 0;
     __syncthreads();
   }
-  flush_table<K64, Sig>(q, bq.gt, st, bq.flags);
+  smem_flush_to_gtable<K64, Sig>(q, bq.gt, st, bq.flags);
 }
 
 template <typename Sig>
@@ -429,73 +410,89 @@ __global__ void __launch_bounds__(1024, 1) k_batch_preagg(const BatchQ* qs, cons
   }
 }
 
-// table init for every query of a group (blockIdx.y = query)
-__global__ void k_batch_init(const BatchQ* qs, int nq) {
-  for (int qi = blockIdx.y; qi < nq; qi += gridDim.y) {
-    const GTable t = qs[qi].gt;
-    const QDesc& q = qs[qi].q;
-    const int stride = 1 + q.naccs;
-    const uint64_t total = (t.cap + 1) * stride;
-    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < total;
-         i += uint64_t(gridDim.x) * blockDim.x) {
-      const uint64_t slot = i / stride;
-      const int w = int(i - slot * stride);
-      unsigned long long v;
-      if (w == 0) v = slot == t.cap ? 0ull : EMPTY64;
-      else {
-        v = 0ull;
+// table init for every query of a batch: blocks are dealt to queries in
+// proportion to their table sizes (blk_prefix[i] = first block of query i)
+__device__ __forceinline__ int batch_query_of_block(const int64_t* blk_prefix, int nq, int64_t b) {
+  int lo = 0, hi = nq - 1;
+  while (lo < hi) {  // largest i with blk_prefix[i] <= b
+    const int mid = (lo + hi + 1) >> 1;
+    if (blk_prefix[mid] <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(256) k_batch_init(const BatchQ* qs, const int64_t* blk_prefix, int nq) {
+  const int qi = batch_query_of_block(blk_prefix, nq, blockIdx.x);
+  const int64_t b = int64_t(blockIdx.x) - blk_prefix[qi];
+  const int64_t nb = blk_prefix[qi + 1] - blk_prefix[qi];
+  const GTable t = qs[qi].gt;
+  const QDesc& q = qs[qi].q;
+  const int stride = 1 + q.naccs;
+  unsigned long long id[GBA_MAX_AGGS];
 #pragma unroll
-        for (int a = 0; a < GBA_MAX_AGGS; ++a)
-          if (a == w - 1) v = acc_identity(q.acc_op[a]);
-      }
-      t.base[i] = v;
+  for (int a = 0; a < GBA_MAX_AGGS; ++a) id[a] = a < q.naccs ? acc_identity(q.acc_op[a]) : 0ull;
+  const uint64_t total = (t.cap + 1) * stride;
+  for (uint64_t i = uint64_t(b) * blockDim.x + threadIdx.x; i < total; i += uint64_t(nb) * blockDim.x) {
+    const uint64_t slot = i / stride;
+    const int w = int(i - slot * stride);
+    unsigned long long v;
+    if (w == 0) v = slot == t.cap ? 0ull : EMPTY64;
+    else {
+      v = 0ull;
+#pragma unroll
+      for (int a = 0; a < GBA_MAX_AGGS; ++a)
+        if (a == w - 1) v = id[a];
     }
+    t.base[i] = v;
   }
 }
 
-// compaction of every query of a group (blockIdx.y = query)
-__global__ void k_batch_compact(const BatchQ* qs, int nq) {
-  for (int qi = blockIdx.y; qi < nq; qi += gridDim.y) {
-    const GTable t = qs[qi].gt;
-    const QDesc& q = qs[qi].q;
-    const OutDesc o = qs[qi].out;
-    const bool K64 = q.key64 != 0;
-    const int stride = 1 + q.naccs;
-    const unsigned lane = lane_id();
-    const uint64_t warp = (blockIdx.x * uint64_t(blockDim.x) + threadIdx.x) >> 5;
-    const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
-    for (uint64_t base = warp * 32; base < t.cap; base += nwarps * 32) {
-      const uint64_t i = base + lane;
-      unsigned long long k = EMPTY64;
-      if (i < t.cap) k = t.base[i * stride];
-      const bool occ = k != EMPTY64;
-      const unsigned m = __ballot_sync(GBA_FULL_MASK, occ);
-      if (m == 0) continue;
-      unsigned long long pos0 = 0;
-      if (lane == 0) pos0 = atomicAdd(o.count, (unsigned long long)__popc(m));
-      pos0 = __shfl_sync(GBA_FULL_MASK, pos0, 0);
-      if (occ) {
-        const unsigned long long pos = pos0 + __popc(m & ((1u << lane) - 1u));
-        if (pos < (unsigned long long)o.capacity) {
-          if (K64) static_cast<unsigned long long*>(o.keys)[pos] = k;
-          else static_cast<unsigned*>(o.keys)[pos] = unsigned(k);
+// compaction of every query of a batch into its own output (blocks dealt as
+// in k_batch_init; block 0 of a query also emits its all-ones-key side slot)
+__global__ void __launch_bounds__(256) k_batch_compact(const BatchQ* qs, const int64_t* blk_prefix, int nq) {
+  const int qi = batch_query_of_block(blk_prefix, nq, blockIdx.x);
+  const int64_t b = int64_t(blockIdx.x) - blk_prefix[qi];
+  const int64_t nb = blk_prefix[qi + 1] - blk_prefix[qi];
+  const GTable t = qs[qi].gt;
+  const QDesc& q = qs[qi].q;
+  const OutDesc o = qs[qi].out;
+  const bool K64 = q.key64 != 0;
+  const int stride = 1 + q.naccs;
+  const unsigned lane = lane_id();
+  const uint64_t warp = (uint64_t(b) * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = (uint64_t(nb) * blockDim.x) >> 5;
+  for (uint64_t base = warp * 32; base < t.cap; base += nwarps * 32) {
+    const uint64_t i = base + lane;
+    unsigned long long k = EMPTY64;
+    if (i < t.cap) k = t.base[i * stride];
+    const bool occ = k != EMPTY64;
+    const unsigned m = __ballot_sync(GBA_FULL_MASK, occ);
+    if (m == 0) continue;
+    unsigned long long pos0 = 0;
+    if (lane == 0) pos0 = atomicAdd(o.count, (unsigned long long)__popc(m));
+    pos0 = __shfl_sync(GBA_FULL_MASK, pos0, 0);
+    if (occ) {
+      const unsigned long long pos = pos0 + __popc(m & ((1u << lane) - 1u));
+      if (pos < (unsigned long long)o.capacity) {
+        if (K64) static_cast<unsigned long long*>(o.keys)[pos] = k;
+        else static_cast<unsigned*>(o.keys)[pos] = unsigned(k);
 #pragma unroll
-          for (int a = 0; a < GBA_MAX_AGGS; ++a)
-            if (a < q.naccs) o.accs[a][pos] = t.base[i * stride + 1 + a];
-        }
+        for (int a = 0; a < GBA_MAX_AGGS; ++a)
+          if (a < q.naccs) o.accs[a][pos] = t.base[i * stride + 1 + a];
       }
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-      const unsigned long long* side = t.base + t.cap * stride;
-      if (side[0] != 0ull) {
-        const unsigned long long pos = atomicAdd(o.count, 1ull);
-        if (pos < (unsigned long long)o.capacity) {
-          if (K64) static_cast<unsigned long long*>(o.keys)[pos] = EMPTY64;
-          else static_cast<unsigned*>(o.keys)[pos] = EMPTY32;
+  }
+  if (b == 0 && threadIdx.x == 0) {
+    const unsigned long long* side = t.base + t.cap * stride;
+    if (side[0] != 0ull) {
+      const unsigned long long pos = atomicAdd(o.count, 1ull);
+      if (pos < (unsigned long long)o.capacity) {
+        if (K64) static_cast<unsigned long long*>(o.keys)[pos] = EMPTY64;
+        else static_cast<unsigned*>(o.keys)[pos] = EMPTY32;
 #pragma unroll
-          for (int a = 0; a < GBA_MAX_AGGS; ++a)
-            if (a < q.naccs) o.accs[a][pos] = side[1 + a];
-        }
+        for (int a = 0; a < GBA_MAX_AGGS; ++a)
+          if (a < q.naccs) o.accs[a][pos] = side[1 + a];
       }
     }
   }
@@ -554,26 +551,43 @@ size_t gba_batch_smem_bytes(const QDesc& q, int S, int T) {
 }
 size_t gba_batch_static_smem() { return sizeof(BatchQ) + 64; }
 
-cudaError_t gba_launch_batch_preagg(const QDesc& proto, const BatchQ* d_qs, const BatchItem* d_items, int nitems,
-                                    unsigned* item_ctr, int S_max, int sprobe, int T, int grid, cudaStream_t s) {
-  const size_t smem = gba_batch_smem_bytes(proto, S_max, T);
+int gba_batch_sig_id(const QDesc& q) {
+  int id = -1;
+  gba_dispatch_sig(q, [&](auto, auto sig) -> cudaError_t {
+    id = gba_sig_index(decltype(sig){});
+    return cudaSuccess;
+  });
+  return id;
+}
+
+cudaError_t gba_prepare_batch_preagg(const QDesc& proto, size_t smem) {
   return gba_dispatch_sig(proto, [&](auto, auto sig) -> cudaError_t {
     using Sig = decltype(sig);
-    cudaError_t e = cudaFuncSetAttribute(k_batch_preagg<Sig>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e != cudaSuccess) return e;
-    k_batch_preagg<Sig><<<grid, 1024, smem, s>>>(d_qs, d_items, nitems, item_ctr, sprobe, T);
+    return cudaFuncSetAttribute(k_batch_preagg<Sig>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  });
+}
+
+cudaError_t gba_launch_batch_preagg(const QDesc& proto, const BatchQ* d_qs, const BatchItem* d_items, int nitems,
+                                    unsigned* item_ctr, size_t smem, int sprobe, int T, int grid, int block,
+                                    cudaStream_t s) {
+  if (nitems <= 0) return cudaSuccess;
+  return gba_dispatch_sig(proto, [&](auto, auto sig) -> cudaError_t {
+    using Sig = decltype(sig);
+    k_batch_preagg<Sig><<<grid, block, smem, s>>>(d_qs, d_items, nitems, item_ctr, sprobe, T);
     return cudaGetLastError();
   });
 }
 
-cudaError_t gba_launch_batch_init(const BatchQ* d_qs, int nq, int gx, cudaStream_t s) {
-  dim3 g(gx, nq < 65535 ? nq : 65535);
-  k_batch_init<<<g, 256, 0, s>>>(d_qs, nq);
+cudaError_t gba_launch_batch_init(const BatchQ* d_qs, const int64_t* blk_prefix, int nq, int64_t nblocks,
+                                  cudaStream_t s) {
+  if (nq <= 0) return cudaSuccess;
+  k_batch_init<<<unsigned(nblocks), 256, 0, s>>>(d_qs, blk_prefix, nq);
   return cudaGetLastError();
 }
 
-cudaError_t gba_launch_batch_compact(const BatchQ* d_qs, int nq, int gx, cudaStream_t s) {
-  dim3 g(gx, nq < 65535 ? nq : 65535);
-  k_batch_compact<<<g, 256, 0, s>>>(d_qs, nq);
+cudaError_t gba_launch_batch_compact(const BatchQ* d_qs, const int64_t* blk_prefix, int nq, int64_t nblocks,
+                                     cudaStream_t s) {
+  if (nq <= 0) return cudaSuccess;
+  k_batch_compact<<<unsigned(nblocks), 256, 0, s>>>(d_qs, blk_prefix, nq);
   return cudaGetLastError();
 }

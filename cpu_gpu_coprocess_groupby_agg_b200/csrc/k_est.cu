@@ -48,6 +48,18 @@ __device__ __forceinline__ uint64_t sample_row(const EstQuery& e, int64_t item) 
   return uint64_t(tb + j * (len / 1024));
 }
 
+// every query's count table to {empty key, 0} (blockIdx.y = query)
+__global__ void k_est_init(const EstQuery* qs, int nq) {
+  for (int qi = blockIdx.y; qi < nq; qi += gridDim.y) {
+    const EstQuery e = qs[qi];
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < e.cap;
+         i += uint64_t(gridDim.x) * blockDim.x) {
+      e.table[2 * i] = EMPTY64;
+      e.table[2 * i + 1] = 0ull;
+    }
+  }
+}
+
 // one thread per sampled row; per-query count table (keys + counts, linear
 // probing, capacity >= 2x the sample) and 64 HLL registers
 __global__ void k_est_sample(const EstQuery* qs, int nq) {
@@ -314,6 +326,11 @@ cudaError_t gba_launch_est_sample(const EstQuery* d_qs, int nq, int64_t max_item
   k_est_sample<<<grid, 256, 0, s>>>(d_qs, nq);
   return cudaGetLastError();
 }
+cudaError_t gba_launch_est_init(const EstQuery* d_qs, int nq, cudaStream_t s) {
+  if (nq <= 0) return cudaSuccess;
+  k_est_init<<<dim3(64, std::min(nq, 65535)), 256, 0, s>>>(d_qs, nq);
+  return cudaGetLastError();
+}
 cudaError_t gba_launch_est_reduce(const EstQuery* d_qs, int nq, cudaStream_t s) {
   k_est_reduce<<<std::min(nq, 4096), 256, 0, s>>>(d_qs, nq);
   return cudaGetLastError();
@@ -521,18 +538,14 @@ gba_status gba_est_features_device(gba_context* ctx, const QDesc* qs, int nq, in
   }
   GBA_CUDA_TRY(ctx, cudaMemsetAsync(base + o_h, 0, 4 * 64 * size_t(nq), s));
   GBA_CUDA_TRY(ctx, cudaMemsetAsync(base + o_s, 0, 8 * 4 * size_t(nq), s));
-  for (int i = 0; i < nq; ++i) {
-    // key words to the empty marker (all ones), count words to zero
-    GBA_CUDA_TRY(ctx, cudaMemsetAsync(base + o_t[i], 0xff, 16 * eq[i].cap, s));
-    GBA_CUDA_TRY(ctx, cudaMemset2DAsync(base + o_t[i] + 8, 16, 0, 8, eq[i].cap, s));
-  }
   GBA_CUDA_TRY(ctx, cudaMemcpyAsync(base + o_q, eq.data(), sizeof(EstQuery) * nq, cudaMemcpyHostToDevice, s));
   const EstQuery* dq = reinterpret_cast<const EstQuery*>(base + o_q);
+  GBA_CUDA_TRY(ctx, gba_launch_est_init(dq, nq, s));
   GBA_CUDA_TRY(ctx, gba_launch_est_sample(dq, nq, max_items, s));
   GBA_CUDA_TRY(ctx, gba_launch_est_reduce(dq, nq, s));
   *feats_out = reinterpret_cast<float*>(base + o_f);
   *stats_out = reinterpret_cast<unsigned long long*>(base + o_s);
-  ctx->stats.kernel_launches += 2;
+  ctx->stats.kernel_launches += 3;
   return GBA_OK;
 }
 

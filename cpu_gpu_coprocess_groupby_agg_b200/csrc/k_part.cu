@@ -272,105 +272,117 @@ template <bool K64, typename Sig>
 __global__ void __launch_bounds__(1024, 1) k_part_agg(PartAgg a) {
   extern __shared__ __align__(16) unsigned char sm[];
   const QDesc& q = a.rows;
-  __shared__ int s_seg;
+  __shared__ int s_item;
   __shared__ unsigned long long s_base;
   const uint64_t emptyk = K64 ? EMPTY64 : uint64_t(EMPTY32);
   for (;;) {
-    if (threadIdx.x == 0) s_seg = int(atomicAdd(a.seg_ctr, 1u));
+    if (threadIdx.x == 0) s_item = int(atomicAdd(a.seg_ctr, 1u));
     __syncthreads();
-    const int seg = s_seg;
-    if (seg >= a.nsegs) break;
-    const int64_t b = a.seg_begin[seg], e = a.seg_begin[seg + 1];
-    // a partition never holds more groups than rows: size the table to the
-    // rows (load <= 0.7) when that is smaller than the shared budget
-    const int64_t want = (e - b) * 10 / 7 + 32;
-    const SmemTable<K64> st = smem_table_carve<K64>(sm, int(want < a.S ? want : a.S), q.nwords);
-    smem_table_init<K64, Sig>(st, q);
-    __syncthreads();
-    // a partition with many more rows than table slots repeats keys heavily
-    // (skew): pre-combine equal keys inside each warp there
-    const bool coal = a.coalesce || (e - b) > 4 * int64_t(a.S);
-    constexpr int kIlp = 2;  // rows loaded per thread before any is processed (x 1024 threads)
-    for (int64_t r0 = b; r0 < e; r0 += int64_t(kIlp) * blockDim.x) {
-      uint64_t keys[kIlp];
-      unsigned long long raw[kIlp][GBA_MAX_COLS];
+    const int item = s_item;
+    if (item >= a.nwork) break;
+    const PartWork w = a.work[item];
+    for (int seg = w.seg_lo; seg < w.seg_hi; ++seg) {
+      const int64_t b = w.partial ? w.row_begin : a.seg_begin[seg];
+      const int64_t e = w.partial ? w.row_end : a.seg_begin[seg + 1];
+      if (e <= b) continue;  // CTA-uniform
+      // a partition never holds more groups than rows: size the table to the
+      // rows (load <= 0.7) when that is smaller than the shared budget
+      const int64_t want = (e - b) * 10 / 7 + 32;
+      const SmemTable<K64> st = smem_table_carve<K64>(sm, int(want < a.S ? want : a.S), q.nwords);
+      smem_table_init<K64, Sig>(st, q);
+      __syncthreads();
+      // a partition with many more rows than table slots repeats keys heavily
+      // (skew): pre-combine equal keys inside each warp there
+      const bool coal = a.coalesce || (e - b) > 4 * int64_t(a.S);
+      constexpr int kIlp = 2;  // rows loaded per thread before any is processed (x 1024 threads)
+      for (int64_t r0 = b; r0 < e; r0 += int64_t(kIlp) * blockDim.x) {
+        uint64_t keys[kIlp];
+        unsigned long long raw[kIlp][GBA_MAX_COLS];
 #pragma unroll
-      for (int u = 0; u < kIlp; ++u) {
-        const int64_t r = r0 + int64_t(u) * blockDim.x + threadIdx.x;
-        keys[u] = emptyk;
+        for (int u = 0; u < kIlp; ++u) {
+          const int64_t r = r0 + int64_t(u) * blockDim.x + threadIdx.x;
+          keys[u] = emptyk;
 #pragma unroll
-        for (int c = 0; c < GBA_MAX_COLS; ++c) raw[u][c] = 0ull;
-        if (r < e) {
-          keys[u] = K64 ? __ldg(static_cast<const unsigned long long*>(q.keys) + r)
-                        : __ldg(static_cast<const unsigned*>(q.keys) + r);
+          for (int c = 0; c < GBA_MAX_COLS; ++c) raw[u][c] = 0ull;
+          if (r < e) {
+            keys[u] = K64 ? __ldg(static_cast<const unsigned long long*>(q.keys) + r)
+                          : __ldg(static_cast<const unsigned*>(q.keys) + r);
 #pragma unroll
-          for (int c = 0; c < GBA_MAX_COLS; ++c)
-            if (c < Sig::ncols(q))
-              raw[u][c] = col_bytes_t(Sig::coltype(q, c)) == 8
-                              ? __ldg(static_cast<const unsigned long long*>(q.cols[c]) + r)
-                              : __ldg(static_cast<const unsigned*>(q.cols[c]) + r);
+            for (int c = 0; c < GBA_MAX_COLS; ++c)
+              if (c < Sig::ncols(q))
+                raw[u][c] = col_bytes_t(Sig::coltype(q, c)) == 8
+                                ? __ldg(static_cast<const unsigned long long*>(q.cols[c]) + r)
+                                : __ldg(static_cast<const unsigned*>(q.cols[c]) + r);
+          }
         }
-      }
 #pragma unroll
-      for (int u = 0; u < kIlp; ++u) {
-        const int64_t r = r0 + int64_t(u) * blockDim.x + threadIdx.x;
-        const bool valid = r < e;
-        uint64_t key = keys[u];
-        unsigned long long rr[GBA_MAX_COLS];
+        for (int u = 0; u < kIlp; ++u) {
+          const int64_t r = r0 + int64_t(u) * blockDim.x + threadIdx.x;
+          const bool valid = r < e;
+          uint64_t key = keys[u];
+          unsigned long long rr[GBA_MAX_COLS];
 #pragma unroll
-        for (int c = 0; c < GBA_MAX_COLS; ++c) rr[c] = raw[u][c];
-        unsigned long long v[Sig::NA];
-        row_contrib<Sig>(q, rr, v);
-        const bool sent = valid && key == emptyk;
-        if (sent) smem_apply_side<K64, Sig>(st, q, v);
-        bool leader = valid && !sent;
-        if (coal) {  // CTA-uniform, so every lane of the warp is here
-          if (!leader) key = emptyk;
-          leader = warp_coalesce<K64, Sig>(q, leader, key, v);
-        }
-        if (leader) {
-          const uint32_t h = table_hash(key);
-          const int slot = smem_find_or_insert<K64>(st, key, h, a.sprobe);
-          if (slot >= 0) smem_apply<K64, Sig>(st, q, slot, v);
-          else {
-            gtable_insert<K64, Sig>(a.fallback, q, key, h, v, a.flags);
-            atomicOr(a.flags, GBA_FLAG_PART_OVERFLOW);
+          for (int c = 0; c < GBA_MAX_COLS; ++c) rr[c] = raw[u][c];
+          unsigned long long v[Sig::NA];
+          row_contrib<Sig>(q, rr, v);
+          const bool sent = valid && key == emptyk;
+          if (sent) smem_apply_side<K64, Sig>(st, q, v);
+          bool leader = valid && !sent;
+          if (coal) {  // CTA-uniform, so every lane of the warp is here
+            if (!leader) key = emptyk;
+            leader = warp_coalesce<K64, Sig>(q, leader, key, v);
+          }
+          if (leader) {
+            const uint32_t h = table_hash(key);
+            const int slot = smem_find_or_insert<K64>(st, key, h, a.sprobe);
+            if (slot >= 0) smem_apply<K64, Sig>(st, q, slot, v);
+            else {
+              gtable_insert<K64, Sig>(a.fallback, q, key, h, v, a.flags);
+              atomicOr(a.flags, GBA_FLAG_PART_OVERFLOW);
+            }
           }
         }
       }
-    }
-    __syncthreads();
-    // emit the segment's groups: block-wide compaction of occupied slots
-    const int S = st.S;
-    unsigned mine = 0;
-    for (int i = threadIdx.x; i < S; i += blockDim.x) mine += st.keys[i] != smem_empty_key<K64>();
-    unsigned long long tot;
-    unsigned long long before = block_excl_scan(mine, &tot);
-    const bool side = *st.side_present != 0u;
-    if (threadIdx.x == 0) s_base = atomicAdd(a.out.count, tot + (side ? 1ull : 0ull));
-    __syncthreads();
-    unsigned long long pos = s_base + before;
-    for (int i = threadIdx.x; i < S; i += blockDim.x) {
-      const uint64_t k = st.keys[i];
-      if (k == uint64_t(smem_empty_key<K64>())) continue;
-      if (pos < (unsigned long long)a.out.capacity) {
-        if (K64) static_cast<unsigned long long*>(a.out.keys)[pos] = k;
-        else static_cast<unsigned*>(a.out.keys)[pos] = unsigned(k);
-#pragma unroll
-        for (int x = 0; x < Sig::NA; ++x) a.out.accs[x][pos] = smem_acc_read<K64, Sig>(st, q, x, i);
+      __syncthreads();
+      if (w.partial) {
+        // a piece of a split partition: its keys recur in the other pieces, so
+        // its groups are merged in the HBM table and emitted from there
+        smem_flush_to_gtable<K64, Sig>(q, a.fallback, st, a.flags);
+        __syncthreads();
+        continue;
       }
-      ++pos;
-    }
-    if (side && threadIdx.x == 0) {
-      const unsigned long long sp = s_base + tot;
-      if (sp < (unsigned long long)a.out.capacity) {
-        if (K64) static_cast<unsigned long long*>(a.out.keys)[sp] = EMPTY64;
-        else static_cast<unsigned*>(a.out.keys)[sp] = EMPTY32;
+      // emit the segment's groups: block-wide compaction of occupied slots
+      const int S = st.S;
+      unsigned mine = 0;
+      for (int i = threadIdx.x; i < S; i += blockDim.x) mine += st.keys[i] != smem_empty_key<K64>();
+      unsigned long long tot;
+      unsigned long long before = block_excl_scan(mine, &tot);
+      const bool side = *st.side_present != 0u;
+      if (threadIdx.x == 0) s_base = atomicAdd(a.out.count, tot + (side ? 1ull : 0ull));
+      __syncthreads();
+      unsigned long long pos = s_base + before;
+      for (int i = threadIdx.x; i < S; i += blockDim.x) {
+        const uint64_t k = st.keys[i];
+        if (k == uint64_t(smem_empty_key<K64>())) continue;
+        if (pos < (unsigned long long)a.out.capacity) {
+          if (K64) static_cast<unsigned long long*>(a.out.keys)[pos] = k;
+          else static_cast<unsigned*>(a.out.keys)[pos] = unsigned(k);
 #pragma unroll
-        for (int x = 0; x < Sig::NA; ++x) a.out.accs[x][sp] = smem_acc_read<K64, Sig>(st, q, x, -1);
+          for (int x = 0; x < Sig::NA; ++x) a.out.accs[x][pos] = smem_acc_read<K64, Sig>(st, q, x, i);
+        }
+        ++pos;
       }
-    }
-    __syncthreads();
+      if (side && threadIdx.x == 0) {
+        const unsigned long long sp = s_base + tot;
+        if (sp < (unsigned long long)a.out.capacity) {
+          if (K64) static_cast<unsigned long long*>(a.out.keys)[sp] = EMPTY64;
+          else static_cast<unsigned*>(a.out.keys)[sp] = EMPTY32;
+#pragma unroll
+          for (int x = 0; x < Sig::NA; ++x) a.out.accs[x][sp] = smem_acc_read<K64, Sig>(st, q, x, -1);
+        }
+      }
+      __syncthreads();
+    }  // segments of the item
   }
 }
 

@@ -23,16 +23,28 @@ struct PartPass {
   const unsigned long long* offsets;
 };
 
-// Final aggregation: one shared-memory table per partition (segment).
+// One work item of the final aggregation: whole partitions [seg_lo, seg_hi),
+// or (partial = 1) the rows [row_begin, row_end) of one partition too large
+// for one CTA; a partial piece merges its groups into the HBM table.
+struct PartWork {
+  int seg_lo, seg_hi;
+  int partial;
+  int pad;
+  int64_t row_begin, row_end;
+};
+
+// Final aggregation: one shared-memory table per partition (or piece).
 struct PartAgg {
   QDesc rows;                 // partitioned rows + aggregate spec
   const long long* seg_begin; // nsegs + 1 entries
   int nsegs;
-  unsigned* seg_ctr;          // dynamic segment queue (zeroed before launch)
+  const PartWork* work;       // work items, largest first
+  int nwork;
+  unsigned* seg_ctr;          // dynamic work queue (zeroed before launch)
   int S;                      // shared table slots
   int sprobe;
   int coalesce;
-  GTable fallback;            // keys whose probe window is full
+  GTable fallback;            // keys whose probe window is full + pieces of split partitions
   unsigned* flags;
   OutDesc out;
 };

@@ -82,6 +82,24 @@ using SigSkewed = SigCT<sig_code(ACC_ADD_I, 0, GBA_I64), sig_code(ACC_CNT, 0, GB
                         sig_code(ACC_MIN_I, 0, GBA_I64), sig_code(ACC_MAX_I, 0, GBA_I64),
                         sig_code(ACC_ADD_F, 1, GBA_F32)>;
 
+// A distinct number for each signature type (queries of one number can share
+// one batched launch; run-time signatures read their ops per query).
+template <int NA>
+constexpr int gba_sig_index(SigRT<NA>) {
+  return 100 + NA;
+}
+template <typename S>
+constexpr int gba_sig_index(S) {
+  return std::is_same<S, SigSkewed>::value        ? 1
+         : std::is_same<S, SigSumSumCount>::value ? 2
+         : std::is_same<S, SigSumI64Count>::value ? 3
+         : std::is_same<S, SigSumI32Count>::value ? 4
+         : std::is_same<S, SigSumU32Count>::value ? 5
+         : std::is_same<S, SigSumU32>::value      ? 6
+         : std::is_same<S, SigCount>::value       ? 7
+                                                  : 0;
+}
+
 // Calls f(std::bool_constant<K64>, Sig) for the query's signature.
 template <typename F>
 inline cudaError_t gba_dispatch_sig(const QDesc& q, F&& f) {

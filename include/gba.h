@@ -109,6 +109,8 @@ typedef struct gba_knobs {
   int32_t smem_probe_cap; /* shared table probe cap (0 = auto) */
   int32_t max_regrow;     /* regrow attempts before GBA_ERR_TABLE_OVERFLOW */
   int32_t timing;         /* 1: time each kernel with CUDA events (gba_stats.kernel_ms) */
+  int32_t use_graph;      /* batch: -1 auto (on), 0 off, 1 on: replay the launch sequence as a CUDA graph */
+  int32_t item_rows;      /* batch: rows per work-queue item (0 = auto) */
 } gba_knobs;
 
 /* What the last call on a context did. */
@@ -125,6 +127,11 @@ typedef struct gba_stats {
    * [0] table/partition setup, [1] the main aggregation kernel,
    * [2] final reduce / compaction, [3] everything else */
   double kernel_ms[4];
+  /* input rows and their bytes (key + value columns) read by the main
+   * aggregation kernels of the call, summed over launches: the algorithmic
+   * bytes behind kernel_ms[1] */
+  int64_t main_rows;
+  int64_t main_bytes;
 } gba_stats;
 
 typedef struct gba_context gba_context;

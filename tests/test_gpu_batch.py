@@ -1,0 +1,111 @@
+"""Parity of the batched path (gba_groupby_batch: work-queue persistent launch,
+graph replay, per-query reruns, partition-strategy members) with the oracle."""
+import numpy as np
+import pytest
+
+from cpu_gpu_coprocess_groupby_agg_b200 import _abi as A
+from cpu_gpu_coprocess_groupby_agg_b200 import estimator as E
+from gpu_util import compare, to_device
+from test_gpu_parity import AGGS_ALL, _data
+
+pytestmark = pytest.mark.gpu
+
+AGG_SETS = [
+    [("sum", 0), ("count", None)],
+    [("count", None)],
+    AGGS_ALL,
+    [("sum", 2), ("count", None)],
+    [("sum", 3)],
+    [("min", 0), ("max", 0), ("sum", 1)],
+    [("sum", 0), ("sum", 2), ("count", None)],
+]
+
+
+def _queries(count, seed, max_n=150_000):
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(rng.integers(0, max_n)) if i % 9 else int(rng.integers(0, 5))
+        kdt = [np.int32, np.uint32, np.int64][i % 3]
+        ndv = int(max(1, min(n // 2 + 1, 10 ** rng.uniform(0, 5))))
+        keys, cols = _data(n, kdt, ndv, seed=seed * 1000 + i, zipf=float(rng.uniform(0, 1.5)))
+        out.append((keys, cols, AGG_SETS[i % len(AGG_SETS)]))
+    return out
+
+
+def _device(qs):
+    dq = []
+    for keys, cols, aggs in qs:
+        dq.append((to_device(keys), [to_device(c) for c in cols], aggs, keys.dtype == np.uint32,
+                   [c.dtype == np.uint32 for c in cols]))
+    return dq
+
+
+def _check(qs, res, label):
+    assert len(res) == len(qs)
+    for i, ((keys, cols, aggs), r) in enumerate(zip(qs, res)):
+        gk = r.keys.cpu().numpy()
+        if keys.dtype == np.uint32:
+            gk = gk.view(np.uint32)
+        compare(gk, [a.cpu().numpy() for a in r.aggs], keys, cols, aggs, f"{label} query {i}")
+
+
+@pytest.mark.parametrize("sizing", ["plain", "learned"])
+def test_batch_matches_oracle(ctx, sizing):
+    if sizing == "learned":
+        assert E.load_default(ctx), "committed estimator weights are missing"
+    qs = _queries(40, seed=1 if sizing == "plain" else 2)
+    res = ctx.groupby_batch(_device(qs), knobs=dict(sizing=sizing))
+    _check(qs, res, sizing)
+
+
+def test_batch_graph_replay_and_direct_launch_agree(ctx):
+    qs1 = _queries(24, seed=5)
+    # same shapes, new data: the second call replays the captured graph
+    qs2 = []
+    for i, (keys, cols, aggs) in enumerate(qs1):
+        rng = np.random.default_rng(900 + i)
+        perm = rng.permutation(len(keys))
+        qs2.append((keys[perm].copy(), [c[perm].copy() for c in cols], aggs))
+    d1, d2 = _device(qs1), _device(qs2)
+    outs = ctx.batch_outputs(d1)
+    _check(qs1, ctx.groupby_batch(d1, outs=outs), "graph first")
+    _check(qs2, ctx.groupby_batch(d2, outs=outs), "graph replay")
+    _check(qs1, ctx.groupby_batch(d1, knobs=dict(use_graph=0)), "direct")
+
+
+@pytest.mark.parametrize("knobs", [dict(tile_rows=2048), dict(blocks_per_sm=2), dict(item_rows=4096),
+                                   dict(smem_slots=128), dict(preagg=0), dict(smem_probe_cap=1)])
+def test_batch_knobs_do_not_change_results(ctx, knobs):
+    qs = _queries(12, seed=7)
+    _check(qs, ctx.groupby_batch(_device(qs), knobs=knobs), str(knobs))
+
+
+def test_batch_overflow_reruns_query_alone(ctx):
+    qs = _queries(10, seed=9)
+    res = ctx.groupby_batch(_device(qs), knobs=dict(sizing="fixed", table_slots=64, probe_cap=16, max_regrow=8,
+                                                      strategy="table"))
+    _check(qs, res, "overflow")
+    assert res[0].stats["regrows"] >= 1
+
+
+def test_batch_with_partition_members(ctx):
+    qs = _queries(6, seed=11)
+    # plain sizing: 4M rows -> a 137 MB table, past the L2-resident bound -> partition
+    keys, cols = _data(4_000_000, np.int64, 2_000_000, seed=99)
+    qs.insert(3, (keys, cols, [("sum", 0), ("count", None)]))
+    res = ctx.groupby_batch(_device(qs))
+    _check(qs, res, "mixed strategies")
+    assert res[0].stats["strategy"] == A.STRATEGY_AUTO  # both kinds ran
+
+
+def test_batch_empty_and_capacity_error(ctx):
+    assert ctx.groupby_batch([]) == []
+    qs = _queries(3, seed=13)
+    keys, cols = _data(10_000, np.int64, 5000, seed=1)
+    qs.append((keys, cols, [("count", None)]))
+    dq = _device(qs)
+    outs = ctx.batch_outputs(dq, capacity=[len(q[0]) + 1 for q in qs[:-1]] + [10])
+    with pytest.raises(A.GbaError) as e:
+        ctx.groupby_batch(dq, outs=outs)
+    assert e.value.status == A.ERR_OUTPUT_CAPACITY

@@ -61,3 +61,18 @@ def test_auto_strategy_picks_partition_for_high_cardinality(ctx):
     gk, ga, res = run_gpu(ctx, keys, cols, w.aggs)
     assert res.stats["strategy"] == 2
     compare(gk, ga, keys, cols, w.aggs, w.name)
+
+
+@pytest.mark.parametrize("bits", [4, 8])
+def test_partition_split_hot_partitions(ctx, bits):
+    """Partitions holding hot keys (far more rows than one CTA should take) are
+    split into pieces whose groups merge through the HBM table; the all-ones
+    key is among the hot ones."""
+    keys, cols = _data(1 << 21, np.int64, 2000, seed=40 + bits, zipf=1.5)
+    keys[::3] = -1
+    gk, ga, res = run_gpu(ctx, keys, cols, AGGS_ALL, knobs=dict(strategy="partition", partition_bits=bits))
+    assert res.stats["strategy"] == 2
+    compare(gk, ga, keys, cols, AGGS_ALL, f"partition split bits={bits}")
+    k32 = keys.astype(np.uint32)
+    gk, ga, _ = run_gpu(ctx, k32, cols, AGGS_ALL, knobs=dict(strategy="partition", partition_bits=bits))
+    compare(gk, ga, k32, cols, AGGS_ALL, f"partition split u32 bits={bits}")
