@@ -6,5 +6,5 @@ A drop-in for the tiled group-by path of PneNPproof/cpu_gpu_coprocess_groupby_ag
 ``include/tiled_groupby_agg_partition.hpp``); this package is its Python host
 binding.
 """
-from .api import Context, Result, gen_device, gen_host, gen_spec, make_knobs  # noqa: F401
+from .api import Context, Result, Server, gen_device, gen_host, gen_spec, make_knobs  # noqa: F401
 from . import _abi  # noqa: F401

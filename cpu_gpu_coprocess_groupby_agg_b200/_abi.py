@@ -110,6 +110,29 @@ class GenSpec(C.Structure):
     ]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [
+        ("device", C.c_int32),
+        ("lanes", C.c_int32),
+        ("memory_budget", C.c_int64),
+        ("max_batch", C.c_int32),
+        ("batch_rows", C.c_int64),
+        ("knobs", Knobs),
+    ]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [
+        ("status", C.c_int32),
+        ("lane", C.c_int32),
+        ("batch_size", C.c_int32),
+        ("n_groups", C.c_int64),
+        ("queue_ms", C.c_double),
+        ("service_ms", C.c_double),
+        ("latency_ms", C.c_double),
+    ]
+
+
 # every function include/gba.h declares, with its ctypes signature
 _P = C.c_void_p
 SIGNATURES = {
@@ -127,6 +150,16 @@ SIGNATURES = {
     "gba_groupby_batch": (C.c_int, [_P, C.c_int32, C.POINTER(Query), C.POINTER(Output), C.POINTER(Knobs), _P,
                                     C.POINTER(C.c_int64)]),
     "gba_groupby_noalloc": (C.c_int, [_P, C.POINTER(Query), C.POINTER(Output), _P, C.POINTER(C.c_int64)]),
+    "gba_groupby_partition_u32": (C.c_int, [_P, _P, _P, C.c_int64, C.c_int32, _P, _P, _P, _P]),
+    "gba_server_default_config": (None, [C.POINTER(ServerConfig)]),
+    "gba_server_create": (C.c_int, [C.POINTER(_P), C.POINTER(ServerConfig)]),
+    "gba_server_estimator_load": (C.c_int, [_P, C.POINTER(C.c_float)]),
+    "gba_server_submit": (C.c_int, [_P, C.POINTER(Query), C.POINTER(Output), C.POINTER(C.c_int64)]),
+    "gba_server_wait": (C.c_int, [_P, C.c_int64, C.c_double, C.POINTER(RequestInfo)]),
+    "gba_server_next_done": (C.c_int, [_P, C.c_double, C.POINTER(C.c_int64), C.POINTER(RequestInfo)]),
+    "gba_server_pending": (C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "gba_server_last_error": (C.c_char_p, [_P]),
+    "gba_server_destroy": (C.c_int, [_P]),
     "gba_estimator_features": (C.c_int, [_P, C.POINTER(Query), C.c_int64, _P, C.POINTER(C.c_float)]),
     "gba_estimator_param_count": (C.c_int64, []),
     "gba_estimator_load": (C.c_int, [_P, C.POINTER(C.c_float)]),

@@ -346,3 +346,93 @@ def gen_device(spec: A.GenSpec, n: int, row0: int = 0, device: int = 0, stream=N
     A.check(A.lib().gba_gen_device(C.byref(spec), row0, n, C.c_void_p(keys.data_ptr()), ptrs,
                                    C.c_void_p(s.cuda_stream)))
     return keys, cols
+
+
+# ---- serving ------------------------------------------------------------------------
+@dataclass
+class RequestInfo:
+    ticket: int
+    status: int
+    n_groups: int
+    lane: int
+    batch_size: int
+    queue_ms: float
+    service_ms: float
+    latency_ms: float
+
+
+class Server:
+    """Continuous-batching request loop over ``lanes`` CUDA streams
+    (gba_server_*).  Requests take device tensors and device output buffers;
+    keep both alive until the request is collected."""
+
+    def __init__(self, device: int = 0, lanes: int = 4, memory_budget: int = 120 << 30, max_batch: int = 64,
+                 batch_rows: int = 1 << 24, knobs=None, estimator_params=None):
+        self._lib = A.lib()
+        cfg = A.ServerConfig()
+        self._lib.gba_server_default_config(C.byref(cfg))
+        cfg.device, cfg.lanes, cfg.memory_budget = device, lanes, memory_budget
+        cfg.max_batch, cfg.batch_rows = max_batch, batch_rows
+        if knobs is not None:
+            cfg.knobs = knobs if isinstance(knobs, A.Knobs) else make_knobs(**knobs)
+        h = C.c_void_p()
+        A.check(self._lib.gba_server_create(C.byref(h), C.byref(cfg)))
+        self._h = h
+        if estimator_params is not None:
+            p = np.ascontiguousarray(estimator_params, dtype=np.float32)
+            self._check(self._lib.gba_server_estimator_load(self._h, p.ctypes.data_as(C.POINTER(C.c_float))))
+
+    def _check(self, st):
+        if st != A.OK:
+            raise A.GbaError(st, f"{self._lib.gba_status_string(st).decode()} "
+                                 f"({self._lib.gba_server_last_error(self._h).decode()})")
+
+    def submit(self, keys, cols, aggs, out, unsigned_keys: bool = False) -> int:
+        """out = (keys_out, [agg_out, ...]) device tensors; returns the ticket."""
+        col_specs = [(c.data_ptr(), _torch_type(c)) for c in cols]
+        q = build_query(keys.numel(), keys.data_ptr(), _torch_type(keys, unsigned_keys), col_specs, parse_aggs(aggs))
+        okeys, oaggs = out
+        o = A.Output()
+        o.keys = okeys.data_ptr()
+        for i, t in enumerate(oaggs):
+            o.aggs[i] = t.data_ptr()
+        o.capacity = okeys.numel()
+        t = C.c_int64(0)
+        self._check(self._lib.gba_server_submit(self._h, C.byref(q), C.byref(o), C.byref(t)))
+        return t.value
+
+    @staticmethod
+    def _info(ticket, i: A.RequestInfo) -> RequestInfo:
+        return RequestInfo(ticket, i.status, i.n_groups, i.lane, i.batch_size, i.queue_ms, i.service_ms,
+                           i.latency_ms)
+
+    def wait(self, ticket: int, timeout: float = 60.0) -> RequestInfo:
+        info = A.RequestInfo()
+        self._check(self._lib.gba_server_wait(self._h, ticket, timeout, C.byref(info)))
+        return self._info(ticket, info)
+
+    def next_done(self, timeout: float = 0.0):
+        """The next finished request, or None if none finished within timeout."""
+        info = A.RequestInfo()
+        t = C.c_int64(0)
+        st = self._lib.gba_server_next_done(self._h, timeout, C.byref(t), C.byref(info))
+        if st == A.ERR_TIMEOUT:
+            return None
+        self._check(st)
+        return self._info(t.value, info)
+
+    def pending(self):
+        q, r, b = C.c_int64(0), C.c_int64(0), C.c_int64(0)
+        self._check(self._lib.gba_server_pending(self._h, C.byref(q), C.byref(r), C.byref(b)))
+        return q.value, r.value, b.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.gba_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -85,7 +85,28 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    build_driver(lib)
     return lib
+
+
+DRIVER_SRC = PKG.parent / "tests" / "drivers" / "tiled_driver.cu"
+
+
+def build_driver(lib: Path) -> Path | None:
+    """``lib/tiled_driver``: a caller of the drop-in C++ API written like the
+    reference's test/test.cu (used by the drop-in parity tests)."""
+    if not DRIVER_SRC.exists():
+        return None
+    exe = LIBDIR / "tiled_driver"
+    hdr = INCLUDE / "tiled_groupby_agg_partition.hpp"
+    if not _stale(exe, [DRIVER_SRC, hdr, lib]):
+        return exe
+    cmd = [nvcc(), *ARCH, "-O2", "-std=c++17", "-I", str(INCLUDE), str(DRIVER_SRC), "-o", str(exe),
+           "-L", str(LIBDIR), "-lgba", "-Xlinker", "-rpath", "-Xlinker", "$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"driver build failed:\n{r.stdout}\n{r.stderr}")
+    return exe
 
 
 if __name__ == "__main__":

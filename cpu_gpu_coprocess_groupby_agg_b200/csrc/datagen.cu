@@ -94,6 +94,8 @@ extern "C" int64_t gba_abi_struct_size(int32_t which) {
     case 2: return int64_t(sizeof(gba_knobs));
     case 3: return int64_t(sizeof(gba_stats));
     case 4: return int64_t(sizeof(gba_gen_spec));
+    case 5: return int64_t(sizeof(gba_server_config));
+    case 6: return int64_t(sizeof(gba_request_info));
   }
   return -1;
 }

@@ -3,6 +3,9 @@
 #include "gba_kernels.h"
 
 #define GBA_EST_MAX_TILES 256
+// largest row count of the tables the shipped weights were trained on
+// (estimator_weights.f32: rows log-uniform in [2^12, 2^24])
+#define GBA_EST_TRAINED_MAX_ROWS (int64_t(1) << 24)
 
 // One query's sampling job and its scratch (all device pointers).
 struct EstQuery {
@@ -17,6 +20,7 @@ struct EstQuery {
   unsigned* hll;              // 64 registers
   float* feat;                // 32 features
   unsigned long long* stats;  // [0] distinct sampled keys, [1] max count, [2] sampled rows, [3] all-ones key count
+  unsigned long long* freq;   // [0] distinct, [1..4] f1, f2, f3, f4+, [5] max count, [6] sampled rows
 };
 
 void gba_est_plan(EstQuery* e, int64_t n, int64_t tile_rows);

@@ -91,6 +91,7 @@ extern "C" gba_status gba_destroy(gba_context* ctx) {
   if (ctx->batch_exec) cudaGraphExecDestroy(ctx->batch_exec);
   if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
   if (ctx->h_batch) cudaFreeHost(ctx->h_batch);
+  if (ctx->rp_buf) cudaFree(ctx->rp_buf);
   delete ctx;
   return GBA_OK;
 }

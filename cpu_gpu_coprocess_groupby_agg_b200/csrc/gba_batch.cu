@@ -184,23 +184,26 @@ extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_
   const int nt = int(tq.size());
 
   // ---- work items ----
-  int64_t total_rows = 0;
-  for (int i : tq) total_rows += qd[i].n;
+  // Query-major: all row ranges of one query are consecutive in the queue and
+  // the largest queries come first, so at any moment the CTAs work on one or
+  // two queries and only their HBM tables compete for L2 (with items dealt
+  // longest-first across queries, every large query's table was live at once
+  // and the random table updates spilled from L2 to DRAM).  A query's rows
+  // are cut into about one item per CTA (at least one tile, at most
+  // item_rows or 2^20 rows), so one query occupies the whole grid.
   const int grid_max = ctx->sms * bps;
-  int64_t item_rows = k.item_rows > 0 ? int64_t(k.item_rows)
-                                      : std::min<int64_t>(int64_t(1) << 20,
-                                                          std::max<int64_t>(4 * int64_t(T), total_rows / (4 * grid_max)));
-  item_rows = std::max<int64_t>(T, (item_rows + T - 1) / T * T);
+  const int64_t item_cap = k.item_rows > 0 ? std::max<int64_t>(T, int64_t(k.item_rows)) : (int64_t(1) << 20);
   std::vector<BatchItem> items;
   for (auto& g : groups) {
     g.item_begin = int64_t(items.size());
-    for (int i : g.members)
-      for (int64_t r = 0; r < qd[i].n; r += item_rows)
-        items.push_back(BatchItem{qi[i].slot, 0, r, std::min(qd[i].n, r + item_rows)});
+    std::vector<int> order = g.members;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return qd[a].n > qd[b].n; });
+    for (int i : order) {
+      int64_t ir = (qd[i].n + grid_max - 1) / grid_max;
+      ir = std::min(item_cap, std::max<int64_t>(T, (ir + T - 1) / T * T));
+      for (int64_t r = 0; r < qd[i].n; r += ir) items.push_back(BatchItem{qi[i].slot, 0, r, std::min(qd[i].n, r + ir)});
+    }
     g.nitems = int64_t(items.size()) - g.item_begin;
-    std::stable_sort(items.begin() + g.item_begin, items.end(), [](const BatchItem& a, const BatchItem& b) {
-      return a.row_end - a.row_begin > b.row_end - b.row_begin;
-    });
     g.grid = int(std::max<int64_t>(1, std::min<int64_t>(g.nitems, grid_max)));
   }
   const int ng = int(groups.size());

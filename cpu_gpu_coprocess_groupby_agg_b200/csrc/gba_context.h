@@ -42,6 +42,9 @@ struct gba_context {
   cudaStream_t cap_stream = nullptr;
   cudaGraphExec_t batch_exec = nullptr;
   std::vector<int64_t> batch_key;
+  // drop-in API: a tile's groups before the reference-layout partitioning
+  void* rp_buf = nullptr;
+  size_t rp_bytes = 0;
   std::string err;
   gba_stats stats{};
 };

@@ -60,11 +60,29 @@ __global__ void k_est_init(const EstQuery* qs, int nq) {
   }
 }
 
+// Frequency-class bookkeeping: a key's count moving from c to c + 1 leaves
+// class min(c, 4) and enters class min(c + 1, 4) (classes 1, 2, 3, 4+), and
+// c == 0 makes it a new distinct key.  Whatever order the increments run in,
+// the totals end exact, so the sample's frequency profile needs no scan of
+// the count table afterwards.  f[0] distinct, f[1..4] f1..f4+, f[5] max count,
+// f[6] sampled rows (block-local shared counters, flushed once per query).
+__device__ __forceinline__ void freq_step(unsigned long long* f, unsigned long long old) {
+  if (old == 0) atomicAdd(&f[0], 1ull);
+  else if (old < 4) atomicAdd(&f[old], ~0ull);  // -1
+  if (old < 4) atomicAdd(&f[old + 1], 1ull);
+  atomicMax(&f[5], old + 1);
+  atomicAdd(&f[6], 1ull);
+}
+
 // one thread per sampled row; per-query count table (keys + counts, linear
-// probing, capacity >= 2x the sample) and 64 HLL registers
+// probing, capacity >= 2x the sample), 64 HLL registers and the frequency
+// classes
 __global__ void k_est_sample(const EstQuery* qs, int nq) {
+  __shared__ unsigned long long sf[7];
   for (int qi = blockIdx.y; qi < nq; qi += gridDim.y) {
     const EstQuery e = qs[qi];
+    if (threadIdx.x < 7) sf[threadIdx.x] = 0ull;
+    __syncthreads();
     const int64_t items = int64_t(e.sampled_tiles) << 10;
     for (int64_t it = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; it < items;
          it += int64_t(gridDim.x) * blockDim.x) {
@@ -79,7 +97,7 @@ __global__ void k_est_sample(const EstQuery* qs, int nq) {
       const unsigned rank = __clz((h << 6) | (1u << 5)) + 1;
       if (rank > __ldcg(&e.hll[reg])) atomicMax(&e.hll[reg], rank);
       if (k == EMPTY64) {  // the table's empty marker (only a 64-bit key can equal it)
-        atomicAdd(&e.stats[3], 1ull);
+        freq_step(sf, atomicAdd(&e.stats[3], 1ull));
         continue;
       }
       uint64_t s = (uint64_t(table_hash(k)) * e.cap) >> 32;
@@ -87,123 +105,138 @@ __global__ void k_est_sample(const EstQuery* qs, int nq) {
         unsigned long long* slot = e.table + 2 * s;
         const unsigned long long cur = __ldcg(slot);
         if (cur == k) {
-          atomicAdd(slot + 1, 1ull);
+          freq_step(sf, atomicAdd(slot + 1, 1ull));
           break;
         }
         if (cur == EMPTY64) {
           const unsigned long long prev = atomicCAS(slot, EMPTY64, k);
           if (prev == EMPTY64 || prev == k) {
-            atomicAdd(slot + 1, 1ull);
+            freq_step(sf, atomicAdd(slot + 1, 1ull));
             break;
           }
         }
         s = s + 1 == e.cap ? 0 : s + 1;
       }
     }
+    __syncthreads();
+    if (threadIdx.x < 7 && sf[threadIdx.x] != 0ull) {
+      if (threadIdx.x == 5) atomicMax(&e.freq[5], sf[5]);
+      else atomicAdd(&e.freq[threadIdx.x], sf[threadIdx.x]);
+    }
+    __syncthreads();
   }
 }
 
-// per query: frequency profile of the sample -> the 32 features
+// per query (one thread each): frequency profile and HLL registers -> the 32
+// features
 __global__ void k_est_reduce(const EstQuery* qs, int nq) {
-  __shared__ unsigned long long acc[7];
-  for (int qi = blockIdx.x; qi < nq; qi += gridDim.x) {
+  for (int qi = blockIdx.x * blockDim.x + threadIdx.x; qi < nq; qi += gridDim.x * blockDim.x) {
     const EstQuery e = qs[qi];
-    if (threadIdx.x < 7) acc[threadIdx.x] = 0;
-    __syncthreads();
-    unsigned long long d = 0, f1 = 0, f2 = 0, f3 = 0, f4 = 0, mx = 0, tot = 0;
-    auto count = [&](unsigned long long c) {
-      if (c == 0) return;
-      ++d;
-      f1 += c == 1;
-      f2 += c == 2;
-      f3 += c == 3;
-      f4 += c >= 4;
-      mx = c > mx ? c : mx;
-      tot += c;
-    };
-    for (uint64_t i = threadIdx.x; i < e.cap; i += blockDim.x) count(e.table[2 * i + 1]);
-    if (threadIdx.x == 0) count(e.stats[3]);
-    atomicAdd(&acc[0], d);
-    atomicAdd(&acc[1], f1);
-    atomicAdd(&acc[2], f2);
-    atomicAdd(&acc[3], f3);
-    atomicAdd(&acc[4], f4);
-    atomicMax(&acc[5], mx);
-    atomicAdd(&acc[6], tot);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      float* f = e.feat;
-      const double n = double(e.n), s = double(acc[6] > 0 ? acc[6] : 1);
-      const double dd = double(acc[0]), a1 = double(acc[1]), a2 = double(acc[2]);
-      const double gee = sqrt(n / s) * a1 + (dd - a1);
-      const double chao = dd + a1 * a1 / (2.0 * (a2 > 1 ? a2 : 1.0));
-      // HLL estimate (m = 64, alpha_64 = 0.709) with the small-range correction
-      double z = 0;
-      int zeros = 0;
-      int hist[16] = {0};
-      for (int r = 0; r < 64; ++r) {
-        const unsigned v = e.hll[r];
-        z += ldexp(1.0, -int(v));
-        zeros += v == 0;
-        hist[v < 15 ? v : 15]++;
-      }
-      double hll = 0.709 * 64 * 64 / z;
-      if (hll <= 2.5 * 64 && zeros > 0) hll = 64 * log(64.0 / zeros);
-      f[0] = float(log2(n + 1) / 32);
-      f[1] = float(log2(s + 1) / 32);
-      f[2] = float(dd / s);
-      f[3] = float(a1 / s);
-      f[4] = float(a2 / s);
-      f[5] = float(double(acc[3]) / s);
-      f[6] = float(double(acc[4]) / s);
-      f[7] = float(log2(dd + 1) / 32);
-      f[8] = float(log2(gee + 1) / 32);
-      f[9] = float(log2(chao + 1) / 32);
-      f[10] = float(log2(hll + 1) / 32);
-      f[11] = float(double(acc[5]) / s);
-      f[12] = e.key64 ? 1.0f : 0.5f;
-      f[13] = float(s / (n > 0 ? n : 1));
-      for (int i = 0; i < 16; ++i) f[14 + i] = float(hist[i]) / 64.0f;
-      f[30] = float(log2(n / s > 1 ? n / s : 1) / 32);
-      f[31] = 1.0f;
-      e.stats[0] = acc[0];
-      e.stats[1] = acc[5];
-      e.stats[2] = acc[6];
+    unsigned long long acc[7];
+#pragma unroll
+    for (int i = 0; i < 7; ++i) acc[i] = e.freq[i];
+    float* f = e.feat;
+    const double n = double(e.n), s = double(acc[6] > 0 ? acc[6] : 1);
+    const double dd = double(acc[0]), a1 = double(acc[1]), a2 = double(acc[2]);
+    const double gee = sqrt(n / s) * a1 + (dd - a1);
+    const double chao = dd + a1 * a1 / (2.0 * (a2 > 1 ? a2 : 1.0));
+    // HLL estimate (m = 64, alpha_64 = 0.709) with the small-range correction
+    double z = 0;
+    int zeros = 0;
+    int hist[16] = {0};
+    for (int r = 0; r < 64; ++r) {
+      const unsigned v = e.hll[r];
+      z += ldexp(1.0, -int(v));
+      zeros += v == 0;
+      hist[v < 15 ? v : 15]++;
     }
-    __syncthreads();
+    double hll = 0.709 * 64 * 64 / z;
+    if (hll <= 2.5 * 64 && zeros > 0) hll = 64 * log(64.0 / zeros);
+    f[0] = float(log2(n + 1) / 32);
+    f[1] = float(log2(s + 1) / 32);
+    f[2] = float(dd / s);
+    f[3] = float(a1 / s);
+    f[4] = float(a2 / s);
+    f[5] = float(double(acc[3]) / s);
+    f[6] = float(double(acc[4]) / s);
+    f[7] = float(log2(dd + 1) / 32);
+    f[8] = float(log2(gee + 1) / 32);
+    f[9] = float(log2(chao + 1) / 32);
+    f[10] = float(log2(hll + 1) / 32);
+    f[11] = float(double(acc[5]) / s);
+    f[12] = e.key64 ? 1.0f : 0.5f;
+    f[13] = float(s / (n > 0 ? n : 1));
+    for (int i = 0; i < 16; ++i) f[14 + i] = float(hist[i]) / 64.0f;
+    f[30] = float(log2(n / s > 1 ? n / s : 1) / 32);
+    f[31] = 1.0f;
+    e.stats[0] = acc[0];
+    e.stats[1] = acc[5];
+    e.stats[2] = acc[6];
   }
 }
 
 // ---- MLP ------------------------------------------------------------------------
 __device__ __forceinline__ float relu(float x) { return x > 0.f ? x : 0.f; }
 
-// one thread per sample
-__global__ void k_mlp_forward(const float* __restrict__ W, const float* __restrict__ X, int n,
-                              float* __restrict__ out) {
-  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < n; b += gridDim.x * blockDim.x) {
-    float x[F], h1[H], h2[H];
+// Inference: a CTA of H threads takes kFwdRows samples; thread j computes
+// hidden unit j of every sample of the CTA, activations stay in shared memory
+// and the output unit is a warp-shuffle sum over the hidden units.
+constexpr int kFwdRows = 8;
+__global__ void __launch_bounds__(H) k_mlp_forward(const float* __restrict__ W, const float* __restrict__ X, int n,
+                                                   float* __restrict__ out) {
+  __shared__ float xs[kFwdRows][F];
+  __shared__ float ha[kFwdRows][H];
+  __shared__ float hb[kFwdRows][H];
+  __shared__ float part[kFwdRows][H / 32];
+  const int j = threadIdx.x;
+  for (int b0 = blockIdx.x * kFwdRows; b0 < n; b0 += gridDim.x * kFwdRows) {
+    const int rows = n - b0 < kFwdRows ? n - b0 : kFwdRows;
+    for (int i = j; i < kFwdRows * F; i += H) xs[i / F][i % F] = i / F < rows ? X[size_t(b0) * F + i] : 0.f;
+    __syncthreads();
+    float acc[kFwdRows];
 #pragma unroll
-    for (int i = 0; i < F; ++i) x[i] = X[size_t(b) * F + i];
-    for (int j = 0; j < H; ++j) {
-      float a = __ldg(W + OB1 + j);
+    for (int r = 0; r < kFwdRows; ++r) acc[r] = __ldg(W + OB1 + j);
+    for (int i = 0; i < F; ++i) {
+      const float w = __ldg(W + OW1 + j * F + i);
 #pragma unroll
-      for (int i = 0; i < F; ++i) a = fmaf(__ldg(W + OW1 + j * F + i), x[i], a);
-      h1[j] = relu(a);
+      for (int r = 0; r < kFwdRows; ++r) acc[r] = fmaf(w, xs[r][i], acc[r]);
     }
-    for (int j = 0; j < H; ++j) {
-      float a = __ldg(W + OB2 + j);
-#pragma unroll 8
-      for (int i = 0; i < H; ++i) a = fmaf(__ldg(W + OW2 + j * H + i), h1[i], a);
-      h2[j] = relu(a);
+#pragma unroll
+    for (int r = 0; r < kFwdRows; ++r) ha[r][j] = relu(acc[r]);
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kFwdRows; ++r) acc[r] = __ldg(W + OB2 + j);
+    for (int i = 0; i < H; ++i) {
+      const float w = __ldg(W + OW2 + j * H + i);
+#pragma unroll
+      for (int r = 0; r < kFwdRows; ++r) acc[r] = fmaf(w, ha[r][i], acc[r]);
     }
-    float y = __ldg(W + OB4);
-    for (int j = 0; j < H; ++j) {
-      float a = __ldg(W + OB3 + j);
-#pragma unroll 8
-      for (int i = 0; i < H; ++i) a = fmaf(__ldg(W + OW3 + j * H + i), h2[i], a);
-      y = fmaf(__ldg(W + OW4 + j), relu(a), y);
+#pragma unroll
+    for (int r = 0; r < kFwdRows; ++r) hb[r][j] = relu(acc[r]);
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kFwdRows; ++r) acc[r] = __ldg(W + OB3 + j);
+    for (int i = 0; i < H; ++i) {
+      const float w = __ldg(W + OW3 + j * H + i);
+#pragma unroll
+      for (int r = 0; r < kFwdRows; ++r) acc[r] = fmaf(w, hb[r][i], acc[r]);
     }
-    out[b] = y;
+    const float w4 = __ldg(W + OW4 + j);
+#pragma unroll
+    for (int r = 0; r < kFwdRows; ++r) {
+      float v = w4 * relu(acc[r]);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(GBA_FULL_MASK, v, o);
+      if ((j & 31) == 0) part[r][j >> 5] = v;
+    }
+    __syncthreads();
+    if (j < rows) {
+      float y = __ldg(W + OB4);
+#pragma unroll
+      for (int w = 0; w < H / 32; ++w) y += part[j][w];
+      out[b0 + j] = y;
+    }
+    __syncthreads();
   }
 }
 
@@ -332,12 +365,13 @@ cudaError_t gba_launch_est_init(const EstQuery* d_qs, int nq, cudaStream_t s) {
   return cudaGetLastError();
 }
 cudaError_t gba_launch_est_reduce(const EstQuery* d_qs, int nq, cudaStream_t s) {
-  k_est_reduce<<<std::min(nq, 4096), 256, 0, s>>>(d_qs, nq);
+  if (nq <= 0) return cudaSuccess;
+  k_est_reduce<<<(nq + 127) / 128, 128, 0, s>>>(d_qs, nq);
   return cudaGetLastError();
 }
 cudaError_t gba_launch_mlp_forward(const float* W, const float* X, int n, float* out, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
-  k_mlp_forward<<<(n + 127) / 128, 128, 0, s>>>(W, X, n, out);
+  k_mlp_forward<<<std::min((n + kFwdRows - 1) / kFwdRows, 1184), H, 0, s>>>(W, X, n, out);
   return cudaGetLastError();
 }
 
@@ -518,6 +552,7 @@ gba_status gba_est_features_device(gba_context* ctx, const QDesc* qs, int nq, in
   const size_t o_f = take(sizeof(float) * F * nq);
   const size_t o_s = take(8 * 4 * size_t(nq));
   const size_t o_h = take(4 * 64 * size_t(nq));
+  const size_t o_fr = take(8 * 8 * size_t(nq));
   std::vector<size_t> o_t(nq);
   int64_t max_items = 0;
   for (int i = 0; i < nq; ++i) {
@@ -535,9 +570,11 @@ gba_status gba_est_features_device(gba_context* ctx, const QDesc* qs, int nq, in
     eq[i].hll = reinterpret_cast<unsigned*>(base + o_h) + 64 * i;
     eq[i].feat = reinterpret_cast<float*>(base + o_f) + F * i;
     eq[i].stats = reinterpret_cast<unsigned long long*>(base + o_s) + 4 * i;
+    eq[i].freq = reinterpret_cast<unsigned long long*>(base + o_fr) + 8 * i;
   }
   GBA_CUDA_TRY(ctx, cudaMemsetAsync(base + o_h, 0, 4 * 64 * size_t(nq), s));
   GBA_CUDA_TRY(ctx, cudaMemsetAsync(base + o_s, 0, 8 * 4 * size_t(nq), s));
+  GBA_CUDA_TRY(ctx, cudaMemsetAsync(base + o_fr, 0, 8 * 8 * size_t(nq), s));
   GBA_CUDA_TRY(ctx, cudaMemcpyAsync(base + o_q, eq.data(), sizeof(EstQuery) * nq, cudaMemcpyHostToDevice, s));
   const EstQuery* dq = reinterpret_cast<const EstQuery*>(base + o_q);
   GBA_CUDA_TRY(ctx, gba_launch_est_init(dq, nq, s));
@@ -581,12 +618,20 @@ gba_status gba_predict_groups(gba_context* ctx, const QDesc& q, cudaStream_t s, 
   GBA_CUDA_TRY(ctx, gba_launch_mlp_forward(ctx->d_est, f, 1, y, s));
   GBA_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_small + 1024, y, 4, cudaMemcpyDeviceToHost, s));
   GBA_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_small + 1032, stats, 32, cudaMemcpyDeviceToHost, s));
+  GBA_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_small + 1088, f, F * sizeof(float), cudaMemcpyDeviceToHost, s));
   GBA_CUDA_TRY(ctx, cudaStreamSynchronize(s));
   ctx->stats.kernel_launches += 1;
   const float t = *reinterpret_cast<float*>(ctx->h_small + 1024);
   const unsigned long long d = *reinterpret_cast<unsigned long long*>(ctx->h_small + 1032);
+  const float* feat = reinterpret_cast<const float*>(ctx->h_small + 1088);
   double g = exp2(double(t) * 32.0);
   g = std::max(g, double(d));
+  // Beyond the row counts the network was trained on it extrapolates; there
+  // it is not trusted below the Chao1 estimate of the same sample (which is
+  // close when the sample is mostly singletons, the case a small sample of a
+  // very large high-cardinality column gives).  An over-estimate only costs
+  // a larger table; an under-estimate costs a re-run.
+  if (q.n > GBA_EST_TRAINED_MAX_ROWS) g = std::max(g, exp2(double(feat[9]) * 32.0) - 1.0);
   g = std::min(g, double(std::max<int64_t>(q.n, 1)));
   *groups = g;
   // share of the sample taken by its most frequent key (skew signal)

@@ -39,6 +39,11 @@ def init_params(seed: int = 0) -> np.ndarray:
     return np.concatenate(parts)
 
 
+def load_weights() -> np.ndarray:
+    """The committed estimator weights (fp32, gba_estimator_param_count values)."""
+    return np.fromfile(WEIGHTS, dtype=np.float32)
+
+
 def load_default(ctx) -> bool:
     """Loads the committed weights into ctx; False when the file is absent."""
     if not WEIGHTS.exists():

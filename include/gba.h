@@ -15,7 +15,7 @@
  *                                           groupby_agg_intra_partition.cuh:5-13
  * Together they compute an exact GROUP BY SUM of u32 values by u32 key.  The
  * C++ drop-ins with those exact signatures are declared in
- * tiled_groupby_agg_partition.hpp and are built on the functions below.
+ * tiled_groupby_agg_partition.hpp and are built on gba_groupby_partition_u32.
  */
 #ifndef GBA_H
 #define GBA_H
@@ -137,7 +137,8 @@ typedef struct gba_stats {
 typedef struct gba_context gba_context;
 
 /* sizeof() of the ABI structs, for binding generators: which = 0 gba_query,
- * 1 gba_output, 2 gba_knobs, 3 gba_stats, 4 gba_gen_spec. */
+ * 1 gba_output, 2 gba_knobs, 3 gba_stats, 4 gba_gen_spec, 5 gba_server_config,
+ * 6 gba_request_info. */
 int64_t gba_abi_struct_size(int32_t which);
 
 void gba_default_knobs(gba_knobs* k);
@@ -192,6 +193,69 @@ gba_status gba_groupby_batch(gba_context* ctx, int32_t n_queries, const gba_quer
  * time on one device race; serialise them.  Synchronises `stream`. */
 gba_status gba_groupby_noalloc(gba_context* ctx, const gba_query* q, const gba_output* out, void* stream,
                                int64_t* n_groups);
+
+/* One tile of the reference's phase 1 on DEVICE columns: the exact GROUP BY
+ * SUM of u32 values by u32 key (the sum wraps mod 2^32 like the reference's
+ * u32 atomicAdd, kernel.cu:48,152), with the groups written to
+ * out_keys / out_vals ordered by partition murmur3_32(key, seed 0) % P.
+ * part_offsets (HOST, P + 1 entries) receives each partition's first group and
+ * the group count.  1 <= P <= 16384.  out_keys / out_vals hold n_rows entries
+ * and may be keys / vals themselves (the reference writes a tile's partitioned
+ * groups over its input, group_then_partition.cu:413-417).  Replaces
+ * compute_groupby_agg_result + compute_partition_result
+ * (group_then_partition.cu:24-306).  Synchronises `stream`.  The C++ drop-ins
+ * of include/tiled_groupby_agg_partition.hpp are built on it. */
+gba_status gba_groupby_partition_u32(gba_context* ctx, const uint32_t* keys, const uint32_t* vals, int64_t n_rows,
+                                     int32_t P, uint32_t* out_keys, uint32_t* out_vals, uint64_t* part_offsets,
+                                     void* stream);
+
+/* ---- serving: continuous batching under a device-memory budget ----------
+ * No counterpart in the reference (one query per call).  A server runs `lanes`
+ * host workers, each with its own CUDA stream and context, so their work
+ * overlaps on the device and each keeps its tables and workspace resident
+ * between requests.  Submitted requests (device columns in, device output
+ * columns out, as gba_groupby) queue in arrival order; a free lane takes the
+ * head of the queue and, when it is small (n_rows <= batch_rows), every
+ * following small request (up to max_batch) that still fits the budget, and
+ * runs them as one gba_groupby_batch call; a larger request runs alone.
+ * Admission: the estimated device bytes of the running requests never exceed
+ * memory_budget; a request that alone exceeds it is refused at submit with
+ * GBA_ERR_BUDGET.  The caller keeps a request's columns and output buffers
+ * alive until it is collected (gba_server_wait / gba_server_next_done). */
+typedef struct gba_server gba_server;
+
+typedef struct gba_server_config {
+  int32_t device;
+  int32_t lanes;         /* concurrent lanes (default 4, at most 64) */
+  int64_t memory_budget; /* bytes (default 120 GiB) */
+  int32_t max_batch;     /* requests per batch call (default 64) */
+  int64_t batch_rows;    /* larger requests run alone (default 2^24) */
+  gba_knobs knobs;       /* knobs of every call (sizing, strategy, ...) */
+} gba_server_config;
+
+typedef struct gba_request_info {
+  int32_t status; /* gba_status of the request */
+  int32_t lane;
+  int32_t batch_size; /* requests in the call it ran in */
+  int64_t n_groups;
+  double queue_ms;   /* submit -> taken by a lane */
+  double service_ms; /* taken -> result complete */
+  double latency_ms; /* submit -> result complete */
+} gba_request_info;
+
+void gba_server_default_config(gba_server_config* c);
+gba_status gba_server_create(gba_server** out, const gba_server_config* cfg);
+/* Loads estimator weights into every lane (learned sizing); only while idle. */
+gba_status gba_server_estimator_load(gba_server* sv, const float* params);
+gba_status gba_server_submit(gba_server* sv, const gba_query* q, const gba_output* out, int64_t* ticket);
+/* Waits up to timeout_s for one request; GBA_ERR_TIMEOUT if it is not done. */
+gba_status gba_server_wait(gba_server* sv, int64_t ticket, double timeout_s, gba_request_info* info);
+/* Waits up to timeout_s for any finished request and collects it. */
+gba_status gba_server_next_done(gba_server* sv, double timeout_s, int64_t* ticket, gba_request_info* info);
+gba_status gba_server_pending(gba_server* sv, int64_t* queued, int64_t* running, int64_t* inflight_bytes);
+const char* gba_server_last_error(const gba_server* sv);
+/* Finishes every submitted request, then stops the lanes and frees them. */
+gba_status gba_server_destroy(gba_server* sv);
 
 /* ---- learned cardinality estimator -------------------------------------- */
 #define GBA_EST_FEATURES 32

@@ -30,7 +30,7 @@ def test_library_exports_every_declared_function():
 
 def test_struct_layouts_match_binding():
     lib = A.lib()
-    for which, cls in enumerate([A.Query, A.Output, A.Knobs, A.Stats, A.GenSpec]):
+    for which, cls in enumerate([A.Query, A.Output, A.Knobs, A.Stats, A.GenSpec, A.ServerConfig, A.RequestInfo]):
         assert lib.gba_abi_struct_size(which) == C.sizeof(cls), cls.__name__
 
 
@@ -56,3 +56,16 @@ def test_invalid_arguments_rejected_without_gpu():
     lib = A.lib()
     assert lib.gba_groupby(None, None, None, None, None, None) == A.ERR_INVALID_ARG
     assert lib.gba_destroy(None) == A.ERR_INVALID_ARG
+
+
+def test_dropin_cxx_entry_points_exported():
+    """The reference's C++ entry points (include/tiled_groupby_agg_partition.hpp)
+    are defined in libgba.so, and the test.cu-style caller links against it."""
+    out = subprocess.run(["nm", "-DC", "--defined-only", str(A.LIB_PATH)], capture_output=True, text=True).stdout
+    assert "groupby_agg_partition<unsigned int, unsigned int>(unsigned int*, unsigned int*, unsigned long, " \
+           "unsigned long, unsigned long, std::vector<par_result" in out
+    assert "groupby_agg_intra_partition(std::vector<par_result" in out
+    driver = A.LIB_PATH.parent / "tiled_driver"
+    assert driver.exists()
+    ldd = subprocess.run(["ldd", str(driver)], capture_output=True, text=True).stdout
+    assert "libgba.so" in ldd and "not found" not in ldd.split("libgba.so")[1].splitlines()[0]
