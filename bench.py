@@ -387,7 +387,7 @@ def run_batch(args, ws, rank, local, pg):
     traffic = None
     tfile = ROOT / "profiles" / "traffic.json"
     if tfile.exists():
-        traffic = json.loads(tfile.read_text()).get(f"{BATCH_NAME}:k_batch_preagg")
+        traffic = json.loads(tfile.read_text()).get(f"{BATCH_NAME}:k_stream_agg")
     line = {
         "metric": "groupby_rows_per_s", "value": round(value, 4), "unit": "G rows/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True,
@@ -400,7 +400,7 @@ def run_batch(args, ws, rank, local, pg):
                    "l2": "inputs larger than L2 (no flush needed)", "parallelism": f"replicas x{ws}",
                    "launch": "one gba_groupby_batch call per step (CUDA graph replay)"},
         "whole_step_hbm_gbs": round(in_bytes / (ms_step / 1e3) / 1e9, 1),
-        "roofline": {"bound": "hbm", "kernel": "k_batch_preagg (+ k_part_agg of partition-strategy queries)",
+        "roofline": {"bound": "hbm", "kernel": "k_stream_agg (+ k_part_agg of partition-strategy queries)",
                      "achieved": round(achieved, 1) if achieved else None, "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4) if achieved else None, "peak_kind": peak_kind,
                      "traffic": traffic, "alg_bytes_per_step": int(main_bytes), "launch_ms": round(main_ms, 4)},

@@ -9,7 +9,7 @@ struct BatchQ {
   OutDesc out;
   unsigned* flags;  // this query's status bits
   int S;            // its shared-table slots (0 = no pre-aggregation)
-  int pad;
+  int pad;          // bit 0: keys and columns 16-byte aligned (vector loads)
 };
 
 // One work-queue item: a row range of one query.
@@ -19,17 +19,18 @@ struct BatchItem {
   int64_t row_begin, row_end;
 };
 
-// dynamic shared memory of a batch CTA: miss list of T rows + a table of S
-// slots laid out for 64-bit keys (one launch serves both key widths)
-size_t gba_batch_smem_bytes(const QDesc& q, int S, int T);
 size_t gba_batch_static_smem();
 // which compiled signature serves q (queries with equal ids share a launch)
 int gba_batch_sig_id(const QDesc& q);
-// sets the kernel's dynamic shared-memory limit (outside any stream capture)
-cudaError_t gba_prepare_batch_preagg(const QDesc& proto, size_t smem);
-cudaError_t gba_launch_batch_preagg(const QDesc& proto, const BatchQ* d_qs, const BatchItem* d_items, int nitems,
-                                    unsigned* item_ctr, size_t smem, int sprobe, int T, int grid, int block,
-                                    cudaStream_t s);
+// Streaming aggregation (k_stream.cu): one persistent launch over work items
+// (d_items == nullptr: query d_qs[0] cut into items of item_rows rows, a
+// multiple of 256).  *item_ctr must be zero at launch.
+size_t gba_stream_smem_bytes(const QDesc& q, int S);
+int gba_stream_rows_per_chunk(const QDesc& q);
+cudaError_t gba_prepare_stream_agg(const QDesc& proto, size_t smem);
+cudaError_t gba_launch_stream_agg(const QDesc& proto, const BatchQ* d_qs, const BatchItem* d_items, int nitems,
+                                  int64_t item_rows, unsigned* item_ctr, size_t smem, int sprobe, int grid,
+                                  cudaStream_t s);
 // blk_prefix[i]: first block of query i (nq + 1 entries, blk_prefix[nq] = nblocks)
 cudaError_t gba_launch_batch_init(const BatchQ* d_qs, const int64_t* blk_prefix, int nq, int64_t nblocks,
                                   cudaStream_t s);

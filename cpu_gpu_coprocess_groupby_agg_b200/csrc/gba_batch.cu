@@ -4,9 +4,9 @@
 // estimator once for the whole batch).  Queries on the table strategy share
 // one launch sequence:
 //   k_batch_init      every query's HBM table (blocks dealt by table size)
-//   k_batch_preagg    one persistent launch per aggregate signature; CTAs pop
-//                     (query, row range) items from a device work queue,
-//                     longest first
+//   k_stream_agg      one persistent launch per aggregate signature and key
+//                     width; CTAs pop (query, row range) items from a device
+//                     work queue, query by query, largest queries first
 //   k_batch_compact   every query's groups into its own output
 // replayed from a CUDA graph while the batch's launch shapes repeat (the
 // per-query descriptors are copied from pinned host memory by the graph's
@@ -82,16 +82,18 @@ gba_status batch_predict(gba_context* ctx, const std::vector<QDesc>& qs, cudaStr
   return GBA_OK;
 }
 
-// Shared-table slots a batch CTA can hold for signature `proto` with tiles of
-// T rows and `bps` CTAs per SM.
-int batch_smem_slots(const gba_context* ctx, const QDesc& proto, int T, int bps) {
-  const size_t budget = size_t(ctx->max_smem_optin) / size_t(bps);
-  const size_t fixed = gba_batch_smem_bytes(proto, 0, T) + gba_batch_static_smem() + 1024;
+// Shared-table slots a streaming CTA can hold for a query (the kernel's
+// dynamic shared memory is the table alone).
+int batch_smem_slots(const gba_context* ctx, const QDesc& q) {
+  const size_t budget = size_t(ctx->max_smem_optin);
+  const size_t fixed = gba_stream_smem_bytes(q, 0) + gba_batch_static_smem() + 1024;
   if (budget <= fixed) return 0;
-  const size_t slot = 8 + 8 * size_t(proto.nwords);
+  const size_t slot = (q.key64 ? 8 : 4) + 8 * size_t(q.nwords);
   const int S = int(std::min<size_t>(16384, (budget - fixed) / slot));
   return S < 32 ? 0 : S;
 }
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
 }  // namespace
 
@@ -140,11 +142,10 @@ extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_
     if (st != GBA_OK) return st;
     ctx->stats.predicted_groups = std::accumulate(pred.begin(), pred.end(), 0.0);
   }
-  const int bps = k.blocks_per_sm == 2 ? 2 : 1;
-  const int block = 1024 / bps;
-  int T = k.tile_rows > 0 ? k.tile_rows : 8192;
-  T = std::min(32768, std::max(block, T / block * block));
-  const int sprobe = k.smem_probe_cap > 0 ? k.smem_probe_cap : 8;
+  // work items are cut at multiples of T rows (vector loads need aligned starts)
+  const int T = 2048;
+  // buckets probed in a shared table before a row goes to the HBM table
+  const int sprobe = k.smem_probe_cap > 0 ? k.smem_probe_cap : 2;
   for (int i = 0; i < nq; ++i) {
     ctx->est_skew = skew[i];
     gba_make_plan(ctx, qd[i], k, pred[i], &qi[i].p);
@@ -158,7 +159,7 @@ extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_
   std::vector<int> tq;  // table-strategy queries, group by group
   for (int i = 0; i < nq; ++i) {
     if (qi[i].strategy != GBA_STRATEGY_TABLE) continue;
-    const int sig = gba_batch_sig_id(qd[i]);
+    const int sig = 2 * gba_batch_sig_id(qd[i]) + (qd[i].key64 ? 1 : 0);  // one launch per signature and key width
     auto it = std::find_if(groups.begin(), groups.end(), [&](const Group& g) { return g.sig == sig; });
     if (it == groups.end()) {
       groups.push_back(Group{sig, qd[i], {}});
@@ -167,16 +168,18 @@ extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_
     it->members.push_back(i);
   }
   for (auto& g : groups) {
-    g.smem = gba_batch_smem_bytes(g.proto, 0, T);
+    g.smem = gba_stream_smem_bytes(g.proto, 0);
     for (int i : g.members) {
       // run-time signatures may differ in accumulator words per member
-      int S = qi[i].p.preagg ? batch_smem_slots(ctx, qd[i], T, bps) : 0;
+      int S = qi[i].p.preagg ? batch_smem_slots(ctx, qd[i]) : 0;
       if (k.smem_slots > 0) S = std::min(S, k.smem_slots);
       // a known-small group count needs only a small shared table (cheaper
       // to clear and flush per work item)
-      if (S > 0 && qi[i].pred > 0) S = std::min<int64_t>(S, std::max<int64_t>(256, int64_t(qi[i].pred * 2.0 + 31) / 32 * 32));
+      // (4 slots per expected group keep nearly every key in its home bucket)
+      if (S > 0 && qi[i].pred > 0) S = std::min<int64_t>(S, std::max<int64_t>(256, int64_t(qi[i].pred * 4.0 + 31) / 32 * 32));
+      S = S / 4 * 4;  // whole 16-byte buckets
       qi[i].S = S;
-      g.smem = std::max(g.smem, gba_batch_smem_bytes(qd[i], S, T));
+      g.smem = std::max(g.smem, gba_stream_smem_bytes(qd[i], S));
       qi[i].slot = int(tq.size());
       tq.push_back(i);
     }
@@ -191,7 +194,7 @@ extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_
   // and the random table updates spilled from L2 to DRAM).  A query's rows
   // are cut into about one item per CTA (at least one tile, at most
   // item_rows or 2^20 rows), so one query occupies the whole grid.
-  const int grid_max = ctx->sms * bps;
+  const int grid_max = ctx->sms;
   const int64_t item_cap = k.item_rows > 0 ? std::max<int64_t>(T, int64_t(k.item_rows)) : (int64_t(1) << 20);
   std::vector<BatchItem> items;
   for (auto& g : groups) {
@@ -256,6 +259,12 @@ extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_
       b.out.count = reinterpret_cast<unsigned long long*>(d + o_stat + 16 * size_t(j) + 8);
       b.flags = reinterpret_cast<unsigned*>(d + o_stat + 16 * size_t(j));
       b.S = qi[i].S;
+      bool vec = aligned16(qd[i].keys);
+      for (int c = 0; c < qd[i].ncols; ++c) vec = vec && aligned16(qd[i].cols[c]);
+      // bits 8..15: buckets probed per row; a table the query's groups will
+      // overfill keeps only what reaches its home bucket
+      const int nbk = (qi[i].S > 0 && qi[i].pred > 2.0 * qi[i].S) ? 1 : 0;
+      b.pad = (vec ? 1 : 0) | (nbk << 8);  // bit 0: columns allow vector loads
       hq[j] = b;
     }
     if (!items.empty()) std::memcpy(h + o_items, items.data(), sizeof(BatchItem) * items.size());
@@ -270,8 +279,11 @@ extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_
   // with timing on, events around the three kernel roles (recorded as graph
   // nodes when captured): [0] table init, [1] pre-aggregation, [2] compaction
   const bool timing = k.timing != 0;
+  const bool as_graph = k.use_graph != 0;
   auto mark = [&](int i, cudaStream_t cs) -> cudaError_t {
-    return timing ? cudaEventRecordWithFlags(ctx->tev[i], cs, cudaEventRecordExternal) : cudaSuccess;
+    if (!timing) return cudaSuccess;
+    // inside a capture the event record must be an external graph node
+    return as_graph ? cudaEventRecordWithFlags(ctx->tev[i], cs, cudaEventRecordExternal) : cudaEventRecord(ctx->tev[i], cs);
   };
   auto enqueue = [&](cudaStream_t cs) -> cudaError_t {
     cudaError_t e = cudaMemcpyAsync(d, h, desc_bytes, cudaMemcpyHostToDevice, cs);
@@ -281,8 +293,8 @@ extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_
       e = gba_launch_batch_init(d_qs, reinterpret_cast<const int64_t*>(d + o_ipre), nt, ipre[nt], cs);
     if (e == cudaSuccess) e = mark(1, cs);
     for (int g = 0; g < ng && e == cudaSuccess; ++g)
-      e = gba_launch_batch_preagg(groups[g].proto, d_qs, d_items + groups[g].item_begin, int(groups[g].nitems),
-                                  d_ctr + g, groups[g].smem, sprobe, T, groups[g].grid, block, cs);
+      e = gba_launch_stream_agg(groups[g].proto, d_qs, d_items + groups[g].item_begin, int(groups[g].nitems), 0,
+                                d_ctr + g, groups[g].smem, sprobe, groups[g].grid, cs);
     if (e == cudaSuccess) e = mark(2, cs);
     if (e == cudaSuccess)
       e = gba_launch_batch_compact(d_qs, reinterpret_cast<const int64_t*>(d + o_cpre), nt, cpre[nt], cs);
@@ -292,8 +304,8 @@ extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_
   };
   if (nt > 0) {
     for (int g = 0; g < ng; ++g)
-      GBA_CUDA_TRY(ctx, gba_prepare_batch_preagg(groups[g].proto, groups[g].smem));
-    if (k.use_graph != 0) {
+      GBA_CUDA_TRY(ctx, gba_prepare_stream_agg(groups[g].proto, groups[g].smem));
+    if (as_graph) {
       // the graph depends only on launch shapes and buffer addresses
       std::vector<int64_t> key = {nt,
                                   int64_t(items.size()),
@@ -303,9 +315,7 @@ extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_
                                   int64_t(stat_bytes),
                                   int64_t(reinterpret_cast<uintptr_t>(d)),
                                   int64_t(reinterpret_cast<uintptr_t>(h)),
-                                  T,
                                   sprobe,
-                                  block,
                                   timing ? 1 : 0};
       for (const auto& g : groups) {
         key.push_back(g.sig);

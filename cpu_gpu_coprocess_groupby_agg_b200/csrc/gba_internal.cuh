@@ -115,18 +115,47 @@ __device__ __forceinline__ void acc_atomic(int op, unsigned long long* p, unsign
   }
 }
 
-// HBM/L2 accumulator update: 64-bit atomics (L2 runs 64- and 32-bit atomics
-// at the same rate); MIN/MAX read first and skip rows that cannot improve.
+// Fire-and-forget reductions into global memory.  The address space is
+// stated explicitly: a table pointer read from shared memory (a batch kernel's
+// query descriptor) is a generic pointer to the compiler, and a generic
+// atomicAdd whose result is unused still compiles to a returning atomic, which
+// the warp then waits for.
+__device__ __forceinline__ void red_add_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "l"(v) : "memory");
+}
+__device__ __forceinline__ void red_min_s64(unsigned long long* p, unsigned long long v) {
+  asm volatile("red.relaxed.gpu.global.min.s64 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "l"(v) : "memory");
+}
+__device__ __forceinline__ void red_max_s64(unsigned long long* p, unsigned long long v) {
+  asm volatile("red.relaxed.gpu.global.max.s64 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "l"(v) : "memory");
+}
+__device__ __forceinline__ void red_add_f64(unsigned long long* p, unsigned long long v) {
+  asm volatile("red.relaxed.gpu.global.add.f64 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "d"(__longlong_as_double(v))
+               : "memory");
+}
+__device__ __forceinline__ unsigned long long cas_global_u64(unsigned long long* p, unsigned long long cmp,
+                                                             unsigned long long val) {
+  unsigned long long old;
+  asm volatile("atom.relaxed.gpu.global.cas.b64 %0, [%1], %2, %3;"
+               : "=l"(old)
+               : "l"(__cvta_generic_to_global(p)), "l"(cmp), "l"(val)
+               : "memory");
+  return old;
+}
+
+// HBM/L2 accumulator update: 64-bit reductions (L2 runs 64- and 32-bit
+// atomics at the same rate); MIN/MAX read first and skip rows that cannot
+// improve.
 __device__ __forceinline__ void global_acc(int op, unsigned long long* p, unsigned long long v) {
   switch (op) {
     case ACC_MIN_I:
-      if ((long long)v < (long long)__ldcg(p)) atomicMin(reinterpret_cast<long long*>(p), (long long)v);
+      if ((long long)v < (long long)__ldcg(p)) red_min_s64(p, v);
       break;
     case ACC_MAX_I:
-      if ((long long)v > (long long)__ldcg(p)) atomicMax(reinterpret_cast<long long*>(p), (long long)v);
+      if ((long long)v > (long long)__ldcg(p)) red_max_s64(p, v);
       break;
-    case ACC_ADD_F: atomicAdd(reinterpret_cast<double*>(p), __longlong_as_double(v)); break;
-    default: atomicAdd(p, v);
+    case ACC_ADD_F: red_add_f64(p, v); break;
+    default: red_add_u64(p, v);
   }
 }
 
@@ -155,7 +184,7 @@ __device__ __forceinline__ void gtable_insert(const GTable& t, const QDesc& q, u
       unsigned long long cur = __ldcg(slotp);  // L2 (coherent point), no L1
       if (cur == key) break;
       if (cur == EMPTY64) {
-        unsigned long long prev = atomicCAS(slotp, EMPTY64, key);
+        unsigned long long prev = cas_global_u64(slotp, EMPTY64, key);
         if (prev == EMPTY64 || prev == key) break;
       }
       if (++p >= t.probe_cap) {
@@ -185,7 +214,7 @@ __device__ __forceinline__ void gtable_finish(const GTable& t, const QDesc& q, u
   for (;;) {
     if (cur == key) break;
     if (cur == EMPTY64) {
-      unsigned long long prev = atomicCAS(slotp, EMPTY64, key);
+      unsigned long long prev = cas_global_u64(slotp, EMPTY64, key);
       if (prev == EMPTY64 || prev == key) break;
     }
     if (++p >= t.probe_cap) {

@@ -4,8 +4,7 @@
 //
 // A server owns `lanes` workers.  Each lane is a host thread with its own CUDA
 // stream and library context, so lanes run on the device at the same time and
-// each context keeps its tables, workspace and batch graph resident between
-// requests.  Requests (device columns in, device columns out) enter one FIFO
+// each context keeps its tables and workspace resident between requests.  Requests (device columns in, device columns out) enter one FIFO
 // queue.  A lane that comes free takes work from the head of the queue:
 //   * a request of more than batch_rows rows runs alone (gba_groupby);
 //   * otherwise the lane takes the head and every following small request
@@ -166,11 +165,6 @@ static void lane_main(gba_server* sv, int lane) {
         cudaFree(ctx->ws);
         ctx->ws = nullptr;
         ctx->ws_bytes = 0;
-        if (ctx->batch_exec) {  // its graph points into the freed workspace
-          cudaGraphExecDestroy(ctx->batch_exec);
-          ctx->batch_exec = nullptr;
-          ctx->batch_key.clear();
-        }
         mine = ctx_resident_bytes(ctx);
       }
       sv->resident[lane] = mine;
@@ -213,6 +207,11 @@ extern "C" gba_status gba_server_create(gba_server** out, const gba_server_confi
   if (c.memory_budget <= 0) c.memory_budget = int64_t(120) << 30;
   if (c.max_batch <= 0) c.max_batch = 64;
   if (c.batch_rows <= 0) c.batch_rows = int64_t(1) << 24;
+  // Lanes do not capture graphs: each batch a lane forms has a new shape (so a
+  // captured graph would rarely be replayed), and a capture on one lane's
+  // thread must not meet another lane's workspace growth, whose cudaFree
+  // synchronises the device.
+  c.knobs.use_graph = 0;
   gba_server* sv = new gba_server();
   sv->cfg = c;
   gba_status st = gba_create(&sv->admin, c.device);

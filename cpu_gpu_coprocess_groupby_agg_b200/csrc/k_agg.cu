@@ -355,61 +355,8 @@ __global__ void k_compact(GTable t, QDesc q, OutDesc o) {
   }
 }
 
-// ---- batched queries ----------------------------------------------------------------
-// One persistent launch per aggregate signature of a batch (both key widths):
-// CTAs pop (query, row range) items from a device work queue; each item is
-// aggregated through the CTA's shared table (sized per query, possibly empty)
-// and flushed into that query's HBM table, then the CTA takes the next item.
-template <bool K64, typename Sig>
-__device__ __forceinline__ void batch_item(const BatchQ& bq, const BatchItem& item, unsigned char* tbase,
-                                           unsigned short* miss, unsigned* s_nmiss, int sprobe, int T) {
-  const QDesc& q = bq.q;
-  const size_t coff[GBA_MAX_COLS] = {0, 0, 0, 0};
-  const SmemTable<K64> st = smem_table_carve<K64>(tbase, bq.S, q.nwords);
-  smem_table_init<K64, Sig>(st, q);
-  __syncthreads();
-  for (int64_t r0 = item.row_begin; r0 < item.row_end; r0 += T) {
-    const int rows = int(item.row_end - r0 < int64_t(T) ? item.row_end - r0 : int64_t(T));
-    tile_two_phase<K64, Sig>(q, bq.gt, st, bq.S, sprobe, 0, false, nullptr, coff, r0, rows, T, miss, s_nmiss,
-                             bq.flags);
-    __syncthreads();
-    if (threadIdx.x == 0) *s_nmiss = 0;
-    __syncthreads();
-  }
-  smem_flush_to_gtable<K64, Sig>(q, bq.gt, st, bq.flags);
-}
-
-template <typename Sig>
-__global__ void __launch_bounds__(1024, 1) k_batch_preagg(const BatchQ* qs, const BatchItem* items, int nitems,
-                                                          unsigned* item_ctr, int sprobe, int T) {
-  extern __shared__ __align__(128) unsigned char smem[];
-  unsigned short* miss = reinterpret_cast<unsigned short*>(smem);
-  unsigned char* tbase = smem + align16(size_t(T) * 2);
-  __shared__ int s_item;
-  __shared__ unsigned s_nmiss;
-  __shared__ __align__(16) BatchQ s_q;
-  const int tid = threadIdx.x;
-  for (;;) {
-    if (tid == 0) {
-      s_item = int(atomicAdd(item_ctr, 1u));
-      s_nmiss = 0;
-    }
-    __syncthreads();
-    const int it = s_item;
-    if (it >= nitems) break;
-    const BatchItem item = items[it];
-    {
-      const unsigned* src = reinterpret_cast<const unsigned*>(qs + item.qi);
-      unsigned* dst = reinterpret_cast<unsigned*>(&s_q);
-      for (int w = tid; w < int(sizeof(BatchQ) / 4); w += blockDim.x) dst[w] = src[w];
-    }
-    __syncthreads();
-    if (s_q.q.key64) batch_item<true, Sig>(s_q, item, tbase, miss, &s_nmiss, sprobe, T);
-    else batch_item<false, Sig>(s_q, item, tbase, miss, &s_nmiss, sprobe, T);
-    __syncthreads();  // s_q and the tables are rewritten by the next item
-  }
-}
-
+// ---- batched queries: table init and compaction (the aggregation itself is
+// k_stream.cu's streaming kernel) ----
 // table init for every query of a batch: blocks are dealt to queries in
 // proportion to their table sizes (blk_prefix[i] = first block of query i)
 __device__ __forceinline__ int batch_query_of_block(const int64_t* blk_prefix, int nq, int64_t b) {
@@ -545,10 +492,6 @@ cudaError_t gba_launch_compact(const GTable& t, const QDesc& q, const OutDesc& o
 }
 
 // ---------------------------------------------------------------------------
-size_t gba_batch_smem_bytes(const QDesc& q, int S, int T) {
-  // sized for 64-bit keys: one launch serves both key widths
-  return align16(size_t(T) * 2) + smem_table_bytes(S, 1, q.nwords) + 64;
-}
 size_t gba_batch_static_smem() { return sizeof(BatchQ) + 64; }
 
 int gba_batch_sig_id(const QDesc& q) {
@@ -558,24 +501,6 @@ int gba_batch_sig_id(const QDesc& q) {
     return cudaSuccess;
   });
   return id;
-}
-
-cudaError_t gba_prepare_batch_preagg(const QDesc& proto, size_t smem) {
-  return gba_dispatch_sig(proto, [&](auto, auto sig) -> cudaError_t {
-    using Sig = decltype(sig);
-    return cudaFuncSetAttribute(k_batch_preagg<Sig>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-  });
-}
-
-cudaError_t gba_launch_batch_preagg(const QDesc& proto, const BatchQ* d_qs, const BatchItem* d_items, int nitems,
-                                    unsigned* item_ctr, size_t smem, int sprobe, int T, int grid, int block,
-                                    cudaStream_t s) {
-  if (nitems <= 0) return cudaSuccess;
-  return gba_dispatch_sig(proto, [&](auto, auto sig) -> cudaError_t {
-    using Sig = decltype(sig);
-    k_batch_preagg<Sig><<<grid, block, smem, s>>>(d_qs, d_items, nitems, item_ctr, sprobe, T);
-    return cudaGetLastError();
-  });
 }
 
 cudaError_t gba_launch_batch_init(const BatchQ* d_qs, const int64_t* blk_prefix, int nq, int64_t nblocks,

@@ -213,7 +213,8 @@ gba_status gba_groupby_partition_u32(gba_context* ctx, const uint32_t* keys, con
  * No counterpart in the reference (one query per call).  A server runs `lanes`
  * host workers, each with its own CUDA stream and context, so their work
  * overlaps on the device and each keeps its tables and workspace resident
- * between requests.  Submitted requests (device columns in, device output
+ * between requests (lanes run without CUDA graphs: knobs.use_graph is
+ * ignored).  Submitted requests (device columns in, device output
  * columns out, as gba_groupby) queue in arrival order; a free lane takes the
  * head of the queue and, when it is small (n_rows <= batch_rows), every
  * following small request (up to max_batch) that still fits the budget, and
