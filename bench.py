@@ -98,6 +98,14 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def max_over_ranks(x: float, dist, device) -> float:
+    """The largest x over all ranks (the job's time is its slowest rank's)."""
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -187,12 +195,16 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batch", choices=["batch", "skewed", "small", "highcard"])
+    ap.add_argument("--workload", default="batch", choices=["batch", "skewed", "small", "highcard", "serve"])
+    ap.add_argument("--duration", type=float, default=10.0, help="serve: seconds of Poisson arrivals")
+    ap.add_argument("--rate", type=float, default=2000.0, help="serve: arrivals per second")
+    ap.add_argument("--max-inflight", type=int, default=256, help="serve: client-side cap on requests in flight")
     ap.add_argument("--sizing", default="learned", choices=["plain", "learned"])
     ap.add_argument("--no-plain-compare", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--knob", action="append", default=[], help="name=value knob override")
+    ap.add_argument("--no-autotune", action="store_true", help="batch: default knobs instead of gba_autotune's")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     ws, rank, local = dist_setup()
@@ -213,6 +225,8 @@ def main():
     from cpu_gpu_coprocess_groupby_agg_b200 import estimator as E
     if args.workload == "batch":
         return run_batch(args, ws, rank, local, pg)
+    if args.workload == "serve":
+        return run_serve(args, ws, rank, local, pg)
     w = get_workload(args.workload)
     ctx = Context(local)
     if args.sizing == "learned" and not E.load_default(ctx):
@@ -253,9 +267,7 @@ def main():
         pg.barrier()
     elapsed = ev0.elapsed_time(ev1)
     if pg:
-        t = torch.tensor([elapsed], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        elapsed = float(t.item())
+        elapsed = max_over_ranks(elapsed, pg, "cuda")
     ms_step = elapsed / args.steps
     value = ws * w.n / (ms_step / 1e3) / 1e9
     G = res.n_groups
@@ -349,9 +361,28 @@ def run_batch(args, ws, rank, local, pg):
     stream = torch.cuda.current_stream()
     base = {"timing": 1}
     base.update(_knob_overrides(args))
+    # knobs per sizing: the autotuner's choice on this batch (outside the timed
+    # region), unless --no-autotune or knob overrides are given
+    tuned = {}
+
+    def knobs_for(sizing):
+        if sizing in tuned:
+            return tuned[sizing][0]
+        kn = make_knobs(**dict(base, sizing=sizing))
+        if not args.no_autotune and not args.knob:
+            best, ms = ctx.autotune(dq, knobs=kn, outs=outs, stream=stream)
+            best.timing = 1
+            tuned[sizing] = (best, ms)
+            return best
+        tuned[sizing] = (kn, None)
+        return kn
+
+    def knob_summary(k):
+        return {"learned_load": k.learned_load, "load_factor": k.load_factor, "item_rows": k.item_rows,
+                "smem_probe_cap": k.smem_probe_cap}
 
     def timed(sizing, steps, clocks=False):
-        knobs = make_knobs(**dict(base, sizing=sizing))
+        knobs = knobs_for(sizing)
         for _ in range(args.warmup):
             res = ctx.groupby_batch(dq, knobs=knobs, outs=outs, stream=stream)
         if pg:
@@ -373,9 +404,7 @@ def run_batch(args, ws, rank, local, pg):
             pg.barrier()
         el = e0.elapsed_time(e1)
         if pg:
-            t = torch.tensor([el], device="cuda")
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            el = float(t.item())
+            el = max_over_ranks(el, pg, "cuda")
         return el / steps, main_ms / steps, main_bytes / steps, launches, res, clk.summary()
 
     ms_step, main_ms, main_bytes, launches, res, clocks = timed(args.sizing, args.steps)
@@ -398,7 +427,10 @@ def run_batch(args, ws, rank, local, pg):
                    "strategy_mix": st["strategy"], "table_slots_total": st["table_slots"],
                    "predicted_groups_total": round(st["predicted_groups"], 1),
                    "l2": "inputs larger than L2 (no flush needed)", "parallelism": f"replicas x{ws}",
-                   "launch": "one gba_groupby_batch call per step (CUDA graph replay)"},
+                   "launch": "one gba_groupby_batch call per step (CUDA graph replay)",
+                   "knobs": knob_summary(tuned[args.sizing][0]),
+                   "knobs_from": "gba_autotune on this batch before timing" if tuned[args.sizing][1] is not None
+                   else "defaults / --knob"},
         "whole_step_hbm_gbs": round(in_bytes / (ms_step / 1e3) / 1e9, 1),
         "roofline": {"bound": "hbm", "kernel": "k_stream_agg (+ k_part_agg of partition-strategy queries)",
                      "achieved": round(achieved, 1) if achieved else None, "peak": peak, "unit": "GB/s",
@@ -412,9 +444,10 @@ def run_batch(args, ws, rank, local, pg):
         line["plain_sizing"] = {"value": round(ws * total_rows / (pms / 1e3) / 1e9, 4), "unit": "G rows/s",
                                 "ms_per_step": round(pms, 4), "strategy_mix": pres[0].stats["strategy"],
                                 "table_slots_total": pres[0].stats["table_slots"],
+                                "knobs": knob_summary(tuned["plain"][0]),
                                 "learned_speedup": round(pms / ms_step, 3)}
     if not args.no_e2e and rank == 0:
-        line["e2e"] = batch_e2e(ctx, allq, dq, outs, make_knobs(**dict(base, sizing=args.sizing)), args)
+        line["e2e"] = batch_e2e(ctx, allq, dq, outs, knobs_for(args.sizing), args)
     if not args.no_cpu_baseline and rank == 0 and ws == 1:
         sys.path.insert(0, str(ROOT / "oracle"))
         import cpu_oracle as O
@@ -437,6 +470,107 @@ def run_batch(args, ws, rank, local, pg):
     if pg:
         pg.barrier()
         pg.destroy_process_group()
+    return 0
+
+
+SERVE_NAME = "serve_poisson_batch256shapes+5%_2^27rows_2^24keys"
+
+
+def run_serve(args, ws, rank, local, pg):
+    """Serving stream: Poisson arrivals of queries drawn from the 256-query
+    batch's shapes, plus 5% large queries (2^27 rows over 2^24 int64 ids), into
+    a gba_server with a 120 GiB budget; inputs device-resident.  Reported: the
+    sustained rows/s (rows of finished requests / time from the first arrival
+    to the last completion) and p50/p99 latency, learned and plain sizing.
+    Timing is host wall clock (a latency is submit -> result on the device)."""
+    import numpy as np
+    import torch
+    from cpu_gpu_coprocess_groupby_agg_b200 import Server, gen_device, make_knobs
+    from cpu_gpu_coprocess_groupby_agg_b200 import estimator as E
+    from cpu_gpu_coprocess_groupby_agg_b200 import workloads as W
+    small = W.batch_queries()
+    large = [W.large_serving_query(seed=900 + i) for i in range(2)]
+    pool = small + large
+    data = []
+    for q in pool:
+        k, c = gen_device(q.spec, q.n, device=local)
+        data.append((k, c, q.aggs))
+    torch.cuda.synchronize()
+    free = [[] for _ in pool]
+
+    def out_for(i):
+        if free[i]:
+            return free[i].pop()
+        q = pool[i]
+        cap = min(q.n, q.spec.ndv) + 1
+        return (torch.empty(cap, dtype=data[i][0].dtype, device=data[i][0].device),
+                [torch.empty(cap, dtype=torch.int64, device=data[i][0].device) for _ in q.aggs])
+
+    def one_run(sizing, seed):
+        rng = np.random.default_rng(seed)
+        n_arr = int(args.rate * args.duration)
+        gaps = rng.exponential(1.0 / args.rate, n_arr)
+        kinds = np.where(rng.random(n_arr) < 0.05, rng.integers(len(small), len(pool), n_arr),
+                         rng.integers(0, len(small), n_arr))
+        sv = Server(local, lanes=4, memory_budget=120 << 30, max_batch=64, batch_rows=1 << 24,
+                    knobs=make_knobs(sizing=sizing),
+                    estimator_params=E.load_weights() if sizing == "learned" else None)
+        inflight = {}
+        infos = []
+
+        def collect(timeout):
+            info = sv.next_done(timeout)
+            while info is not None:
+                i, o, lag = inflight.pop(info.ticket)
+                free[i].append(o)
+                infos.append((info, pool[i].n, lag))
+                info = sv.next_done(0.0)
+        t0 = time.perf_counter()
+        t_next = t0
+        for j in range(n_arr):
+            t_next += gaps[j]
+            while True:
+                now = time.perf_counter()
+                if now >= t_next and len(inflight) < args.max_inflight:
+                    break
+                collect(min(0.002, max(t_next - now, 0.0005)))
+            i = int(kinds[j])
+            o = out_for(i)
+            t = sv.submit(data[i][0], data[i][1], data[i][2], o)
+            # a request held back by the client's in-flight cap waits from its
+            # scheduled arrival: that wait is part of its latency
+            inflight[t] = (i, o, (time.perf_counter() - t_next) * 1e3)
+        while inflight:
+            collect(1.0)
+        t_end = time.perf_counter()
+        sv.close()
+        bad = [x for x, _, _ in infos if x.status != 0]
+        if bad:
+            raise SystemExit(f"serving: {len(bad)} requests failed, first status {bad[0].status}")
+        lat = np.array([x.latency_ms + lag for x, _, lag in infos])
+        rows = sum(n for _, n, _ in infos)
+        return {"value": round(rows / (t_end - t0) / 1e9, 4), "unit": "G rows/s", "requests": len(infos),
+                "seconds": round(t_end - t0, 3), "offered_seconds": round(float(np.sum(gaps)), 3),
+                "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                "mean_batch": round(float(np.mean([x.batch_size for x, _, _ in infos])), 2)}
+
+    learned = one_run("learned", 5)
+    plain = one_run("plain", 5)
+    line = {
+        "metric": "groupby_rows_per_s", "value": learned["value"], "unit": "G rows/s", "n_gpus": ws,
+        "steps": learned["requests"], "warmup": 0, "ms_per_step": None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "data": "synthetic (seeded PCG32 generator, generated on device)",
+        "config": {"workload": SERVE_NAME, "rate_per_s": args.rate, "duration_s": args.duration, "lanes": 4,
+                   "max_inflight": args.max_inflight,
+                   "latency": "scheduled arrival -> result complete (client-side wait included)",
+                   "memory_budget_gib": 120, "max_batch": 64, "sizing": "learned",
+                   "timer": "host wall clock, first arrival to last completion"},
+        "latency_ms": {"p50": learned["p50_ms"], "p99": learned["p99_ms"]},
+        "serve": learned, "plain_sizing": plain,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     return 0
 
 

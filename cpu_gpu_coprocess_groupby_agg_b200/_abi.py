@@ -76,6 +76,7 @@ class Knobs(C.Structure):
         ("timing", C.c_int32),
         ("use_graph", C.c_int32),
         ("item_rows", C.c_int32),
+        ("learned_load", C.c_double),
     ]
 
 
@@ -151,6 +152,8 @@ SIGNATURES = {
                                     C.POINTER(C.c_int64)]),
     "gba_groupby_noalloc": (C.c_int, [_P, C.POINTER(Query), C.POINTER(Output), _P, C.POINTER(C.c_int64)]),
     "gba_groupby_partition_u32": (C.c_int, [_P, _P, _P, C.c_int64, C.c_int32, _P, _P, _P, _P]),
+    "gba_autotune": (C.c_int, [_P, C.c_int32, C.POINTER(Query), C.POINTER(Output), C.POINTER(Knobs), _P, C.c_int32,
+                               C.POINTER(Knobs), C.POINTER(C.c_double)]),
     "gba_server_default_config": (None, [C.POINTER(ServerConfig)]),
     "gba_server_create": (C.c_int, [C.POINTER(_P), C.POINTER(ServerConfig)]),
     "gba_server_estimator_load": (C.c_int, [_P, C.POINTER(C.c_float)]),

@@ -167,6 +167,41 @@ class Context:
             outs.append((okeys, oaggs))
         return outs
 
+    def _batch_arrays(self, queries: Sequence, outs):
+        nq = len(queries)
+        qarr = (A.Query * max(nq, 1))()
+        oarr = (A.Output * max(nq, 1))()
+        for i, q in enumerate(queries):
+            keys, cols, aggs = q[0], q[1], q[2]
+            uk = bool(q[3]) if len(q) > 3 else False
+            uc = list(q[4]) if len(q) > 4 else []
+            uc += [False] * (len(cols) - len(uc))
+            if not keys.is_cuda:
+                raise ValueError("device tensors expected")
+            col_specs = [(c.data_ptr(), _torch_type(c, u)) for c, u in zip(cols, uc)]
+            qarr[i] = build_query(keys.numel(), keys.data_ptr(), _torch_type(keys, uk), col_specs, parse_aggs(aggs))
+            okeys, oaggs = outs[i]
+            oarr[i].keys = okeys.data_ptr()
+            for a, t in enumerate(oaggs):
+                oarr[i].aggs[a] = t.data_ptr()
+            oarr[i].capacity = okeys.numel()
+        return qarr, oarr
+
+    def autotune(self, queries: Sequence, knobs=None, outs=None, stream=None, reps: int = 2):
+        """gba_autotune over device queries (one query: gba_groupby knobs; several:
+        gba_groupby_batch knobs).  Returns (best knobs, best ms per call)."""
+        import torch
+        if outs is None:
+            outs = self.batch_outputs(queries)
+        qarr, oarr = self._batch_arrays(queries, outs)
+        kn = knobs if isinstance(knobs, A.Knobs) else make_knobs(**(knobs or {}))
+        best = A.Knobs()
+        ms = C.c_double(0)
+        s = stream if stream is not None else torch.cuda.current_stream(queries[0][0].device)
+        A.check(self._lib.gba_autotune(self._h, len(queries), qarr, oarr, C.byref(kn), C.c_void_p(s.cuda_stream),
+                                       reps, C.byref(best), C.byref(ms)), self._h)
+        return best, ms.value
+
     def groupby_batch(self, queries: Sequence, knobs=None, stream=None, outs=None) -> list:
         """Many independent queries in one call (gba_groupby_batch).
 

@@ -291,6 +291,8 @@ __device__ __forceinline__ void stream_chunk(const BatchQ& bq, const SmemTable<K
   }
   if (miss == 0) return;
   // HBM-table pass: every missed row's home-slot load first, then the inserts
+  // (measured: also loading the slot after the home slot, to place displaced
+  // keys without a second round trip, costs more in L2 requests than it saves)
   constexpr int stride = 1 + NA;
   uint64_t home[R];
   unsigned long long cur[R];

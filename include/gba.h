@@ -111,6 +111,7 @@ typedef struct gba_knobs {
   int32_t timing;         /* 1: time each kernel with CUDA events (gba_stats.kernel_ms) */
   int32_t use_graph;      /* batch: -1 auto (on), 0 off, 1 on: replay the launch sequence as a CUDA graph */
   int32_t item_rows;      /* batch: rows per work-queue item (0 = auto) */
+  double learned_load;    /* learned sizing: HBM table load at the predicted group count (0 = auto, 0.35) */
 } gba_knobs;
 
 /* What the last call on a context did. */
@@ -208,6 +209,18 @@ gba_status gba_groupby_noalloc(gba_context* ctx, const gba_query* q, const gba_o
 gba_status gba_groupby_partition_u32(gba_context* ctx, const uint32_t* keys, const uint32_t* vals, int64_t n_rows,
                                      int32_t P, uint32_t* out_keys, uint32_t* out_vals, uint64_t* part_offsets,
                                      void* stream);
+
+/* Autotuner: times the caller's own queries (device columns, as gba_groupby /
+ * gba_groupby_batch take them) under candidate knobs by coordinate descent
+ * from `base` and writes the fastest setting to *best (and its mean time per
+ * call in ms to *best_ms).  One query: tile_rows, blocks_per_sm,
+ * partition_bits and the HBM table load; a batch (n_queries > 1): the table
+ * load, item_rows and smem_probe_cap.  The load tuned is learned_load under
+ * learned sizing, load_factor otherwise.  Every trial writes the outputs; rerun
+ * with *best for the result.  No counterpart in the reference (its tile
+ * length and partition count are constants, test/test.cu:94-98). */
+gba_status gba_autotune(gba_context* ctx, int32_t n_queries, const gba_query* qs, const gba_output* outs,
+                        const gba_knobs* base, void* stream, int32_t reps, gba_knobs* best, double* best_ms);
 
 /* ---- serving: continuous batching under a device-memory budget ----------
  * No counterpart in the reference (one query per call).  A server runs `lanes`
