@@ -381,10 +381,12 @@ def run_batch(args, ws, rank, local, pg):
         return {"learned_load": k.learned_load, "load_factor": k.load_factor, "item_rows": k.item_rows,
                 "smem_probe_cap": k.smem_probe_cap}
 
+    pb = ctx.prepare_batch(dq, outs)
+
     def timed(sizing, steps, clocks=False):
         knobs = knobs_for(sizing)
         for _ in range(args.warmup):
-            res = ctx.groupby_batch(dq, knobs=knobs, outs=outs, stream=stream)
+            ctx.run_batch(pb, knobs=knobs, stream=stream)
         if pg:
             pg.barrier()
         torch.cuda.synchronize()
@@ -393,8 +395,8 @@ def run_batch(args, ws, rank, local, pg):
         with ClockSampler(local) as clk:
             e0.record(stream)
             for _ in range(steps):
-                res = ctx.groupby_batch(dq, knobs=knobs, outs=outs, stream=stream)
-                st = res[0].stats
+                ng = ctx.run_batch(pb, knobs=knobs, stream=stream)
+                st = ctx.stats()
                 main_ms += st["kernel_ms"][1]
                 main_bytes += st["main_bytes"]
                 launches += st["kernel_launches"]
@@ -405,12 +407,12 @@ def run_batch(args, ws, rank, local, pg):
         el = e0.elapsed_time(e1)
         if pg:
             el = max_over_ranks(el, pg, "cuda")
-        return el / steps, main_ms / steps, main_bytes / steps, launches, res, clk.summary()
+        return el / steps, main_ms / steps, main_bytes / steps, launches, (ng, st), clk.summary()
 
     ms_step, main_ms, main_bytes, launches, res, clocks = timed(args.sizing, args.steps)
     value = ws * total_rows / (ms_step / 1e3) / 1e9
-    st = res[0].stats
-    groups = sum(r.n_groups for r in res)
+    ng, st = res
+    groups = int(ng.sum())
     peak, peak_kind = peaks()
     achieved = main_bytes / (main_ms / 1e3) / 1e9 if main_ms > 0 else None
     traffic = None
@@ -442,8 +444,8 @@ def run_batch(args, ws, rank, local, pg):
     if args.sizing == "learned" and not args.no_plain_compare:
         pms, pmain, pbytes, _, pres, _ = timed("plain", max(3, min(args.steps, 5)))
         line["plain_sizing"] = {"value": round(ws * total_rows / (pms / 1e3) / 1e9, 4), "unit": "G rows/s",
-                                "ms_per_step": round(pms, 4), "strategy_mix": pres[0].stats["strategy"],
-                                "table_slots_total": pres[0].stats["table_slots"],
+                                "ms_per_step": round(pms, 4), "strategy_mix": pres[1]["strategy"],
+                                "table_slots_total": pres[1]["table_slots"],
                                 "knobs": knob_summary(tuned["plain"][0]),
                                 "learned_speedup": round(pms / ms_step, 3)}
     if not args.no_e2e and rank == 0:
@@ -543,10 +545,11 @@ def run_serve(args, ws, rank, local, pg):
         while inflight:
             collect(1.0)
         t_end = time.perf_counter()
+        err = sv._lib.gba_server_last_error(sv._h).decode()
         sv.close()
         bad = [x for x, _, _ in infos if x.status != 0]
         if bad:
-            raise SystemExit(f"serving: {len(bad)} requests failed, first status {bad[0].status}")
+            raise SystemExit(f"serving: {len(bad)} requests failed, first status {bad[0].status}: {err}")
         lat = np.array([x.latency_ms + lag for x, _, lag in infos])
         rows = sum(n for _, n, _ in infos)
         return {"value": round(rows / (t_end - t0) / 1e9, 4), "unit": "G rows/s", "requests": len(infos),

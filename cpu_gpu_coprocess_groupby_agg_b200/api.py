@@ -73,6 +73,15 @@ def build_query(n: int, key_ptr: int, key_type: int, cols: Sequence[tuple[int, i
 
 
 @dataclass
+class PreparedBatch:
+    queries: Sequence
+    outs: list
+    qarr: object
+    oarr: object
+    ng: object
+
+
+@dataclass
 class Result:
     keys: object
     aggs: list
@@ -186,6 +195,26 @@ class Context:
                 oarr[i].aggs[a] = t.data_ptr()
             oarr[i].capacity = okeys.numel()
         return qarr, oarr
+
+    def prepare_batch(self, queries: Sequence, outs=None) -> "PreparedBatch":
+        """Packs a batch's query and output descriptors once, for repeated
+        run_batch calls on the same tensors (the per-call Python packing of
+        hundreds of descriptors otherwise costs milliseconds of host time)."""
+        if outs is None:
+            outs = self.batch_outputs(queries)
+        qarr, oarr = self._batch_arrays(queries, outs)
+        return PreparedBatch(queries, outs, qarr, oarr, (C.c_int64 * max(len(queries), 1))())
+
+    def run_batch(self, pb: "PreparedBatch", knobs=None, stream=None) -> np.ndarray:
+        """gba_groupby_batch on a prepared batch; returns the group counts
+        (numpy int64, one per query).  Query i's groups are
+        pb.outs[i][0][:n], [a[:n] for a in pb.outs[i][1]]."""
+        import torch
+        kn = knobs if isinstance(knobs, A.Knobs) else make_knobs(**(knobs or {}))
+        s = stream if stream is not None else torch.cuda.current_stream(pb.queries[0][0].device)
+        A.check(self._lib.gba_groupby_batch(self._h, len(pb.queries), pb.qarr, pb.oarr, C.byref(kn),
+                                            C.c_void_p(s.cuda_stream), pb.ng), self._h)
+        return np.ctypeslib.as_array(pb.ng)[:len(pb.queries)].copy()
 
     def autotune(self, queries: Sequence, knobs=None, outs=None, stream=None, reps: int = 2):
         """gba_autotune over device queries (one query: gba_groupby knobs; several:

@@ -17,7 +17,10 @@
 // No counterpart in the reference: its host loop runs one query, one tile per
 // stream at a time (group_then_partition.cu:332-424).
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <string>
@@ -29,6 +32,26 @@
 #include "gba_plan.h"
 
 namespace {
+
+// GBA_TRACE=1 in the environment: host-side phase times of each batch call on
+// stderr (where a step's time goes between the kernels).
+struct PhaseTrace {
+  bool on = std::getenv("GBA_TRACE") != nullptr;
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now(), last = t0;
+  std::string line;
+  void mark(const char* what) {
+    if (!on) return;
+    const auto now = std::chrono::steady_clock::now();
+    char buf[96];
+    std::snprintf(buf, sizeof(buf), " %s=%.3fms", what, std::chrono::duration<double, std::milli>(now - last).count());
+    line += buf;
+    last = now;
+  }
+  ~PhaseTrace() {
+    if (on) std::fprintf(stderr, "gba_groupby_batch:%s total=%.3fms\n", line.c_str(),
+                         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+  }
+};
 
 struct QInfo {
   QDesc q;
@@ -108,6 +131,7 @@ extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_
   if (knobs) k = *knobs;
   else gba_default_knobs(&k);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  PhaseTrace trace;
 
   // ---- validate and describe every query ----
   std::vector<QInfo> qi(nq);
@@ -138,8 +162,10 @@ extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_
       ctx->err = "learned sizing requested but no estimator weights are loaded";
       return GBA_ERR_INVALID_ARG;
     }
+    trace.mark("validate");
     gba_status st = batch_predict(ctx, qd, s, &pred, &skew);
     if (st != GBA_OK) return st;
+    trace.mark("estimate");
     ctx->stats.predicted_groups = std::accumulate(pred.begin(), pred.end(), 0.0);
   }
   // work items are cut at multiples of T rows (vector loads need aligned starts)
@@ -302,6 +328,7 @@ extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_
     if (e == cudaSuccess) e = cudaMemcpyAsync(h + h_stat, d + o_stat, stat_bytes, cudaMemcpyDeviceToHost, cs);
     return e;
   };
+  trace.mark("plan");
   if (nt > 0) {
     for (int g = 0; g < ng; ++g)
       GBA_CUDA_TRY(ctx, gba_prepare_stream_agg(groups[g].proto, groups[g].smem));
@@ -345,7 +372,9 @@ extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_
     } else {
       GBA_CUDA_TRY(ctx, enqueue(s));
     }
+    trace.mark("launch");
     GBA_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    trace.mark("table_queries");
     for (int r = 0; timing && r < 3; ++r) {
       float ms = 0.f;
       if (cudaEventElapsedTime(&ms, ctx->tev[r], ctx->tev[r + 1]) == cudaSuccess) ctx->stats.kernel_ms[r] += ms;
@@ -419,6 +448,7 @@ extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_
       return st;
     }
   }
+  trace.mark("partition_queries_and_reruns");
   acc.strategy = nt == nq ? GBA_STRATEGY_TABLE : (nt == 0 ? GBA_STRATEGY_PARTITION : GBA_STRATEGY_AUTO);
   acc.preagg = 0;
   for (int j = 0; j < nt; ++j) acc.preagg += qi[tq[j]].S > 0;

@@ -298,3 +298,24 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 }
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+// Dynamic shared-memory limit for a kernel: always the most the device allows
+// beside the kernel's static shared memory.  The attribute is process-wide per
+// kernel, so setting it to each launch's own size would race between host
+// threads launching the same kernel with different sizes (one thread's
+// smaller limit failing the other's launch); this value is the same for every
+// caller and does not change a launch's occupancy, which follows the shared
+// memory the launch asks for.
+template <typename K>
+inline cudaError_t gba_allow_max_smem(K* kernel) {
+  static const int optin = [] {
+    int d = 0, v = 0;
+    cudaGetDevice(&d);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, d);
+    return v;
+  }();
+  cudaFuncAttributes a;
+  cudaError_t e = cudaFuncGetAttributes(&a, kernel);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - int(a.sharedSizeBytes));
+}
+

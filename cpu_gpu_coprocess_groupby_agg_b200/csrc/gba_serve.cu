@@ -66,6 +66,7 @@ struct gba_server {
   int64_t submitted = 0, finished = 0;
   bool stop = false;
   gba_context* admin = nullptr;  // validates queries at submit (under mu)
+  std::string last_failure;      // message of the latest failed request
 };
 
 static int64_t ctx_resident_bytes(const gba_context* c) {
@@ -168,6 +169,10 @@ static void lane_main(gba_server* sv, int lane) {
         mine = ctx_resident_bytes(ctx);
       }
       sv->resident[lane] = mine;
+      for (Request* r : take)
+        if (r->info.status != GBA_OK)
+          sv->last_failure = "lane " + std::to_string(lane) + ": " + gba_status_string(gba_status(r->info.status)) +
+                             ": " + ctx->err;
       for (Request* r : take) {
         r->t_end = t_end;
         r->info.lane = lane;
@@ -333,7 +338,8 @@ extern "C" gba_status gba_server_pending(gba_server* sv, int64_t* queued, int64_
 }
 
 extern "C" const char* gba_server_last_error(const gba_server* sv) {
-  return sv && sv->admin ? sv->admin->err.c_str() : "null server";
+  if (!sv || !sv->admin) return "null server";
+  return sv->last_failure.empty() ? sv->admin->err.c_str() : sv->last_failure.c_str();
 }
 
 extern "C" gba_status gba_server_destroy(gba_server* sv) {

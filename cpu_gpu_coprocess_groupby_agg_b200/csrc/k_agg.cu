@@ -313,46 +313,80 @@ __global__ void k_table_init(GTable t, int naccs, QDesc q) {
   }
 }
 
-template <bool K64>
-__global__ void k_compact(GTable t, QDesc q, OutDesc o) {
+// Compaction of table slots [lo, hi) (hi - lo <= 2048) by a whole CTA of 256
+// threads: every thread takes 8 slots, the CTA counts its occupied ones with
+// a block scan and reserves their output rows with ONE atomic on the output
+// counter, then each thread writes its slots in order.  (Reserving per warp
+// put millions of atomics on one counter per query, which serialised in L2.)
+constexpr int kCompactThreads = 256, kCompactPer = 8, kCompactSlots = kCompactThreads * kCompactPer;
+__device__ __forceinline__ void compact_range(const GTable& t, const QDesc& q, const OutDesc& o, uint64_t lo,
+                                              uint64_t hi) {
+  __shared__ unsigned s_warp[kCompactThreads / 32];
+  __shared__ unsigned long long s_base;
   const int stride = 1 + q.naccs;
-  const unsigned lane = lane_id();
-  const uint64_t warp = (blockIdx.x * uint64_t(blockDim.x) + threadIdx.x) >> 5;
-  const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
-  for (uint64_t base = warp * 32; base < t.cap; base += nwarps * 32) {
-    const uint64_t i = base + lane;
-    unsigned long long k = EMPTY64;
-    if (i < t.cap) k = t.base[i * stride];
-    const bool occ = k != EMPTY64;
-    const unsigned m = __ballot_sync(GBA_FULL_MASK, occ);
-    if (m == 0) continue;
-    unsigned long long pos0 = 0;
-    if (lane == 0) pos0 = atomicAdd(o.count, (unsigned long long)__popc(m));
-    pos0 = __shfl_sync(GBA_FULL_MASK, pos0, 0);
-    if (occ) {
-      const unsigned long long pos = pos0 + __popc(m & ((1u << lane) - 1u));
-      if (pos < (unsigned long long)o.capacity) {
-        if (K64) static_cast<unsigned long long*>(o.keys)[pos] = k;
-        else static_cast<unsigned*>(o.keys)[pos] = unsigned(k);
+  const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
+  unsigned long long k[kCompactPer];
+  unsigned cnt = 0;
 #pragma unroll
-        for (int a = 0; a < GBA_MAX_AGGS; ++a)
-          if (a < q.naccs) o.accs[a][pos] = t.base[i * stride + 1 + a];
-      }
-    }
+  for (int j = 0; j < kCompactPer; ++j) {
+    const uint64_t i = lo + uint64_t(j) * kCompactThreads + threadIdx.x;
+    k[j] = i < hi ? t.base[i * stride] : EMPTY64;
+    cnt += k[j] != EMPTY64;
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    const unsigned long long* side = t.base + t.cap * stride;
-    if (side[0] != 0ull) {
-      const unsigned long long pos = atomicAdd(o.count, 1ull);
-      if (pos < (unsigned long long)o.capacity) {
-        if (K64) static_cast<unsigned long long*>(o.keys)[pos] = EMPTY64;
-        else static_cast<unsigned*>(o.keys)[pos] = EMPTY32;
+  unsigned x = cnt;  // inclusive warp scan
 #pragma unroll
-        for (int a = 0; a < GBA_MAX_AGGS; ++a)
-          if (a < q.naccs) o.accs[a][pos] = side[1 + a];
-      }
-    }
+  for (int d = 1; d < 32; d <<= 1) {
+    const unsigned y = __shfl_up_sync(GBA_FULL_MASK, x, d);
+    if (int(lane) >= d) x += y;
   }
+  if (lane == 31) s_warp[warp] = x;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned run = 0;
+    for (int w = 0; w < kCompactThreads / 32; ++w) {
+      const unsigned c = s_warp[w];
+      s_warp[w] = run;
+      run += c;
+    }
+    s_base = run ? atomicAdd(o.count, (unsigned long long)run) : 0ull;
+  }
+  __syncthreads();
+  unsigned long long pos = s_base + s_warp[warp] + (x - cnt);
+  const bool K64 = q.key64 != 0;
+#pragma unroll
+  for (int j = 0; j < kCompactPer; ++j) {
+    if (k[j] == EMPTY64) continue;
+    const uint64_t i = lo + uint64_t(j) * kCompactThreads + threadIdx.x;
+    if (pos < (unsigned long long)o.capacity) {
+      if (K64) static_cast<unsigned long long*>(o.keys)[pos] = k[j];
+      else static_cast<unsigned*>(o.keys)[pos] = unsigned(k[j]);
+#pragma unroll
+      for (int a = 0; a < GBA_MAX_AGGS; ++a)
+        if (a < q.naccs) o.accs[a][pos] = t.base[i * stride + 1 + a];
+    }
+    ++pos;
+  }
+  __syncthreads();  // s_warp / s_base are reused by the next range
+}
+
+// the all-ones key's side slot, if present (one thread)
+__device__ __forceinline__ void compact_side(const GTable& t, const QDesc& q, const OutDesc& o) {
+  const int stride = 1 + q.naccs;
+  const unsigned long long* side = t.base + t.cap * stride;
+  if (side[0] == 0ull) return;
+  const unsigned long long pos = atomicAdd(o.count, 1ull);
+  if (pos >= (unsigned long long)o.capacity) return;
+  if (q.key64) static_cast<unsigned long long*>(o.keys)[pos] = EMPTY64;
+  else static_cast<unsigned*>(o.keys)[pos] = EMPTY32;
+#pragma unroll
+  for (int a = 0; a < GBA_MAX_AGGS; ++a)
+    if (a < q.naccs) o.accs[a][pos] = side[1 + a];
+}
+
+__global__ void __launch_bounds__(kCompactThreads) k_compact(GTable t, QDesc q, OutDesc o) {
+  for (uint64_t lo = uint64_t(blockIdx.x) * kCompactSlots; lo < t.cap; lo += uint64_t(gridDim.x) * kCompactSlots)
+    compact_range(t, q, o, lo, lo + kCompactSlots < t.cap ? lo + kCompactSlots : t.cap);
+  if (blockIdx.x == 0 && threadIdx.x == 0) compact_side(t, q, o);
 }
 
 // ---- batched queries: table init and compaction (the aggregation itself is
@@ -396,53 +430,19 @@ __global__ void __launch_bounds__(256) k_batch_init(const BatchQ* qs, const int6
 }
 
 // compaction of every query of a batch into its own output (blocks dealt as
-// in k_batch_init; block 0 of a query also emits its all-ones-key side slot)
-__global__ void __launch_bounds__(256) k_batch_compact(const BatchQ* qs, const int64_t* blk_prefix, int nq) {
+// in k_batch_init, one block per 2048 slots; block 0 of a query also emits
+// its all-ones-key side slot)
+__global__ void __launch_bounds__(kCompactThreads) k_batch_compact(const BatchQ* qs, const int64_t* blk_prefix,
+                                                                   int nq) {
   const int qi = batch_query_of_block(blk_prefix, nq, blockIdx.x);
   const int64_t b = int64_t(blockIdx.x) - blk_prefix[qi];
   const int64_t nb = blk_prefix[qi + 1] - blk_prefix[qi];
   const GTable t = qs[qi].gt;
-  const QDesc& q = qs[qi].q;
+  const QDesc q = qs[qi].q;
   const OutDesc o = qs[qi].out;
-  const bool K64 = q.key64 != 0;
-  const int stride = 1 + q.naccs;
-  const unsigned lane = lane_id();
-  const uint64_t warp = (uint64_t(b) * blockDim.x + threadIdx.x) >> 5;
-  const uint64_t nwarps = (uint64_t(nb) * blockDim.x) >> 5;
-  for (uint64_t base = warp * 32; base < t.cap; base += nwarps * 32) {
-    const uint64_t i = base + lane;
-    unsigned long long k = EMPTY64;
-    if (i < t.cap) k = t.base[i * stride];
-    const bool occ = k != EMPTY64;
-    const unsigned m = __ballot_sync(GBA_FULL_MASK, occ);
-    if (m == 0) continue;
-    unsigned long long pos0 = 0;
-    if (lane == 0) pos0 = atomicAdd(o.count, (unsigned long long)__popc(m));
-    pos0 = __shfl_sync(GBA_FULL_MASK, pos0, 0);
-    if (occ) {
-      const unsigned long long pos = pos0 + __popc(m & ((1u << lane) - 1u));
-      if (pos < (unsigned long long)o.capacity) {
-        if (K64) static_cast<unsigned long long*>(o.keys)[pos] = k;
-        else static_cast<unsigned*>(o.keys)[pos] = unsigned(k);
-#pragma unroll
-        for (int a = 0; a < GBA_MAX_AGGS; ++a)
-          if (a < q.naccs) o.accs[a][pos] = t.base[i * stride + 1 + a];
-      }
-    }
-  }
-  if (b == 0 && threadIdx.x == 0) {
-    const unsigned long long* side = t.base + t.cap * stride;
-    if (side[0] != 0ull) {
-      const unsigned long long pos = atomicAdd(o.count, 1ull);
-      if (pos < (unsigned long long)o.capacity) {
-        if (K64) static_cast<unsigned long long*>(o.keys)[pos] = EMPTY64;
-        else static_cast<unsigned*>(o.keys)[pos] = EMPTY32;
-#pragma unroll
-        for (int a = 0; a < GBA_MAX_AGGS; ++a)
-          if (a < q.naccs) o.accs[a][pos] = side[1 + a];
-      }
-    }
-  }
+  for (uint64_t lo = uint64_t(b) * kCompactSlots; lo < t.cap; lo += uint64_t(nb) * kCompactSlots)
+    compact_range(t, q, o, lo, lo + kCompactSlots < t.cap ? lo + kCompactSlots : t.cap);
+  if (b == 0 && threadIdx.x == 0) compact_side(t, q, o);
 }
 
 }  // namespace
@@ -478,7 +478,7 @@ cudaError_t gba_launch_preagg(const QDesc& q, const GTable& t, const PreaggCfg& 
   return gba_dispatch_sig(q, [&](auto K, auto sig) -> cudaError_t {
     constexpr bool k64 = decltype(K)::value;
     using Sig = decltype(sig);
-    cudaError_t e = cudaFuncSetAttribute(k_preagg<k64, Sig>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    cudaError_t e = gba_allow_max_smem(k_preagg<k64, Sig>);
     if (e != cudaSuccess) return e;
     k_preagg<k64, Sig><<<c.grid, c.block, smem, s>>>(P);
     return cudaGetLastError();
@@ -486,8 +486,7 @@ cudaError_t gba_launch_preagg(const QDesc& q, const GTable& t, const PreaggCfg& 
 }
 
 cudaError_t gba_launch_compact(const GTable& t, const QDesc& q, const OutDesc& o, int grid, cudaStream_t s) {
-  if (q.key64) k_compact<true><<<grid, 256, 0, s>>>(t, q, o);
-  else k_compact<false><<<grid, 256, 0, s>>>(t, q, o);
+  k_compact<<<grid, kCompactThreads, 0, s>>>(t, q, o);
   return cudaGetLastError();
 }
 
@@ -513,6 +512,6 @@ cudaError_t gba_launch_batch_init(const BatchQ* d_qs, const int64_t* blk_prefix,
 cudaError_t gba_launch_batch_compact(const BatchQ* d_qs, const int64_t* blk_prefix, int nq, int64_t nblocks,
                                      cudaStream_t s) {
   if (nq <= 0) return cudaSuccess;
-  k_batch_compact<<<unsigned(nblocks), 256, 0, s>>>(d_qs, blk_prefix, nq);
+  k_batch_compact<<<unsigned(nblocks), kCompactThreads, 0, s>>>(d_qs, blk_prefix, nq);
   return cudaGetLastError();
 }

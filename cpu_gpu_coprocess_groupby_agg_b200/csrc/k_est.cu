@@ -60,23 +60,29 @@ __global__ void k_est_init(const EstQuery* qs, int nq) {
   }
 }
 
-// Frequency-class bookkeeping: a key's count moving from c to c + 1 leaves
-// class min(c, 4) and enters class min(c + 1, 4) (classes 1, 2, 3, 4+), and
+// Frequency-class bookkeeping: a key's count moving from c to c + m leaves
+// class min(c, 4) and enters class min(c + m, 4) (classes 1, 2, 3, 4+), and
 // c == 0 makes it a new distinct key.  Whatever order the increments run in,
 // the totals end exact, so the sample's frequency profile needs no scan of
 // the count table afterwards.  f[0] distinct, f[1..4] f1..f4+, f[5] max count,
 // f[6] sampled rows (block-local shared counters, flushed once per query).
-__device__ __forceinline__ void freq_step(unsigned long long* f, unsigned long long old) {
+__device__ __forceinline__ void freq_step(unsigned long long* f, unsigned long long old, unsigned long long m) {
+  const unsigned long long nw = old + m;
+  const unsigned long long co = old < 4 ? old : 4, cn = nw < 4 ? nw : 4;
   if (old == 0) atomicAdd(&f[0], 1ull);
-  else if (old < 4) atomicAdd(&f[old], ~0ull);  // -1
-  if (old < 4) atomicAdd(&f[old + 1], 1ull);
-  atomicMax(&f[5], old + 1);
-  atomicAdd(&f[6], 1ull);
+  if (co != cn) {
+    if (co) atomicAdd(&f[co], ~0ull);  // -1
+    atomicAdd(&f[cn], 1ull);
+  }
+  atomicMax(&f[5], nw);
+  atomicAdd(&f[6], m);
 }
 
 // one thread per sampled row; per-query count table (keys + counts, linear
 // probing, capacity >= 2x the sample), 64 HLL registers and the frequency
-// classes
+// classes.  Lanes of a warp holding the same key add their rows with one
+// atomic from the lowest of them (a skewed column's hot key would otherwise
+// serialise thousands of atomics on one counter).
 __global__ void k_est_sample(const EstQuery* qs, int nq) {
   __shared__ unsigned long long sf[7];
   for (int qi = blockIdx.y; qi < nq; qi += gridDim.y) {
@@ -84,20 +90,29 @@ __global__ void k_est_sample(const EstQuery* qs, int nq) {
     if (threadIdx.x < 7) sf[threadIdx.x] = 0ull;
     __syncthreads();
     const int64_t items = int64_t(e.sampled_tiles) << 10;
-    for (int64_t it = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; it < items;
-         it += int64_t(gridDim.x) * blockDim.x) {
-      const uint64_t r = sample_row(e, it);
-      if (r == ~0ull) continue;
-      const uint64_t k = e.key64 ? static_cast<const unsigned long long*>(e.keys)[r]
-                                 : static_cast<const unsigned*>(e.keys)[r];
-      const uint32_t h = e.key64 ? murmur3_64(k, 0x5bd1e995u) : murmur3_32(uint32_t(k), 0x5bd1e995u);
-      // HLL: the top 6 bits select the register, the rank of the first set
-      // bit among the remaining 26 is its candidate value
-      const unsigned reg = h >> 26;
-      const unsigned rank = __clz((h << 6) | (1u << 5)) + 1;
-      if (rank > __ldcg(&e.hll[reg])) atomicMax(&e.hll[reg], rank);
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    // whole warps iterate together (for __match_any_sync)
+    for (int64_t base = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) & ~int64_t(31); base < items;
+         base += stride) {
+      const int64_t it = base + lane_id();
+      const uint64_t r = it < items ? sample_row(e, it) : ~0ull;
+      const bool live = r != ~0ull;
+      uint64_t k = 0;
+      if (live) {
+        k = e.key64 ? static_cast<const unsigned long long*>(e.keys)[r] : static_cast<const unsigned*>(e.keys)[r];
+        const uint32_t h = e.key64 ? murmur3_64(k, 0x5bd1e995u) : murmur3_32(uint32_t(k), 0x5bd1e995u);
+        // HLL: the top 6 bits select the register, the rank of the first set
+        // bit among the remaining 26 is its candidate value
+        const unsigned reg = h >> 26;
+        const unsigned rank = __clz((h << 6) | (1u << 5)) + 1;
+        if (rank > __ldcg(&e.hll[reg])) atomicMax(&e.hll[reg], rank);
+      }
+      const unsigned live_mask = __ballot_sync(GBA_FULL_MASK, live);
+      const unsigned peers = __match_any_sync(GBA_FULL_MASK, live ? k : ~0ull) & live_mask;
+      if (!live || (peers & ((1u << lane_id()) - 1u))) continue;  // not the group's lowest lane
+      const unsigned long long m = __popc(peers);
       if (k == EMPTY64) {  // the table's empty marker (only a 64-bit key can equal it)
-        freq_step(sf, atomicAdd(&e.stats[3], 1ull));
+        freq_step(sf, atomicAdd(&e.stats[3], m), m);
         continue;
       }
       uint64_t s = (uint64_t(table_hash(k)) * e.cap) >> 32;
@@ -105,13 +120,13 @@ __global__ void k_est_sample(const EstQuery* qs, int nq) {
         unsigned long long* slot = e.table + 2 * s;
         const unsigned long long cur = __ldcg(slot);
         if (cur == k) {
-          freq_step(sf, atomicAdd(slot + 1, 1ull));
+          freq_step(sf, atomicAdd(slot + 1, m), m);
           break;
         }
         if (cur == EMPTY64) {
           const unsigned long long prev = atomicCAS(slot, EMPTY64, k);
           if (prev == EMPTY64 || prev == k) {
-            freq_step(sf, atomicAdd(slot + 1, 1ull));
+            freq_step(sf, atomicAdd(slot + 1, m), m);
             break;
           }
         }
@@ -354,7 +369,10 @@ size_t train_smem() { return sizeof(float) * (size_t(kTrainB) * (F + 5 * H) + kT
 // ---------------------------------------------------------------------------
 // launchers
 cudaError_t gba_launch_est_sample(const EstQuery* d_qs, int nq, int64_t max_items, cudaStream_t s) {
-  const int gx = int(std::min<int64_t>((max_items + 255) / 256, 1184));
+  // up to 16 sampled rows per thread: with one row per thread, the largest
+  // query set the grid's width and the many small queries of a batch left
+  // most of their blocks empty (hundreds of thousands of idle blocks)
+  const int gx = int(std::min<int64_t>((max_items + 256 * 16 - 1) / (256 * 16), 64));
   dim3 grid(std::max(gx, 1), std::min(nq, 65535));
   k_est_sample<<<grid, 256, 0, s>>>(d_qs, nq);
   return cudaGetLastError();

@@ -443,11 +443,11 @@ cudaError_t gba_launch_part_scatter(const PartPass& p, int grid, int T, cudaStre
   const size_t smem = gba_part_scatter_smem(p.in, p.bits, T);
   cudaError_t e;
   if (p.in.key64) {
-    e = cudaFuncSetAttribute(k_part_scatter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    e = gba_allow_max_smem(k_part_scatter<true>);
     if (e != cudaSuccess) return e;
     k_part_scatter<true><<<grid, 512, smem, s>>>(p, T);
   } else {
-    e = cudaFuncSetAttribute(k_part_scatter<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    e = gba_allow_max_smem(k_part_scatter<false>);
     if (e != cudaSuccess) return e;
     k_part_scatter<false><<<grid, 512, smem, s>>>(p, T);
   }
@@ -459,7 +459,7 @@ cudaError_t gba_launch_part_agg(const PartAgg& a, int grid, cudaStream_t s) {
   return gba_dispatch_sig(a.rows, [&](auto K, auto sig) -> cudaError_t {
     constexpr bool k64 = decltype(K)::value;
     using Sig = decltype(sig);
-    cudaError_t e = cudaFuncSetAttribute(k_part_agg<k64, Sig>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    cudaError_t e = gba_allow_max_smem(k_part_agg<k64, Sig>);
     if (e != cudaSuccess) return e;
     k_part_agg<k64, Sig><<<grid, 1024, smem, s>>>(a);
     return cudaGetLastError();

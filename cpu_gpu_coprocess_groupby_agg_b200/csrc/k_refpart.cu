@@ -114,7 +114,7 @@ cudaError_t gba_launch_refpart(const unsigned* keys, const unsigned long long* s
   const int grid = int(want < 1 ? 1 : (want > int64_t(sms) * 4 ? int64_t(sms) * 4 : want));
   if (n > 0) {
     if (size_t(P) * 4 > 48 * 1024) {
-      e = cudaFuncSetAttribute(k_rp_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, int(size_t(P) * 4));
+      e = gba_allow_max_smem(k_rp_hist);
       if (e != cudaSuccess) return e;
     }
     k_rp_hist<<<grid, 512, size_t(P) * 4, s>>>(keys, n, unsigned(P), hist);

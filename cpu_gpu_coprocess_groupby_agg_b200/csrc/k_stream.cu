@@ -387,7 +387,7 @@ cudaError_t gba_prepare_stream_agg(const QDesc& proto, size_t smem) {
   return gba_dispatch_sig(proto, [&](auto K, auto sig) -> cudaError_t {
     constexpr bool k64 = decltype(K)::value;
     using Sig = decltype(sig);
-    return cudaFuncSetAttribute(k_stream_agg<k64, Sig>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    return gba_allow_max_smem(k_stream_agg<k64, Sig>);
   });
 }
 

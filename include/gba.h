@@ -267,6 +267,7 @@ gba_status gba_server_wait(gba_server* sv, int64_t ticket, double timeout_s, gba
 /* Waits up to timeout_s for any finished request and collects it. */
 gba_status gba_server_next_done(gba_server* sv, double timeout_s, int64_t* ticket, gba_request_info* info);
 gba_status gba_server_pending(gba_server* sv, int64_t* queued, int64_t* running, int64_t* inflight_bytes);
+/* The latest failed request's lane and message, else the latest refused submit's. */
 const char* gba_server_last_error(const gba_server* sv);
 /* Finishes every submitted request, then stops the lanes and frees them. */
 gba_status gba_server_destroy(gba_server* sv);
