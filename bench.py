@@ -205,6 +205,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--knob", action="append", default=[], help="name=value knob override")
     ap.add_argument("--no-autotune", action="store_true", help="batch: default knobs instead of gba_autotune's")
+    ap.add_argument("--ndv-range", default="", help="batch: only queries with LO <= distinct ids < HI ('LO:HI')")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     ws, rank, local = dist_setup()
@@ -347,6 +348,12 @@ def run_batch(args, ws, rank, local, pg):
     from cpu_gpu_coprocess_groupby_agg_b200 import estimator as E
     from cpu_gpu_coprocess_groupby_agg_b200 import workloads as W
     allq = W.batch_queries()
+    name = BATCH_NAME
+    if args.ndv_range:
+        # a slice of the batch by distinct ids (profiling one cardinality class)
+        lo, hi = (float(x) for x in args.ndv_range.split(":"))
+        allq = [q for q in allq if lo <= q.meta["ndv"] < hi]
+        name = f"{BATCH_NAME}[ndv {args.ndv_range}]"
     ctx = Context(local)
     if args.sizing == "learned" and not E.load_default(ctx):
         raise SystemExit(f"learned sizing needs trained weights at {E.WEIGHTS}")
@@ -378,8 +385,8 @@ def run_batch(args, ws, rank, local, pg):
         return kn
 
     def knob_summary(k):
-        return {"learned_load": k.learned_load, "load_factor": k.load_factor, "item_rows": k.item_rows,
-                "smem_probe_cap": k.smem_probe_cap}
+        return {"blocks_per_sm": k.blocks_per_sm, "learned_load": k.learned_load, "load_factor": k.load_factor,
+                "item_rows": k.item_rows, "smem_probe_cap": k.smem_probe_cap}
 
     pb = ctx.prepare_batch(dq, outs)
 
@@ -418,13 +425,13 @@ def run_batch(args, ws, rank, local, pg):
     traffic = None
     tfile = ROOT / "profiles" / "traffic.json"
     if tfile.exists():
-        traffic = json.loads(tfile.read_text()).get(f"{BATCH_NAME}:k_stream_agg")
+        traffic = json.loads(tfile.read_text()).get(f"{name}:k_stream_agg")
     line = {
         "metric": "groupby_rows_per_s", "value": round(value, 4), "unit": "G rows/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int64",
         "data": "synthetic (seeded PCG32 generator, generated on device)",
-        "config": {"workload": BATCH_NAME, "queries": len(allq), "rows": total_rows, "input_bytes": in_bytes,
+        "config": {"workload": name, "queries": len(allq), "rows": total_rows, "input_bytes": in_bytes,
                    "groups": groups, "aggs": ["sum(0)", "count(*)"], "sizing": args.sizing,
                    "strategy_mix": st["strategy"], "table_slots_total": st["table_slots"],
                    "predicted_groups_total": round(st["predicted_groups"], 1),

@@ -24,12 +24,14 @@ size_t gba_batch_static_smem();
 int gba_batch_sig_id(const QDesc& q);
 // Streaming aggregation (k_stream.cu): one persistent launch over work items
 // (d_items == nullptr: query d_qs[0] cut into items of item_rows rows, a
-// multiple of 256).  *item_ctr must be zero at launch.
+// multiple of 256).  *item_ctr must be zero at launch.  minb = CTAs per SM the
+// launch is built for: 1 (512 threads with the whole shared memory and all
+// registers) or 2 (two such CTAs, each with half of both).
 size_t gba_stream_smem_bytes(const QDesc& q, int S);
-int gba_stream_rows_per_chunk(const QDesc& q);
-cudaError_t gba_prepare_stream_agg(const QDesc& proto, size_t smem);
-cudaError_t gba_launch_stream_agg(const QDesc& proto, const BatchQ* d_qs, const BatchItem* d_items, int nitems,
-                                  int64_t item_rows, unsigned* item_ctr, size_t smem, int sprobe, int grid,
+int gba_stream_rows_per_chunk(const QDesc& q, int minb);
+cudaError_t gba_prepare_stream_agg(const QDesc& proto, int minb);
+cudaError_t gba_launch_stream_agg(const QDesc& proto, int minb, const BatchQ* d_qs, const BatchItem* d_items,
+                                  int nitems, int64_t item_rows, unsigned* item_ctr, size_t smem, int sprobe, int grid,
                                   cudaStream_t s);
 // blk_prefix[i]: first block of query i (nq + 1 entries, blk_prefix[nq] = nblocks)
 cudaError_t gba_launch_batch_init(const BatchQ* d_qs, const int64_t* blk_prefix, int nq, int64_t nblocks,

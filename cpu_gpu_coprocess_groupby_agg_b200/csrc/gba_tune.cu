@@ -10,8 +10,8 @@
 //   one query (gba_groupby):   tile_rows (TMA tile length), blocks_per_sm,
 //                              partition_bits (around the automatic choice),
 //                              learned_load / load_factor (HBM table load)
-//   a batch (gba_groupby_batch): learned_load / load_factor, item_rows,
-//                              smem_probe_cap (shared-table buckets probed)
+//   a batch (gba_groupby_batch): blocks_per_sm, learned_load / load_factor,
+//                              item_rows, smem_probe_cap (buckets probed)
 // The outputs are written by every trial; the last trial leaves a complete,
 // correct result for the best knobs only if the caller reruns with them.
 #include <cmath>
@@ -94,6 +94,9 @@ extern "C" gba_status gba_autotune(gba_context* ctx, int32_t nq, const gba_query
                       }});
     axes.push_back({"load", {nan, 0.25, 0.5, 0.7}, set_load});
   } else {
+    axes.push_back({"blocks_per_sm", {nan, 1, 4}, [](gba_knobs& k, double v) {
+                      k.blocks_per_sm = std::isnan(v) ? 0 : int32_t(v);
+                    }});
     axes.push_back({"load", {nan, 0.25, 0.5}, set_load});
     axes.push_back({"item_rows", {nan, double(1 << 17), double(1 << 19)}, [](gba_knobs& k, double v) {
                       k.item_rows = std::isnan(v) ? 0 : int32_t(v);

@@ -25,10 +25,12 @@
 
 namespace {
 
-// rows per lane per chunk: fewer when a row carries many accumulators
-template <typename Sig>
+// rows per lane per chunk: fewer when a row carries many accumulators, and
+// half as many when two CTAs share an SM (MINB = 2: half the registers)
+template <typename Sig, int MINB>
 __host__ __device__ constexpr int stream_rows_per_lane() {
-  return Sig::NA <= 2 ? 8 : (Sig::NA <= 4 ? 4 : 2);
+  return (Sig::NA <= 2 ? 8 : (Sig::NA <= 4 ? 4 : 2)) / MINB > 0 ? (Sig::NA <= 2 ? 8 : (Sig::NA <= 4 ? 4 : 2)) / MINB
+                                                                 : 1;
 }
 
 // V consecutive 4-byte / 8-byte elements starting at p (aligned to V * width)
@@ -178,11 +180,10 @@ __device__ __noinline__ void gtable_insert_slow(const GTable gt, const QDesc& q,
   gtable_finish<K64, Sig>(gt, q, key, home, cur, v, flags);
 }
 
-template <bool K64, typename Sig>
+template <bool K64, typename Sig, int R>
 __device__ __forceinline__ void stream_chunk(const BatchQ& bq, const SmemTable<K64>& st, int nbk, int64_t c0,
                                              int64_t row_end, bool vec) {
   constexpr int NA = Sig::NA;
-  constexpr int R = stream_rows_per_lane<Sig>();
   constexpr int V = (16 / (K64 ? 8 : 4)) < R ? (16 / (K64 ? 8 : 4)) : R;  // rows per key vector
   constexpr int U = R / V;
   const QDesc& q = bq.q;
@@ -322,14 +323,14 @@ __device__ __forceinline__ void stream_chunk(const BatchQ& bq, const SmemTable<K
 // nullptr means one query (qs[0]) cut into items of `item_rows` rows.
 // sprobe: buckets probed before a row goes to the HBM table (BatchQ.pad bits
 // 8..15 override it per query when nonzero).
-template <bool K64, typename Sig>
-__global__ void __launch_bounds__(512, 1) k_stream_agg(const BatchQ* qs, const BatchItem* items, int nitems,
+template <bool K64, typename Sig, int MINB>
+__global__ void __launch_bounds__(512, MINB) k_stream_agg(const BatchQ* qs, const BatchItem* items, int nitems,
                                                        int64_t item_rows, unsigned* item_ctr, int sprobe) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ int s_item;
   __shared__ unsigned long long s_next;
   __shared__ __align__(16) BatchQ s_q;
-  constexpr int R = stream_rows_per_lane<Sig>();
+  constexpr int R = stream_rows_per_lane<Sig, MINB>();
   const int tid = threadIdx.x;
   for (;;) {
     if (tid == 0) s_item = int(atomicAdd(item_ctr, 1u));
@@ -361,7 +362,7 @@ __global__ void __launch_bounds__(512, 1) k_stream_agg(const BatchQ* qs, const B
       if (lane_id() == 0) c0 = atomicAdd(&s_next, (unsigned long long)(32 * R));
       c0 = __shfl_sync(GBA_FULL_MASK, c0, 0);
       if (int64_t(c0) >= item.row_end) break;
-      stream_chunk<K64, Sig>(s_q, st, nbk, int64_t(c0), item.row_end, vec);
+      stream_chunk<K64, Sig, R>(s_q, st, nbk, int64_t(c0), item.row_end, vec);
     }
     __syncthreads();
     if (s_q.S > 0) smem_flush_to_gtable<K64, Sig>(s_q.q, s_q.gt, st, s_q.flags);
@@ -372,10 +373,12 @@ __global__ void __launch_bounds__(512, 1) k_stream_agg(const BatchQ* qs, const B
 }  // namespace
 
 // ---------------------------------------------------------------------------
-int gba_stream_rows_per_chunk(const QDesc& q) {
+int gba_stream_rows_per_chunk(const QDesc& q, int minb) {
   int r = 0;
   gba_dispatch_sig(q, [&](auto, auto sig) -> cudaError_t {
-    r = 32 * stream_rows_per_lane<decltype(sig)>();
+    r = 32 * (minb == 4   ? stream_rows_per_lane<decltype(sig), 4>()
+              : minb == 2 ? stream_rows_per_lane<decltype(sig), 2>()
+                          : stream_rows_per_lane<decltype(sig), 1>());
     return cudaSuccess;
   });
   return r;
@@ -383,22 +386,27 @@ int gba_stream_rows_per_chunk(const QDesc& q) {
 
 size_t gba_stream_smem_bytes(const QDesc& q, int S) { return smem_table_bytes(S, q.key64, q.nwords) + 64; }
 
-cudaError_t gba_prepare_stream_agg(const QDesc& proto, size_t smem) {
+cudaError_t gba_prepare_stream_agg(const QDesc& proto, int minb) {
   return gba_dispatch_sig(proto, [&](auto K, auto sig) -> cudaError_t {
     constexpr bool k64 = decltype(K)::value;
     using Sig = decltype(sig);
-    return gba_allow_max_smem(k_stream_agg<k64, Sig>);
+    return minb == 4   ? gba_allow_max_smem(k_stream_agg<k64, Sig, 4>)
+           : minb == 2 ? gba_allow_max_smem(k_stream_agg<k64, Sig, 2>)
+                       : gba_allow_max_smem(k_stream_agg<k64, Sig, 1>);
   });
 }
 
-cudaError_t gba_launch_stream_agg(const QDesc& proto, const BatchQ* d_qs, const BatchItem* d_items, int nitems,
-                                  int64_t item_rows, unsigned* item_ctr, size_t smem, int sprobe, int grid,
+cudaError_t gba_launch_stream_agg(const QDesc& proto, int minb, const BatchQ* d_qs, const BatchItem* d_items,
+                                  int nitems, int64_t item_rows, unsigned* item_ctr, size_t smem, int sprobe, int grid,
                                   cudaStream_t s) {
   if (nitems <= 0) return cudaSuccess;
   return gba_dispatch_sig(proto, [&](auto K, auto sig) -> cudaError_t {
     constexpr bool k64 = decltype(K)::value;
     using Sig = decltype(sig);
-    k_stream_agg<k64, Sig><<<grid, 512, smem, s>>>(d_qs, d_items, nitems, item_rows, item_ctr, sprobe);
+    if (minb == 4) k_stream_agg<k64, Sig, 4><<<grid, 512, smem, s>>>(d_qs, d_items, nitems, item_rows, item_ctr, sprobe);
+    else if (minb == 2)
+      k_stream_agg<k64, Sig, 2><<<grid, 512, smem, s>>>(d_qs, d_items, nitems, item_rows, item_ctr, sprobe);
+    else k_stream_agg<k64, Sig, 1><<<grid, 512, smem, s>>>(d_qs, d_items, nitems, item_rows, item_ctr, sprobe);
     return cudaGetLastError();
   });
 }

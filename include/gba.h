@@ -99,7 +99,7 @@ typedef struct gba_knobs {
   int32_t preagg;         /* -1 auto, 0 off, 1 on */
   int32_t smem_slots;     /* shared-memory table slots per CTA */
   int32_t partition_bits; /* radix fan-out 2^bits */
-  int32_t blocks_per_sm;
+  int32_t blocks_per_sm;  /* single query: CTAs per SM of the pre-aggregation grid; batch: 1, 2 or 4 (0 = 2) */
   int32_t block_threads;
   int32_t tile_rows;
   int32_t nstages;        /* TMA pipeline depth */
@@ -214,8 +214,8 @@ gba_status gba_groupby_partition_u32(gba_context* ctx, const uint32_t* keys, con
  * gba_groupby_batch take them) under candidate knobs by coordinate descent
  * from `base` and writes the fastest setting to *best (and its mean time per
  * call in ms to *best_ms).  One query: tile_rows, blocks_per_sm,
- * partition_bits and the HBM table load; a batch (n_queries > 1): the table
- * load, item_rows and smem_probe_cap.  The load tuned is learned_load under
+ * partition_bits and the HBM table load; a batch (n_queries > 1):
+ * blocks_per_sm, the table load, item_rows and smem_probe_cap.  The load tuned is learned_load under
  * learned sizing, load_factor otherwise.  Every trial writes the outputs; rerun
  * with *best for the result.  No counterpart in the reference (its tile
  * length and partition count are constants, test/test.cu:94-98). */
