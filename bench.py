@@ -115,7 +115,8 @@ def dist_setup():
 
 def get_workload(name: str):
     from cpu_gpu_coprocess_groupby_agg_b200 import workloads as W
-    return {"skewed": W.skewed, "small": W.small, "highcard": W.high_card}[name]()
+    return {"skewed": W.skewed, "small": W.small, "highcard": W.high_card,
+            "large": lambda: W.large_serving_query(seed=900)}[name]()
 
 
 BATCH_NAME = "batch_256q_rows2^12-2^24_logu_ndv16-rows/2_zipf0-1.5_sum+count"
@@ -195,7 +196,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batch", choices=["batch", "skewed", "small", "highcard", "serve"])
+    ap.add_argument("--workload", default="batch", choices=["batch", "skewed", "small", "highcard", "large", "serve"])
     ap.add_argument("--duration", type=float, default=10.0, help="serve: seconds of Poisson arrivals")
     ap.add_argument("--rate", type=float, default=2000.0, help="serve: arrivals per second")
     ap.add_argument("--max-inflight", type=int, default=256, help="serve: client-side cap on requests in flight")

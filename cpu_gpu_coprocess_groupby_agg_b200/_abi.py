@@ -77,6 +77,7 @@ class Knobs(C.Structure):
         ("use_graph", C.c_int32),
         ("item_rows", C.c_int32),
         ("learned_load", C.c_double),
+        ("learned_min_rows", C.c_int64),
     ]
 
 

@@ -3,9 +3,10 @@
 // Fan-out: the reference uses a fixed P=300 (test/test.cu:96) and then merges
 // small partitions greedily so each merged partition fills a global table of
 // `Capacity` slots (groupby_agg_intra_partition.cu:13-48).  Here the fan-out is
-// chosen so that every final partition's groups fit one CTA's shared-memory
-// table: bits = ceil(log2(groups / groups_per_table)), split over one or two
-// MSD passes of at most 10 bits so each scatter pass keeps its write runs long.
+// chosen so that every final partition's groups fill a quarter of one CTA's
+// shared-memory table: bits = ceil(log2(groups / (S / 4))), split over one or
+// two MSD passes of at most 10 bits so each scatter pass keeps its write runs
+// long.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -67,7 +68,11 @@ gba_status gba_run_partition(gba_context* ctx, const QDesc& q, const gba_output*
   const int64_t n = q.n;
   int S = part_table_slots(ctx, q);
   if (k.smem_slots > 0) S = std::max(32, std::min(S, k.smem_slots));
-  const double per_table = 0.55 * S;
+  // groups aimed at per partition: a quarter of the shared table (measured on
+  // B200, best or within 8% of the best fan-out on the 2^28-row high-cardinality
+  // query (16 bits), the 2^27-row serving query (14) and the 2^26-row skewed
+  // query (11 vs 12); fuller tables make k_part_agg probe longer)
+  const double per_table = 0.25 * S;
   double groups = double(std::max<int64_t>(n, 1));
   if (k.sizing == GBA_SIZING_LEARNED && predicted_groups > 0) groups = std::min(groups, predicted_groups * 1.25 + 64);
   int B = k.partition_bits > 0 ? k.partition_bits : int(std::ceil(std::log2(std::max(1.0, groups / per_table))));

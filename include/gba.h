@@ -112,6 +112,8 @@ typedef struct gba_knobs {
   int32_t use_graph;      /* batch: -1 auto (on), 0 off, 1 on: replay the launch sequence as a CUDA graph */
   int32_t item_rows;      /* batch: rows per work-queue item (0 = auto) */
   double learned_load;    /* learned sizing: HBM table load at the predicted group count (0 = auto, 0.35) */
+  int64_t learned_min_rows; /* single query, learned sizing: smaller queries are sized plainly
+                               (0 = auto: while the plain table is <= 256 MB; -1 = always estimate) */
 } gba_knobs;
 
 /* What the last call on a context did. */

@@ -91,7 +91,7 @@ def test_learned_sizing_results_exact(ctx):
         ctx.est_load(E.init_params(0))
     for n, ndv, z in [(300_000, 50, 0.0), (500_000, 200_000, 0.0), (400_000, 60_000, 1.1)]:
         keys, cols = _data(n, np.int64, ndv, seed=n, zipf=z)
-        gk, ga, res = run_gpu(ctx, keys, cols, AGGS_ALL, knobs=dict(sizing="learned"))
+        gk, ga, res = run_gpu(ctx, keys, cols, AGGS_ALL, knobs=dict(sizing="learned", learned_min_rows=-1))
         assert res.stats["predicted_groups"] > 0
         compare(gk, ga, keys, cols, AGGS_ALL, f"learned n={n} ndv={ndv}")
     # a deliberately useless network (predicts 1 group) still gives exact results
@@ -99,5 +99,11 @@ def test_learned_sizing_results_exact(ctx):
     bad[:] = 0
     ctx.est_load(bad)
     keys, cols = _data(200_000, np.int64, 150_000, seed=3)
-    gk, ga, res = run_gpu(ctx, keys, cols, AGGS_ALL, knobs=dict(sizing="learned", strategy="table"))
+    gk, ga, res = run_gpu(ctx, keys, cols, AGGS_ALL, knobs=dict(sizing="learned", strategy="table",
+                                                                learned_min_rows=-1))
+    assert res.stats["predicted_groups"] > 0
     compare(gk, ga, keys, cols, AGGS_ALL, "learned with a useless network")
+    # a small query under learned sizing is sized plainly unless told otherwise
+    gk, ga, res = run_gpu(ctx, keys, cols, AGGS_ALL, knobs=dict(sizing="learned"))
+    assert res.stats["predicted_groups"] < 0
+    compare(gk, ga, keys, cols, AGGS_ALL, "learned sizing of a small query")
