@@ -5,8 +5,8 @@
 // `Capacity` slots (groupby_agg_intra_partition.cu:13-48).  Here the fan-out is
 // chosen so that every final partition's groups fill a quarter of one CTA's
 // shared-memory table: bits = ceil(log2(groups / (S / 4))), split over one or
-// two MSD passes of at most 10 bits so each scatter pass keeps its write runs
-// long.
+// two MSD passes (two from 10 bits on) so each scatter pass keeps its write
+// runs long.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -77,13 +77,16 @@ gba_status gba_run_partition(gba_context* ctx, const QDesc& q, const gba_output*
   if (k.sizing == GBA_SIZING_LEARNED && predicted_groups > 0) groups = std::min(groups, predicted_groups * 1.25 + 64);
   int B = k.partition_bits > 0 ? k.partition_bits : int(std::ceil(std::log2(std::max(1.0, groups / per_table))));
   B = std::max(1, std::min(B, 20));
-  const int T = 2048;  // scatter tile rows (<= 8 per thread)
+  const int T = 2048;  // scatter tile rows (<= 4 per thread of k_part_scatter's 512)
   const int64_t L = std::max<int64_t>(T, ((n + int64_t(ctx->sms) * 8 - 1) / (int64_t(ctx->sms) * 8) + T - 1) / T * T);
   const size_t rb = row_bytes(q);
 
   for (int attempt = 0;; ++attempt) {
     std::vector<int> passes;
-    if (B <= 10) passes = {B};
+    // one pass up to 512 digits; beyond that two passes (measured on the
+    // 2^26-row skewed query: 10 bits in one pass scatter 1.5x slower than
+    // 11 bits in two, a 2048-row tile leaving about 2 rows per digit)
+    if (B <= 9) passes = {B};
     else passes = {(B + 1) / 2, B / 2};
     ctx->stats.partition_bits = B;
 
@@ -186,7 +189,7 @@ gba_status gba_run_partition(gba_context* ctx, const QDesc& q, const gba_output*
                                              s));
       tm.end();
       tm.begin(3);
-      GBA_CUDA_TRY(ctx, gba_launch_part_scatter(pp, std::min<int>(pp.nchunks, ctx->sms * 3), T, s));
+      GBA_CUDA_TRY(ctx, gba_launch_part_scatter(pp, std::min<int>(pp.nchunks, ctx->sms * 2), T, s));
       tm.end();
       GBA_CUDA_TRY(ctx, gba_launch_seg_begins(pp.offsets, reinterpret_cast<const long long*>(W + o_cbase),
                                               reinterpret_cast<const int*>(W + o_snch), nseg_in, bits, n, d_seg, s));

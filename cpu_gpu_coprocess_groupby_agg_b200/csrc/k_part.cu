@@ -144,8 +144,9 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_excl(const unsigned* in, 
 // ---- staged scatter ---------------------------------------------------------------
 // shared layout: cursor[nb] (u64), lhist[nb] (u32), loff[nb] (u32), digits[T] (u16),
 // staged rows: keys[T] then one array per column [T]
-template <bool K64>
-__global__ void __launch_bounds__(512) k_part_scatter(PartPass p, int T) {
+// NC: value columns (compile time, so only their registers exist)
+template <bool K64, int NC>
+__global__ void __launch_bounds__(512, 2) k_part_scatter(PartPass p, int T) {
   extern __shared__ __align__(16) unsigned char sm[];
   const int nb = 1 << p.bits;
   unsigned long long* cursor = reinterpret_cast<unsigned long long*>(sm);
@@ -174,17 +175,31 @@ __global__ void __launch_bounds__(512) k_part_scatter(PartPass p, int T) {
       const int rows = int(ch.row_end - t0 < T ? ch.row_end - t0 : T);
       for (int d = threadIdx.x; d < nb; d += blockDim.x) lhist[d] = 0;
       __syncthreads();
-      // pass A: digit + local rank of every row (rows stay in registers)
-      constexpr int kMaxRpt = 8;
+      // pass A: every row's key and values into registers (all loads of the
+      // tile issued together), its digit, and its rank among the tile's rows
+      // of that digit
+      constexpr int kMaxRpt = 4;  // T <= 4 * 512
       unsigned rank[kMaxRpt];
       unsigned short dg[kMaxRpt];
       uint64_t kreg[kMaxRpt];
+      unsigned long long vreg[kMaxRpt][NC > 0 ? NC : 1];
 #pragma unroll
       for (int i = 0; i < kMaxRpt; ++i) {
         const int j = i * blockDim.x + threadIdx.x;
         if (j < rows) {
-          kreg[i] = K64 ? static_cast<const unsigned long long*>(p.in.keys)[t0 + j]
-                        : static_cast<const unsigned*>(p.in.keys)[t0 + j];
+          kreg[i] = K64 ? __ldcs(static_cast<const unsigned long long*>(p.in.keys) + t0 + j)
+                        : __ldcs(static_cast<const unsigned*>(p.in.keys) + t0 + j);
+#pragma unroll
+          for (int c = 0; c < NC; ++c)
+              vreg[i][c] = col_bytes_t(p.in.col_type[c]) == 8
+                               ? __ldcs(static_cast<const unsigned long long*>(p.in.cols[c]) + t0 + j)
+                               : __ldcs(static_cast<const unsigned*>(p.in.cols[c]) + t0 + j);
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < kMaxRpt; ++i) {
+        const int j = i * blockDim.x + threadIdx.x;
+        if (j < rows) {
           dg[i] = (unsigned short)digit_of<K64>(kreg[i], p.shift_hi, p.bits);
           rank[i] = atomicAdd(&lhist[dg[i]], 1u);
         }
@@ -225,14 +240,11 @@ __global__ void __launch_bounds__(512) k_part_scatter(PartPass p, int T) {
           if (K64) reinterpret_cast<unsigned long long*>(stg)[pos] = kreg[i];
           else reinterpret_cast<unsigned*>(stg)[pos] = unsigned(kreg[i]);
 #pragma unroll
-          for (int c = 0; c < GBA_MAX_COLS; ++c) {
-            if (c < p.in.ncols) {
-              if (col_bytes_t(p.in.col_type[c]) == 8)
-                reinterpret_cast<unsigned long long*>(scol[c])[pos] =
-                    static_cast<const unsigned long long*>(p.in.cols[c])[t0 + j];
-              else
-                reinterpret_cast<unsigned*>(scol[c])[pos] = static_cast<const unsigned*>(p.in.cols[c])[t0 + j];
-            }
+          for (int c = 0; c < NC; ++c) {
+            if (col_bytes_t(p.in.col_type[c]) == 8)
+              reinterpret_cast<unsigned long long*>(scol[c])[pos] = vreg[i][c];
+            else
+              reinterpret_cast<unsigned*>(scol[c])[pos] = unsigned(vreg[i][c]);
           }
         }
       }
@@ -441,17 +453,21 @@ cudaError_t gba_launch_scan_excl(const unsigned* in, unsigned long long* out, in
 
 cudaError_t gba_launch_part_scatter(const PartPass& p, int grid, int T, cudaStream_t s) {
   const size_t smem = gba_part_scatter_smem(p.in, p.bits, T);
-  cudaError_t e;
-  if (p.in.key64) {
-    e = gba_allow_max_smem(k_part_scatter<true>);
+  auto go = [&](auto kernel) -> cudaError_t {
+    cudaError_t e = gba_allow_max_smem(kernel);
     if (e != cudaSuccess) return e;
-    k_part_scatter<true><<<grid, 512, smem, s>>>(p, T);
-  } else {
-    e = gba_allow_max_smem(k_part_scatter<false>);
-    if (e != cudaSuccess) return e;
-    k_part_scatter<false><<<grid, 512, smem, s>>>(p, T);
+    kernel<<<grid, 512, smem, s>>>(p, T);
+    return cudaGetLastError();
+  };
+  const bool k64 = p.in.key64 != 0;
+  switch (p.in.ncols) {
+    case 0: return k64 ? go(k_part_scatter<true, 0>) : go(k_part_scatter<false, 0>);
+    case 1: return k64 ? go(k_part_scatter<true, 1>) : go(k_part_scatter<false, 1>);
+    case 2: return k64 ? go(k_part_scatter<true, 2>) : go(k_part_scatter<false, 2>);
+    case 3: return k64 ? go(k_part_scatter<true, 3>) : go(k_part_scatter<false, 3>);
+    case 4: return k64 ? go(k_part_scatter<true, 4>) : go(k_part_scatter<false, 4>);
   }
-  return cudaGetLastError();
+  return cudaErrorInvalidValue;
 }
 
 cudaError_t gba_launch_part_agg(const PartAgg& a, int grid, cudaStream_t s) {
