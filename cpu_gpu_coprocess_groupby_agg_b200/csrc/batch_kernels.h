@@ -12,26 +12,30 @@ struct BatchQ {
   int pad;          // bit 0: keys and columns 16-byte aligned (vector loads)
 };
 
-// One work-queue item: a row range of one query.
-struct BatchItem {
+// The work-queue items of one query, described at once: items first_item ..
+// of item_rows rows each (the last one shorter) over query qi's rows.  A
+// launch takes its queries' spans in queue order; item it belongs to the last
+// span whose first_item <= it.
+struct BatchSpan {
   int qi;
   int pad;
-  int64_t row_begin, row_end;
+  int64_t item_rows;
+  int64_t first_item;
 };
 
 size_t gba_batch_static_smem();
 // which compiled signature serves q (queries with equal ids share a launch)
 int gba_batch_sig_id(const QDesc& q);
-// Streaming aggregation (k_stream.cu): one persistent launch over work items
-// (d_items == nullptr: query d_qs[0] cut into items of item_rows rows, a
-// multiple of 256).  *item_ctr must be zero at launch.  minb = CTAs per SM the
-// launch is built for: 1 (512 threads with the whole shared memory and all
-// registers) or 2 (two such CTAs, each with half of both).
+// Streaming aggregation (k_stream.cu): one persistent launch over the nitems
+// work items of nspans query spans (item_rows a multiple of 256).  *item_ctr
+// must be zero at launch.  minb = CTAs per SM the launch is built for: 1 (512
+// threads with the whole shared memory and all registers), 2 or 4 (that many
+// such CTAs, each with its share of both).
 size_t gba_stream_smem_bytes(const QDesc& q, int S);
 int gba_stream_rows_per_chunk(const QDesc& q, int minb);
 cudaError_t gba_prepare_stream_agg(const QDesc& proto, int minb);
-cudaError_t gba_launch_stream_agg(const QDesc& proto, int minb, const BatchQ* d_qs, const BatchItem* d_items,
-                                  int nitems, int64_t item_rows, unsigned* item_ctr, size_t smem, int sprobe, int grid,
+cudaError_t gba_launch_stream_agg(const QDesc& proto, int minb, const BatchQ* d_qs, const BatchSpan* d_spans,
+                                  int nspans, int64_t nitems, unsigned* item_ctr, size_t smem, int sprobe, int grid,
                                   cudaStream_t s);
 // blk_prefix[i]: first block of query i (nq + 1 entries, blk_prefix[nq] = nblocks)
 cudaError_t gba_launch_batch_init(const BatchQ* d_qs, const int64_t* blk_prefix, int nq, int64_t nblocks,

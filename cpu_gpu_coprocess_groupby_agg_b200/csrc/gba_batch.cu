@@ -67,7 +67,8 @@ struct Group {
   QDesc proto;
   std::vector<int> members;  // indices into the batch's queries
   size_t smem = 0;           // dynamic shared memory of the group's launch
-  int64_t item_begin = 0, nitems = 0;
+  int64_t item_begin = 0, nitems = 0;  // item_begin: index of the group's first span
+  int nspans = 0;
   int grid = 0;
 };
 
@@ -172,12 +173,12 @@ extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_
   }
   // work items are cut at multiples of T rows (vector loads need aligned starts)
   const int T = 2048;
-  // CTAs per SM of the streaming kernel (1, 2 or 4; automatic: 2).  More CTAs
+  // CTAs per SM of the streaming kernel (1, 2 or 4; automatic: 4).  More CTAs
   // split each SM's shared memory and registers into smaller tables and fewer
   // rows per lane, but keep more warps and L2 requests in flight: measured on
-  // the 256-query batch, the kernel takes 16.4 ms at 1, 11.1 ms at 2 and
-  // 10.5 ms at 4 (where registers start to spill).
-  const int bps = k.blocks_per_sm == 1 ? 1 : (k.blocks_per_sm == 4 ? 4 : 2);
+  // the 256-query batch, the kernel takes 16.4 ms at 1, 11.1-12.3 ms at 2 and
+  // 10.3 ms at 4 (where some registers spill).
+  const int bps = k.blocks_per_sm == 1 ? 1 : (k.blocks_per_sm == 2 ? 2 : 4);
   // buckets probed in a shared table before a row goes to the HBM table
   const int sprobe = k.smem_probe_cap > 0 ? k.smem_probe_cap : 2;
   for (int i = 0; i < nq; ++i) {
@@ -230,17 +231,29 @@ extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_
   // item_rows or 2^20 rows), so one query occupies the whole grid.
   const int grid_max = ctx->sms * bps;
   const int64_t item_cap = k.item_rows > 0 ? std::max<int64_t>(T, int64_t(k.item_rows)) : (int64_t(1) << 20);
-  std::vector<BatchItem> items;
+  std::vector<BatchSpan> spans;
   for (auto& g : groups) {
-    g.item_begin = int64_t(items.size());
+    g.item_begin = int64_t(spans.size());  // the group's first span
     std::vector<int> order = g.members;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return qd[a].n > qd[b].n; });
+    int64_t first = 0;
     for (int i : order) {
       int64_t ir = (qd[i].n + grid_max - 1) / grid_max;
+      // an item ends by merging its shared table into HBM (one insert per
+      // group it saw, up to S): items of at least 16 such merges' worth of
+      // rows keep that merge a small share of the item's L2 traffic
+      const int64_t merges =
+          qi[i].S > 0 ? int64_t(std::min<double>(qi[i].pred > 0 ? qi[i].pred : double(qi[i].S), double(qi[i].S)))
+                      : 0;
+      ir = std::max<int64_t>(ir, 16 * merges);
       ir = std::min(item_cap, std::max<int64_t>(T, (ir + T - 1) / T * T));
-      for (int64_t r = 0; r < qd[i].n; r += ir) items.push_back(BatchItem{qi[i].slot, 0, r, std::min(qd[i].n, r + ir)});
+      const int64_t nit = (qd[i].n + ir - 1) / ir;
+      if (nit == 0) continue;
+      spans.push_back(BatchSpan{qi[i].slot, 0, ir, first});
+      first += nit;
     }
-    g.nitems = int64_t(items.size()) - g.item_begin;
+    g.nspans = int(int64_t(spans.size()) - g.item_begin);
+    g.nitems = first;
     g.grid = int(std::max<int64_t>(1, std::min<int64_t>(g.nitems, grid_max)));
   }
   const int ng = int(groups.size());
@@ -253,7 +266,7 @@ extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_
     return o;
   };
   const size_t o_q = take(sizeof(BatchQ) * size_t(nt));
-  const size_t o_items = take(sizeof(BatchItem) * items.size());
+  const size_t o_items = take(sizeof(BatchSpan) * spans.size());
   const size_t o_ipre = take(8 * size_t(nt + 1));
   const size_t o_cpre = take(8 * size_t(nt + 1));
   const size_t desc_bytes = off;
@@ -301,14 +314,14 @@ extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_
       b.pad = (vec ? 1 : 0) | (nbk << 8);  // bit 0: columns allow vector loads
       hq[j] = b;
     }
-    if (!items.empty()) std::memcpy(h + o_items, items.data(), sizeof(BatchItem) * items.size());
+    if (!spans.empty()) std::memcpy(h + o_items, spans.data(), sizeof(BatchSpan) * spans.size());
     std::memcpy(h + o_ipre, ipre.data(), 8 * size_t(nt + 1));
     std::memcpy(h + o_cpre, cpre.data(), 8 * size_t(nt + 1));
   }
 
   // ---- the launch sequence (direct or as a replayed graph) ----
   const BatchQ* d_qs = reinterpret_cast<const BatchQ*>(d + o_q);
-  const BatchItem* d_items = reinterpret_cast<const BatchItem*>(d + o_items);
+  const BatchSpan* d_spans = reinterpret_cast<const BatchSpan*>(d + o_items);
   unsigned* d_ctr = reinterpret_cast<unsigned*>(d + o_stat + 16 * size_t(nt));
   // with timing on, events around the three kernel roles (recorded as graph
   // nodes when captured): [0] table init, [1] pre-aggregation, [2] compaction
@@ -327,8 +340,8 @@ extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_
       e = gba_launch_batch_init(d_qs, reinterpret_cast<const int64_t*>(d + o_ipre), nt, ipre[nt], cs);
     if (e == cudaSuccess) e = mark(1, cs);
     for (int g = 0; g < ng && e == cudaSuccess; ++g)
-      e = gba_launch_stream_agg(groups[g].proto, bps, d_qs, d_items + groups[g].item_begin, int(groups[g].nitems),
-                                0, d_ctr + g, groups[g].smem, sprobe, groups[g].grid, cs);
+      e = gba_launch_stream_agg(groups[g].proto, bps, d_qs, d_spans + groups[g].item_begin, groups[g].nspans,
+                                groups[g].nitems, d_ctr + g, groups[g].smem, sprobe, groups[g].grid, cs);
     if (e == cudaSuccess) e = mark(2, cs);
     if (e == cudaSuccess)
       e = gba_launch_batch_compact(d_qs, reinterpret_cast<const int64_t*>(d + o_cpre), nt, cpre[nt], cs);
@@ -343,7 +356,7 @@ extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_
     if (as_graph) {
       // the graph depends only on launch shapes and buffer addresses
       std::vector<int64_t> key = {nt,
-                                  int64_t(items.size()),
+                                  int64_t(spans.size()),
                                   ipre[nt],
                                   cpre[nt],
                                   int64_t(desc_bytes),
@@ -358,6 +371,7 @@ extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_
         key.push_back(int64_t(g.smem));
         key.push_back(g.item_begin);
         key.push_back(g.nitems);
+        key.push_back(g.nspans);
         key.push_back(g.grid);
       }
       if (!ctx->batch_exec || key != ctx->batch_key) {

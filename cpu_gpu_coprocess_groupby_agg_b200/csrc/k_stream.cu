@@ -319,32 +319,38 @@ __device__ __forceinline__ void stream_chunk(const BatchQ& bq, const SmemTable<K
   }
 }
 
-// Persistent streaming aggregation over a work queue of items.  items ==
-// nullptr means one query (qs[0]) cut into items of `item_rows` rows.
+// Persistent streaming aggregation over a work queue of items given as query
+// spans (see BatchSpan).
 // sprobe: buckets probed before a row goes to the HBM table (BatchQ.pad bits
 // 8..15 override it per query when nonzero).
 template <bool K64, typename Sig, int MINB>
-__global__ void __launch_bounds__(512, MINB) k_stream_agg(const BatchQ* qs, const BatchItem* items, int nitems,
-                                                       int64_t item_rows, unsigned* item_ctr, int sprobe) {
+__global__ void __launch_bounds__(512, MINB) k_stream_agg(const BatchQ* qs, const BatchSpan* spans, int nspans,
+                                                          int64_t nitems, unsigned* item_ctr, int sprobe) {
   extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ int s_item;
+  __shared__ unsigned s_item;
   __shared__ unsigned long long s_next;
   __shared__ __align__(16) BatchQ s_q;
   constexpr int R = stream_rows_per_lane<Sig, MINB>();
   const int tid = threadIdx.x;
   for (;;) {
-    if (tid == 0) s_item = int(atomicAdd(item_ctr, 1u));
+    if (tid == 0) s_item = atomicAdd(item_ctr, 1u);
     __syncthreads();
-    const int it = s_item;
+    const int64_t it = int64_t(s_item);
     if (it >= nitems) break;
-    BatchItem item;
-    if (items) {
-      item = items[it];
-    } else {
-      item.qi = 0;
-      item.row_begin = int64_t(it) * item_rows;
-      item.row_end = item.row_begin + item_rows < qs[0].q.n ? item.row_begin + item_rows : qs[0].q.n;
+    int lo = 0, hi = nspans - 1;
+    while (lo < hi) {  // last span starting at or before item it
+      const int mid = (lo + hi + 1) >> 1;
+      if (spans[mid].first_item <= it) lo = mid;
+      else hi = mid - 1;
     }
+    const BatchSpan sp = spans[lo];
+    struct {
+      int qi;
+      int64_t row_begin, row_end;
+    } item;
+    item.qi = sp.qi;
+    item.row_begin = (it - sp.first_item) * sp.item_rows;
+    item.row_end = item.row_begin + sp.item_rows < qs[sp.qi].q.n ? item.row_begin + sp.item_rows : qs[sp.qi].q.n;
     {
       const unsigned* src = reinterpret_cast<const unsigned*>(qs + item.qi);
       unsigned* dst = reinterpret_cast<unsigned*>(&s_q);
@@ -396,17 +402,17 @@ cudaError_t gba_prepare_stream_agg(const QDesc& proto, int minb) {
   });
 }
 
-cudaError_t gba_launch_stream_agg(const QDesc& proto, int minb, const BatchQ* d_qs, const BatchItem* d_items,
-                                  int nitems, int64_t item_rows, unsigned* item_ctr, size_t smem, int sprobe, int grid,
+cudaError_t gba_launch_stream_agg(const QDesc& proto, int minb, const BatchQ* d_qs, const BatchSpan* d_spans,
+                                  int nspans, int64_t nitems, unsigned* item_ctr, size_t smem, int sprobe, int grid,
                                   cudaStream_t s) {
-  if (nitems <= 0) return cudaSuccess;
+  if (nitems <= 0 || nspans <= 0) return cudaSuccess;
   return gba_dispatch_sig(proto, [&](auto K, auto sig) -> cudaError_t {
     constexpr bool k64 = decltype(K)::value;
     using Sig = decltype(sig);
-    if (minb == 4) k_stream_agg<k64, Sig, 4><<<grid, 512, smem, s>>>(d_qs, d_items, nitems, item_rows, item_ctr, sprobe);
+    if (minb == 4) k_stream_agg<k64, Sig, 4><<<grid, 512, smem, s>>>(d_qs, d_spans, nspans, nitems, item_ctr, sprobe);
     else if (minb == 2)
-      k_stream_agg<k64, Sig, 2><<<grid, 512, smem, s>>>(d_qs, d_items, nitems, item_rows, item_ctr, sprobe);
-    else k_stream_agg<k64, Sig, 1><<<grid, 512, smem, s>>>(d_qs, d_items, nitems, item_rows, item_ctr, sprobe);
+      k_stream_agg<k64, Sig, 2><<<grid, 512, smem, s>>>(d_qs, d_spans, nspans, nitems, item_ctr, sprobe);
+    else k_stream_agg<k64, Sig, 1><<<grid, 512, smem, s>>>(d_qs, d_spans, nspans, nitems, item_ctr, sprobe);
     return cudaGetLastError();
   });
 }
