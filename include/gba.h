@@ -229,7 +229,8 @@ gba_status gba_autotune(gba_context* ctx, int32_t n_queries, const gba_query* qs
  * host workers, each with its own CUDA stream and context, so their work
  * overlaps on the device and each keeps its tables and workspace resident
  * between requests (lanes run without CUDA graphs: knobs.use_graph is
- * ignored).  Submitted requests (device columns in, device output
+ * ignored; knobs.blocks_per_sm defaults to 2 so that two lanes' batch kernels
+ * fit on the GPU together).  Submitted requests (device columns in, device output
  * columns out, as gba_groupby) queue in arrival order; a free lane takes the
  * head of the queue and, when it is small (n_rows <= batch_rows), every
  * following small request (up to max_batch) that still fits the budget, and
