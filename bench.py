@@ -280,7 +280,8 @@ def main():
     traffic = None
     tfile = ROOT / "profiles" / "traffic.json"
     if tfile.exists():
-        traffic = json.loads(tfile.read_text()).get(f"{w.name}:k_preagg")
+        traffic = json.loads(tfile.read_text()).get(
+            f"{w.name}:{'k_part_agg' if res.stats['strategy'] == 2 else 'k_preagg'}")
     whole_bytes = w.n * w.row_bytes() + G * w.out_row_bytes()
 
     line = {
@@ -293,7 +294,8 @@ def main():
                    "strategy": res.stats["strategy"], "table_slots": res.stats["table_slots"],
                    "l2": "inputs larger than L2 (no flush needed)", "parallelism": f"replicas x{ws}"},
         "whole_step_hbm_gbs": round(whole_bytes / (ms_step / 1e3) / 1e9, 1),
-        "roofline": {"bound": "hbm", "kernel": "k_preagg", "achieved": round(achieved, 1) if achieved else None,
+        "roofline": {"bound": "hbm", "kernel": "k_part_agg" if res.stats["strategy"] == 2 else "k_preagg",
+                     "achieved": round(achieved, 1) if achieved else None,
                      "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4) if achieved else None,
                      "peak_kind": peak_kind, "traffic": traffic,
                      "alg_bytes_per_launch": alg_bytes, "launch_ms": round(main_avg, 4)},
