@@ -140,32 +140,35 @@ __device__ __forceinline__ void smem_apply_rows(const SmemTable<K64>& t, const Q
 #pragma unroll
   for (int a = 0; a < Sig::NA; ++a) {
     const int op = Sig::op(q, a);
-    unsigned long long* base = t.acc + size_t(Sig::woff(q, a)) * t.S;
+    const int w = Sig::woff(q, a);
+    // split word: low halves at lo32[slot], high halves at lo32[S + slot]
+    unsigned* lo32 = reinterpret_cast<unsigned*>(t.acc + size_t(w) * t.S);
     if (op == ACC_CNT) {
 #pragma unroll
       for (int i = 0; i < R; ++i)
-        if (rows >> i & 1u) atomicAdd(reinterpret_cast<unsigned*>(base + slot[i]), unsigned(v[i][a]));
+        if (rows >> i & 1u) atomicAdd(lo32 + slot[i], unsigned(v[i][a]));
     } else if (op == ACC_ADD_I) {
       unsigned old[R];
 #pragma unroll
       for (int i = 0; i < R; ++i) {
         old[i] = 0u;
-        if (rows >> i & 1u) old[i] = atomicAdd(reinterpret_cast<unsigned*>(base + slot[i]), unsigned(v[i][a]));
+        if (rows >> i & 1u) old[i] = atomicAdd(lo32 + slot[i], unsigned(v[i][a]));
       }
 #pragma unroll
       for (int i = 0; i < R; ++i) {
         if (!(rows >> i & 1u)) continue;
         const unsigned lo = unsigned(v[i][a]), hi = unsigned(v[i][a] >> 32);
         const unsigned add_hi = hi + ((old[i] + lo) < old[i] ? 1u : 0u);
-        if (add_hi) atomicAdd(reinterpret_cast<unsigned*>(base + slot[i]) + 1, add_hi);
+        if (add_hi) atomicAdd(lo32 + t.S + slot[i], add_hi);
       }
     } else {
 #pragma unroll
       for (int i = 0; i < R; ++i) {
         if (!(rows >> i & 1u)) continue;
-        unsigned long long* w0 = base + slot[i];
-        if (op == ACC_ADD_F) smem_fsum(w0, size_t(t.S), __longlong_as_double(v[i][a]));
-        else smem_acc(op, w0, v[i][a]);
+        if (op == ACC_ADD_F)
+          smem_fsum(smem_ref<K64>(t, w, slot[i]), smem_ref<K64>(t, w + 1, slot[i]), smem_ref<K64>(t, w + 2, slot[i]),
+                    __longlong_as_double(v[i][a]));
+        else smem_acc(op, smem_ref<K64>(t, w, slot[i]), v[i][a]);
       }
     }
   }
