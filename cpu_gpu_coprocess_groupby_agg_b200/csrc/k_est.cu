@@ -79,7 +79,7 @@ __device__ __forceinline__ void freq_step(unsigned long long* f, unsigned long l
 }
 
 // one thread per sampled row; per-query count table (keys + counts, linear
-// probing, capacity >= 2x the sample), 64 HLL registers and the frequency
+// probing, capacity 1.5x the sample), 64 HLL registers and the frequency
 // classes.  Lanes of a warp holding the same key add their rows with one
 // atomic from the lowest of them (a skewed column's hot key would otherwise
 // serialise thousands of atomics on one counter).
@@ -403,7 +403,9 @@ void gba_est_plan(EstQuery* e, int64_t n, int64_t tile_rows) {
   e->tile_step = std::max<int64_t>(1, (ntiles + GBA_EST_MAX_TILES - 1) / GBA_EST_MAX_TILES);
   e->sampled_tiles = int((ntiles + e->tile_step - 1) / e->tile_step);
   const uint64_t s_max = uint64_t(e->sampled_tiles) * 1024;
-  e->cap = std::max<uint64_t>(64, gba_pow2_ceil(2 * s_max));
+  // load <= 2/3 (slots are addressed by a multiply-shift, so any capacity
+  // works; a power of two would cost up to 2x the table clear and footprint)
+  e->cap = std::max<uint64_t>(64, s_max + s_max / 2);
 }
 
 // ---- host API ---------------------------------------------------------------------
