@@ -23,7 +23,7 @@ OK, ERR_INVALID_ARG, ERR_CUDA, ERR_OOM, ERR_OUTPUT_CAPACITY, ERR_TABLE_OVERFLOW,
 # gba_type
 I32, I64, F32, U32 = 0, 1, 2, 3
 # gba_op
-SUM, COUNT, MIN, MAX = 0, 1, 2, 3
+SUM, COUNT, MIN, MAX, AVG = 0, 1, 2, 3, 4
 # gba_sizing
 SIZING_PLAIN, SIZING_LEARNED, SIZING_FIXED = 0, 1, 2
 # gba_strategy

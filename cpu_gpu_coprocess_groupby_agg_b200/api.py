@@ -14,7 +14,7 @@ import numpy as np
 
 from . import _abi as A
 
-_OPS = {"sum": A.SUM, "count": A.COUNT, "min": A.MIN, "max": A.MAX}
+_OPS = {"sum": A.SUM, "count": A.COUNT, "min": A.MIN, "max": A.MAX, "avg": A.AVG}
 
 
 def _np_type(a: np.ndarray) -> int:
@@ -40,7 +40,8 @@ def parse_aggs(aggs: Sequence) -> list[tuple[int, int]]:
 
 
 def agg_is_fp(op: int, col_type: int) -> bool:
-    return op == A.SUM and col_type == A.F32
+    """Does the aggregate's output column hold doubles (else int64)?"""
+    return op == A.AVG or (op == A.SUM and col_type == A.F32)
 
 
 def make_knobs(**kw) -> A.Knobs:

@@ -92,6 +92,7 @@ extern "C" gba_status gba_destroy(gba_context* ctx) {
   if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
   if (ctx->h_batch) cudaFreeHost(ctx->h_batch);
   if (ctx->rp_buf) cudaFree(ctx->rp_buf);
+  if (ctx->avg_buf) cudaFree(ctx->avg_buf);
   delete ctx;
   return GBA_OK;
 }
@@ -257,7 +258,7 @@ gba_status gba_build_qdesc(gba_context* ctx, const gba_query* q, QDesc* d) {
     const int t = q->cols[c].type;
     d->acc_col[a] = c;
     d->acc_ctype[a] = t;
-    if (t == GBA_F32) {
+    if (t == GBA_F32 && op != GBA_AVG) {
       if (op != GBA_SUM) {
         ctx->err = "only SUM is supported on fp32 columns";
         return GBA_ERR_UNSUPPORTED;
@@ -266,7 +267,10 @@ gba_status gba_build_qdesc(gba_context* ctx, const gba_query* q, QDesc* d) {
     } else if (op == GBA_SUM) d->acc_op[a] = ACC_ADD_I;
     else if (op == GBA_MIN) d->acc_op[a] = ACC_MIN_I;
     else if (op == GBA_MAX) d->acc_op[a] = ACC_MAX_I;
-    else {
+    else if (op == GBA_AVG) {
+      ctx->err = "AVG is supported by gba_groupby only";
+      return GBA_ERR_UNSUPPORTED;
+    } else {
       ctx->err = "unknown aggregate op";
       return GBA_ERR_INVALID_ARG;
     }
@@ -495,8 +499,74 @@ static gba_status check_output(gba_context* ctx, const gba_query* q, const gba_o
   return GBA_OK;
 }
 
+static gba_status groupby_device(gba_context* ctx, const gba_query* q, const gba_output* out,
+                                 const gba_knobs* knobs, void* stream, int64_t* n_groups);
+
+// AVG: the query runs with each AVG as a SUM into the caller's column and one
+// COUNT (the query's own, or one added into a context buffer); a last kernel
+// turns each SUM column into SUM / COUNT in place.
 extern "C" gba_status gba_groupby(gba_context* ctx, const gba_query* q, const gba_output* out,
                                   const gba_knobs* knobs, void* stream, int64_t* n_groups) {
+  if (!ctx || !q || !n_groups) return GBA_ERR_INVALID_ARG;
+  int navg = 0, cnt = -1;
+  for (int a = 0; a < q->n_aggs && a < GBA_MAX_AGGS; ++a) {
+    navg += q->aggs[a].op == GBA_AVG;
+    if (q->aggs[a].op == GBA_COUNT && cnt < 0) cnt = a;
+  }
+  if (navg == 0) return groupby_device(ctx, q, out, knobs, stream, n_groups);
+  if (!out || out->capacity < 0) return GBA_ERR_INVALID_ARG;
+  cudaSetDevice(ctx->device);
+  gba_query qa = *q;
+  gba_output oa = *out;
+  AvgDesc ad{};
+  for (int a = 0; a < q->n_aggs; ++a) {
+    if (q->aggs[a].op != GBA_AVG) continue;
+    const int c = q->aggs[a].col;
+    if (c < 0 || c >= q->n_cols) {
+      ctx->err = "aggregate column index out of range";
+      return GBA_ERR_INVALID_ARG;
+    }
+    qa.aggs[a].op = GBA_SUM;
+    ad.col[ad.n] = static_cast<unsigned long long*>(out->aggs[a]);
+    ad.fp[ad.n] = q->cols[c].type == GBA_F32;
+    ++ad.n;
+  }
+  if (cnt < 0) {
+    if (qa.n_aggs >= GBA_MAX_AGGS) {
+      ctx->err = "AVG needs a COUNT: at most 7 aggregates with AVG and no COUNT";
+      return GBA_ERR_INVALID_ARG;
+    }
+    const size_t bytes = size_t(std::max<int64_t>(out->capacity, 1)) * 8;
+    if (bytes > ctx->avg_bytes) {
+      if (ctx->avg_buf) {
+        GBA_CUDA_TRY(ctx, cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+        cudaFree(ctx->avg_buf);
+        ctx->avg_buf = nullptr;
+        ctx->avg_bytes = 0;
+      }
+      GBA_CUDA_TRY(ctx, cudaMalloc(&ctx->avg_buf, bytes));
+      ctx->avg_bytes = bytes;
+    }
+    cnt = qa.n_aggs++;
+    qa.aggs[cnt].op = GBA_COUNT;
+    qa.aggs[cnt].col = 0;
+    oa.aggs[cnt] = ctx->avg_buf;
+  }
+  ad.count = static_cast<const unsigned long long*>(oa.aggs[cnt]);
+  gba_status st = groupby_device(ctx, &qa, &oa, knobs, stream, n_groups);
+  if (st != GBA_OK) return st;
+  const int64_t g = std::min<int64_t>(*n_groups, out->capacity);
+  if (g > 0) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    GBA_CUDA_TRY(ctx, gba_launch_avg_finish(ad, g, ctx->sms, s));
+    GBA_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    ctx->stats.kernel_launches += 1;
+  }
+  return GBA_OK;
+}
+
+static gba_status groupby_device(gba_context* ctx, const gba_query* q, const gba_output* out,
+                                 const gba_knobs* knobs, void* stream, int64_t* n_groups) {
   if (!ctx || !q || !n_groups) return GBA_ERR_INVALID_ARG;
   cudaSetDevice(ctx->device);
   ctx->stats = gba_stats{};

@@ -45,6 +45,9 @@ struct gba_context {
   // drop-in API: a tile's groups before the reference-layout partitioning
   void* rp_buf = nullptr;
   size_t rp_bytes = 0;
+  // AVG without a COUNT in the query: the added COUNT's output column
+  void* avg_buf = nullptr;
+  size_t avg_bytes = 0;
   std::string err;
   gba_stats stats{};
 };

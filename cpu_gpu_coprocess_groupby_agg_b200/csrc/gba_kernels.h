@@ -72,6 +72,16 @@ struct PreaggCfg {
   int coalesce;
 };
 
+// AVG finishing pass: col[i][r] (an int64 SUM, or fp64 bits when fp[i]) becomes
+// the double SUM / count[r], for the first n rows.
+struct AvgDesc {
+  unsigned long long* col[GBA_MAX_AGGS];
+  int fp[GBA_MAX_AGGS];
+  int n;
+  const unsigned long long* count;
+};
+cudaError_t gba_launch_avg_finish(const AvgDesc& d, int64_t rows, int sms, cudaStream_t s);
+
 size_t gba_preagg_smem_bytes(const QDesc& q, int S, int T, int nstages, int use_tma);
 cudaError_t gba_launch_table_init(const GTable& t, const QDesc& q, int grid, cudaStream_t s);
 cudaError_t gba_launch_preagg(const QDesc& q, const GTable& t, const PreaggCfg& c, unsigned* flags,

@@ -445,10 +445,29 @@ __global__ void __launch_bounds__(kCompactThreads) k_batch_compact(const BatchQ*
   if (b == 0 && threadIdx.x == 0) compact_side(t, q, o);
 }
 
+__global__ void k_avg_finish(AvgDesc d, int64_t rows) {
+  for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < rows; r += int64_t(gridDim.x) * blockDim.x) {
+    const double c = double(d.count[r]);
+#pragma unroll
+    for (int i = 0; i < GBA_MAX_AGGS; ++i) {
+      if (i >= d.n) break;
+      const unsigned long long x = d.col[i][r];
+      const double sum = d.fp[i] ? __longlong_as_double(x) : double((long long)x);
+      d.col[i][r] = __double_as_longlong(sum / c);
+    }
+  }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
 // Host launchers.
+cudaError_t gba_launch_avg_finish(const AvgDesc& d, int64_t rows, int sms, cudaStream_t s) {
+  const int64_t want = (rows + 255) / 256;
+  k_avg_finish<<<int(want < int64_t(sms) * 8 ? want : int64_t(sms) * 8), 256, 0, s>>>(d, rows);
+  return cudaGetLastError();
+}
+
 size_t gba_preagg_smem_bytes(const QDesc& q, int S, int T, int nstages, int use_tma) {
   size_t b = 128;
   if (use_tma) b += stage_bytes(q, T) * nstages;

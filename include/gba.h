@@ -47,9 +47,12 @@ typedef enum gba_status {
 typedef enum gba_type { GBA_I32 = 0, GBA_I64 = 1, GBA_F32 = 2, GBA_U32 = 3 } gba_type;
 
 /* Aggregates.  SUM/COUNT/MIN/MAX of integer columns accumulate in int64 and are
- * exact (SUM wraps mod 2^64); SUM of an F32 column accumulates in fp64.  The
- * reference computes SUM only, in u32 (kernel.cu:48,152,334). */
-typedef enum gba_op { GBA_SUM = 0, GBA_COUNT = 1, GBA_MIN = 2, GBA_MAX = 3 } gba_op;
+ * exact (SUM wraps mod 2^64); SUM of an F32 column accumulates in fp64.  AVG
+ * (gba_groupby only; the other entry points return GBA_ERR_UNSUPPORTED) is the
+ * double SUM / COUNT of the group: the int64 sum (fp64 for an F32 column)
+ * rounded to double, divided by the row count.  The reference computes SUM
+ * only, in u32 (kernel.cu:48,152,334). */
+typedef enum gba_op { GBA_SUM = 0, GBA_COUNT = 1, GBA_MIN = 2, GBA_MAX = 3, GBA_AVG = 4 } gba_op;
 
 typedef struct gba_column {
   int32_t type;     /* gba_type */
@@ -71,7 +74,8 @@ typedef struct gba_query {
 } gba_query;
 
 /* Output columns: one row per distinct key, in no particular order.  aggs[a]
- * holds capacity 8-byte values: int64, or double for SUM of an F32 column. */
+ * holds capacity 8-byte values: int64, or double for SUM of an F32 column and
+ * for AVG. */
 typedef struct gba_output {
   void* keys;
   void* aggs[GBA_MAX_AGGS];

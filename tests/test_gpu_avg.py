@@ -1,0 +1,75 @@
+"""AVG through gba_groupby: the double SUM / COUNT of each group.
+
+Integer columns: the oracle's exact int64 sum rounded to double and divided by
+the count is the same IEEE computation the kernel does, so the result is
+bit-exact.  fp32 columns: the sums are fp64 in different orders, so the
+averages agree to the fp32-SUM tolerance (1e-6 relative, plus the sum's
+condition-number floor).  AVG is checked with and without a COUNT of its own in
+the query, on the table and the partition strategy, with learned sizing, and
+refused by the batch entry point."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import cpu_oracle as O
+from cpu_gpu_coprocess_groupby_agg_b200 import _abi as A
+from cpu_gpu_coprocess_groupby_agg_b200 import estimator as E
+from gpu_util import FP_ABS_PER_ABSSUM, FP_RTOL, run_gpu, sort_result, to_device
+from test_gpu_parity import _data
+
+pytestmark = pytest.mark.gpu
+
+
+def _expected(keys, cols, col):
+    ok, (s, c) = O.groupby(keys, cols, [("sum", col), ("count", None)], nthreads=8)
+    if s.dtype == np.float64:
+        _, (a,) = O.groupby(keys, cols, [("sumabs", col)], nthreads=8)
+        return ok, s / c.astype(np.float64), a / c.astype(np.float64)
+    return ok, s.astype(np.float64) / c.astype(np.float64), None
+
+
+@pytest.mark.parametrize("strategy", ["table", "partition"])
+@pytest.mark.parametrize("kdt", [np.int32, np.int64])
+def test_avg_matches_oracle(ctx, strategy, kdt):
+    keys, cols = _data(200_003, kdt, 20_000, seed=9, zipf=0.7 if kdt == np.int64 else 0.0)
+    aggs = [("avg", 0), ("sum", 2), ("avg", 2), ("avg", 1), ("max", 0)]  # no COUNT: one is added
+    gk, ga, res = run_gpu(ctx, keys, cols, aggs, knobs=dict(strategy=strategy))
+    gk, ga = sort_result(gk, ga, False)
+    for ai, col in ((0, 0), (2, 2), (3, 1)):
+        ok, avg, abs_avg = _expected(keys, cols, col)
+        np.testing.assert_array_equal(gk, ok)
+        assert ga[ai].dtype == np.float64
+        if abs_avg is None:
+            np.testing.assert_array_equal(ga[ai], avg, err_msg=f"avg of column {col}")
+        else:
+            bound = FP_RTOL * np.abs(avg) + FP_ABS_PER_ABSSUM * abs_avg
+            assert (np.abs(ga[ai] - avg) <= bound).all(), f"avg of fp32 column {col}"
+    ok, (s2, mx) = O.groupby(keys, cols, [("sum", 2), ("max", 0)], nthreads=8)
+    np.testing.assert_array_equal(ga[1], s2)
+    np.testing.assert_array_equal(ga[4], mx)
+
+
+def test_avg_with_count_and_learned_sizing(ctx):
+    if not E.load_default(ctx):
+        pytest.skip("no estimator weights")
+    keys, cols = _data(300_000, np.int64, 50_000, seed=4)
+    aggs = [("count", None), ("avg", 2)]
+    gk, ga, res = run_gpu(ctx, keys, cols, aggs, knobs=dict(sizing="learned", learned_min_rows=-1))
+    assert res.stats["predicted_groups"] > 0
+    gk, ga = sort_result(gk, ga, False)
+    ok, avg, _ = _expected(keys, cols, 2)
+    np.testing.assert_array_equal(gk, ok)
+    np.testing.assert_array_equal(ga[1], avg)
+    _, (c,) = O.groupby(keys, cols, [("count", None)], nthreads=8)
+    np.testing.assert_array_equal(ga[0], c)
+
+
+def test_avg_refused_by_batch(ctx):
+    import torch
+    keys, cols = _data(10_000, np.int64, 100, seed=1)
+    q = [(to_device(keys), [to_device(c) for c in cols], [("avg", 0)])]
+    with pytest.raises(A.GbaError) as e:
+        ctx.groupby_batch(q)
+    assert e.value.status == A.ERR_UNSUPPORTED
+    torch.cuda.synchronize()
