@@ -242,22 +242,7 @@ class Context:
         nq = len(queries)
         if outs is None:
             outs = self.batch_outputs(queries)
-        qarr = (A.Query * max(nq, 1))()
-        oarr = (A.Output * max(nq, 1))()
-        for i, q in enumerate(queries):
-            keys, cols, aggs = q[0], q[1], q[2]
-            uk = bool(q[3]) if len(q) > 3 else False
-            uc = list(q[4]) if len(q) > 4 else []
-            uc += [False] * (len(cols) - len(uc))
-            if not keys.is_cuda:
-                raise ValueError("groupby_batch() takes device tensors")
-            col_specs = [(c.data_ptr(), _torch_type(c, u)) for c, u in zip(cols, uc)]
-            qarr[i] = build_query(keys.numel(), keys.data_ptr(), _torch_type(keys, uk), col_specs, parse_aggs(aggs))
-            okeys, oaggs = outs[i]
-            oarr[i].keys = okeys.data_ptr()
-            for a, t in enumerate(oaggs):
-                oarr[i].aggs[a] = t.data_ptr()
-            oarr[i].capacity = okeys.numel()
+        qarr, oarr = self._batch_arrays(queries, outs)
         kn = knobs if isinstance(knobs, A.Knobs) else make_knobs(**(knobs or {}))
         ng = (C.c_int64 * max(nq, 1))()
         dev = queries[0][0].device if nq else torch.device("cuda", 0)

@@ -268,7 +268,7 @@ gba_status gba_build_qdesc(gba_context* ctx, const gba_query* q, QDesc* d) {
     else if (op == GBA_MIN) d->acc_op[a] = ACC_MIN_I;
     else if (op == GBA_MAX) d->acc_op[a] = ACC_MAX_I;
     else if (op == GBA_AVG) {
-      ctx->err = "AVG is supported by gba_groupby only";
+      ctx->err = "AVG is supported by gba_groupby and gba_groupby_batch only";
       return GBA_ERR_UNSUPPORTED;
     } else {
       ctx->err = "unknown aggregate op";

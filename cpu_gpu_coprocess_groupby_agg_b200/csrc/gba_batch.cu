@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -123,8 +124,87 @@ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) ==
 
 }  // namespace
 
+static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs, const gba_output* outs,
+                               const gba_knobs* knobs, void* stream, int64_t* n_groups);
+
+// AVG, as in gba_groupby: every AVG runs as a SUM into the caller's column,
+// each query with an AVG gets one COUNT (its own, or one added into a slice of
+// a context buffer), and after the batch one kernel per such query turns its
+// SUM columns into SUM / COUNT in place.
 extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_query* qs, const gba_output* outs,
                                         const gba_knobs* knobs, void* stream, int64_t* n_groups) {
+  if (!ctx || nq < 0 || (nq > 0 && (!qs || !outs || !n_groups))) return GBA_ERR_INVALID_ARG;
+  bool any = false;
+  for (int i = 0; i < nq && !any; ++i)
+    for (int a = 0; a < qs[i].n_aggs && a < GBA_MAX_AGGS; ++a) any = any || qs[i].aggs[a].op == GBA_AVG;
+  if (!any) return batch_device(ctx, nq, qs, outs, knobs, stream, n_groups);
+  GBA_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  std::vector<gba_query> q2(qs, qs + nq);
+  std::vector<gba_output> o2(outs, outs + nq);
+  std::vector<AvgDesc> fin(nq);
+  std::vector<int> cnt(nq, -1);
+  std::vector<size_t> scratch_off(nq, SIZE_MAX);  // SIZE_MAX: the query's own COUNT
+  size_t scratch = 0;
+  for (int i = 0; i < nq; ++i) {
+    fin[i] = AvgDesc{};
+    for (int a = 0; a < qs[i].n_aggs && a < GBA_MAX_AGGS; ++a) {
+      if (qs[i].aggs[a].op == GBA_COUNT && cnt[i] < 0) cnt[i] = a;
+      if (qs[i].aggs[a].op != GBA_AVG) continue;
+      const int c = qs[i].aggs[a].col;
+      if (c < 0 || c >= qs[i].n_cols) {
+        ctx->err = "query " + std::to_string(i) + ": aggregate column index out of range";
+        return GBA_ERR_INVALID_ARG;
+      }
+      q2[i].aggs[a].op = GBA_SUM;
+      fin[i].col[fin[i].n] = static_cast<unsigned long long*>(outs[i].aggs[a]);
+      fin[i].fp[fin[i].n] = qs[i].cols[c].type == GBA_F32;
+      ++fin[i].n;
+    }
+    if (fin[i].n > 0 && cnt[i] < 0) {
+      if (q2[i].n_aggs >= GBA_MAX_AGGS) {
+        ctx->err = "query " + std::to_string(i) + ": AVG needs a COUNT: at most 7 aggregates with AVG and no COUNT";
+        return GBA_ERR_INVALID_ARG;
+      }
+      scratch_off[i] = scratch;
+      scratch += size_t(std::max<int64_t>(outs[i].capacity, 1)) * 8;
+      cnt[i] = q2[i].n_aggs++;
+      q2[i].aggs[cnt[i]].op = GBA_COUNT;
+      q2[i].aggs[cnt[i]].col = 0;
+    }
+  }
+  if (scratch > ctx->avg_bytes) {
+    if (ctx->avg_buf) {
+      GBA_CUDA_TRY(ctx, cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+      cudaFree(ctx->avg_buf);
+      ctx->avg_buf = nullptr;
+      ctx->avg_bytes = 0;
+    }
+    GBA_CUDA_TRY(ctx, cudaMalloc(&ctx->avg_buf, scratch));
+    ctx->avg_bytes = scratch;
+  }
+  for (int i = 0; i < nq; ++i) {
+    if (fin[i].n == 0) continue;
+    if (scratch_off[i] != SIZE_MAX)
+      o2[i].aggs[cnt[i]] = static_cast<unsigned char*>(ctx->avg_buf) + scratch_off[i];
+    fin[i].count = static_cast<const unsigned long long*>(o2[i].aggs[cnt[i]]);
+  }
+  gba_status st = batch_device(ctx, nq, q2.data(), o2.data(), knobs, stream, n_groups);
+  if (st != GBA_OK) return st;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int launches = 0;
+  for (int i = 0; i < nq; ++i) {
+    const int64_t g = std::min<int64_t>(n_groups[i], outs[i].capacity);
+    if (fin[i].n == 0 || g <= 0) continue;
+    GBA_CUDA_TRY(ctx, gba_launch_avg_finish(fin[i], g, ctx->sms, s));
+    ++launches;
+  }
+  if (launches) GBA_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+  ctx->stats.kernel_launches += launches;
+  return GBA_OK;
+}
+
+static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs, const gba_output* outs,
+                               const gba_knobs* knobs, void* stream, int64_t* n_groups) {
   if (!ctx || nq < 0 || (nq > 0 && (!qs || !outs || !n_groups))) return GBA_ERR_INVALID_ARG;
   GBA_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   ctx->stats = gba_stats{};

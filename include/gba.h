@@ -48,7 +48,8 @@ typedef enum gba_type { GBA_I32 = 0, GBA_I64 = 1, GBA_F32 = 2, GBA_U32 = 3 } gba
 
 /* Aggregates.  SUM/COUNT/MIN/MAX of integer columns accumulate in int64 and are
  * exact (SUM wraps mod 2^64); SUM of an F32 column accumulates in fp64.  AVG
- * (gba_groupby only; the other entry points return GBA_ERR_UNSUPPORTED) is the
+ * (gba_groupby and gba_groupby_batch; the other entry points return
+ * GBA_ERR_UNSUPPORTED) is the
  * double SUM / COUNT of the group: the int64 sum (fp64 for an F32 column)
  * rounded to double, divided by the row count.  The reference computes SUM
  * only, in u32 (kernel.cu:48,152,334). */

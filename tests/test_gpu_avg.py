@@ -5,15 +5,12 @@ the count is the same IEEE computation the kernel does, so the result is
 bit-exact.  fp32 columns: the sums are fp64 in different orders, so the
 averages agree to the fp32-SUM tolerance (1e-6 relative, plus the sum's
 condition-number floor).  AVG is checked with and without a COUNT of its own in
-the query, on the table and the partition strategy, with learned sizing, and
-refused by the batch entry point."""
-import ctypes as C
-
+the query, on the table and the partition strategy, with learned sizing, and through the
+batch entry point."""
 import numpy as np
 import pytest
 
 import cpu_oracle as O
-from cpu_gpu_coprocess_groupby_agg_b200 import _abi as A
 from cpu_gpu_coprocess_groupby_agg_b200 import estimator as E
 from gpu_util import FP_ABS_PER_ABSSUM, FP_RTOL, run_gpu, sort_result, to_device
 from test_gpu_parity import _data
@@ -65,11 +62,38 @@ def test_avg_with_count_and_learned_sizing(ctx):
     np.testing.assert_array_equal(ga[0], c)
 
 
-def test_avg_refused_by_batch(ctx):
-    import torch
-    keys, cols = _data(10_000, np.int64, 100, seed=1)
-    q = [(to_device(keys), [to_device(c) for c in cols], [("avg", 0)])]
-    with pytest.raises(A.GbaError) as e:
-        ctx.groupby_batch(q)
-    assert e.value.status == A.ERR_UNSUPPORTED
-    torch.cuda.synchronize()
+def test_avg_in_batch(ctx):
+    """gba_groupby_batch: queries with AVG (with and without their own COUNT)
+    beside queries without one, int32 and int64 keys, small and large
+    cardinalities; every AVG against the oracle, every other aggregate exact."""
+    specs = [  # (rows, key dtype, distinct keys, seed, aggs)
+        (50_000, np.int32, 300, 1, [("avg", 0), ("sum", 1)]),
+        (120_000, np.int64, 40_000, 2, [("count", None), ("avg", 2), ("min", 0)]),
+        (30_000, np.int64, 50, 3, [("sum", 1), ("max", 2)]),
+        (80_000, np.int32, 70_000, 4, [("avg", 1), ("avg", 2), ("avg", 0)]),
+        (1_000, np.int64, 1_000, 5, [("avg", 2)]),
+    ]
+    host = [(_data(n, kdt, ndv, seed=sd), aggs) for n, kdt, ndv, sd, aggs in specs]
+    qs = [(to_device(k), [to_device(c) for c in cols], aggs) for (k, cols), aggs in host]
+    res = ctx.groupby_batch(qs)
+    for qi, (((keys, cols), aggs), r) in enumerate(zip(host, res)):
+        gk, ga = sort_result(r.keys.cpu().numpy(), [t.cpu().numpy() for t in r.aggs], False)
+        for ai, (op, col) in enumerate(aggs):
+            msg = f"query {qi} aggregate {ai} ({op})"
+            if op == "avg":
+                ok, avg, abs_avg = _expected(keys, cols, col)
+                np.testing.assert_array_equal(gk, ok, err_msg=msg)
+                assert ga[ai].dtype == np.float64, msg
+                if abs_avg is None:
+                    np.testing.assert_array_equal(ga[ai], avg, err_msg=msg)
+                else:
+                    bound = FP_RTOL * np.abs(avg) + FP_ABS_PER_ABSSUM * abs_avg
+                    assert (np.abs(ga[ai] - avg) <= bound).all(), msg
+            else:
+                ok, (e,) = O.groupby(keys, cols, [(op, col)], nthreads=8)
+                np.testing.assert_array_equal(gk, ok, err_msg=msg)
+                if e.dtype == np.float64:
+                    _, (a,) = O.groupby(keys, cols, [("sumabs", col)], nthreads=8)
+                    assert (np.abs(ga[ai] - e) <= FP_RTOL * np.abs(e) + FP_ABS_PER_ABSSUM * a).all(), msg
+                else:
+                    np.testing.assert_array_equal(ga[ai], e, err_msg=msg)
