@@ -78,6 +78,7 @@ class Knobs(C.Structure):
         ("item_rows", C.c_int32),
         ("learned_load", C.c_double),
         ("learned_min_rows", C.c_int64),
+        ("sort_output", C.c_int32),
     ]
 
 

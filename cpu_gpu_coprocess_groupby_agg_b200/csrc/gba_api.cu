@@ -13,6 +13,7 @@
 
 #include "gba_context.h"
 #include "gba_plan.h"
+#include "sort_kernels.h"
 
 size_t gba_round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 uint64_t gba_pow2_ceil(uint64_t x) {
@@ -502,11 +503,23 @@ static gba_status check_output(gba_context* ctx, const gba_query* q, const gba_o
 static gba_status groupby_device(gba_context* ctx, const gba_query* q, const gba_output* out,
                                  const gba_knobs* knobs, void* stream, int64_t* n_groups);
 
+static gba_status groupby_avg(gba_context* ctx, const gba_query* q, const gba_output* out,
+                              const gba_knobs* knobs, void* stream, int64_t* n_groups);
+
+// Key order (knobs->sort_output) is a device sort of the finished groups.
+extern "C" gba_status gba_groupby(gba_context* ctx, const gba_query* q, const gba_output* out,
+                                  const gba_knobs* knobs, void* stream, int64_t* n_groups) {
+  gba_status st = groupby_avg(ctx, q, out, knobs, stream, n_groups);
+  if (st != GBA_OK || !knobs || !knobs->sort_output) return st;
+  const SortJob j = gba_sort_job(q, out, std::min<int64_t>(*n_groups, out->capacity));
+  return gba_sort_groups(ctx, &j, 1, static_cast<cudaStream_t>(stream));
+}
+
 // AVG: the query runs with each AVG as a SUM into the caller's column and one
 // COUNT (the query's own, or one added into a context buffer); a last kernel
 // turns each SUM column into SUM / COUNT in place.
-extern "C" gba_status gba_groupby(gba_context* ctx, const gba_query* q, const gba_output* out,
-                                  const gba_knobs* knobs, void* stream, int64_t* n_groups) {
+static gba_status groupby_avg(gba_context* ctx, const gba_query* q, const gba_output* out,
+                              const gba_knobs* knobs, void* stream, int64_t* n_groups) {
   if (!ctx || !q || !n_groups) return GBA_ERR_INVALID_ARG;
   int navg = 0, cnt = -1;
   for (int a = 0; a < q->n_aggs && a < GBA_MAX_AGGS; ++a) {

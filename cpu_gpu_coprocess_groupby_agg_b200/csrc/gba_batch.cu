@@ -31,6 +31,7 @@
 #include "est_kernels.h"
 #include "gba_context.h"
 #include "gba_plan.h"
+#include "sort_kernels.h"
 
 namespace {
 
@@ -126,13 +127,26 @@ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) ==
 
 static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs, const gba_output* outs,
                                const gba_knobs* knobs, void* stream, int64_t* n_groups);
+static gba_status batch_avg(gba_context* ctx, int32_t nq, const gba_query* qs, const gba_output* outs,
+                            const gba_knobs* knobs, void* stream, int64_t* n_groups);
+
+// Key order (knobs->sort_output): every query's groups sorted on the device
+// after the batch, one query after another.
+extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_query* qs, const gba_output* outs,
+                                        const gba_knobs* knobs, void* stream, int64_t* n_groups) {
+  gba_status st = batch_avg(ctx, nq, qs, outs, knobs, stream, n_groups);
+  if (st != GBA_OK || !knobs || !knobs->sort_output) return st;
+  std::vector<SortJob> jobs(nq);
+  for (int i = 0; i < nq; ++i) jobs[i] = gba_sort_job(&qs[i], &outs[i], std::min<int64_t>(n_groups[i], outs[i].capacity));
+  return gba_sort_groups(ctx, jobs.data(), nq, static_cast<cudaStream_t>(stream));
+}
 
 // AVG, as in gba_groupby: every AVG runs as a SUM into the caller's column,
 // each query with an AVG gets one COUNT (its own, or one added into a slice of
 // a context buffer), and after the batch one kernel per such query turns its
 // SUM columns into SUM / COUNT in place.
-extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_query* qs, const gba_output* outs,
-                                        const gba_knobs* knobs, void* stream, int64_t* n_groups) {
+static gba_status batch_avg(gba_context* ctx, int32_t nq, const gba_query* qs, const gba_output* outs,
+                            const gba_knobs* knobs, void* stream, int64_t* n_groups) {
   if (!ctx || nq < 0 || (nq > 0 && (!qs || !outs || !n_groups))) return GBA_ERR_INVALID_ARG;
   bool any = false;
   for (int i = 0; i < nq && !any; ++i)

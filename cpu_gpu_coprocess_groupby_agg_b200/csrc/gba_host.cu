@@ -13,6 +13,7 @@
 
 #include "gba_context.h"
 #include "gba_plan.h"
+#include "sort_kernels.h"
 
 static int tbytes(int t) { return t == GBA_I64 ? 8 : 4; }
 
@@ -198,6 +199,11 @@ extern "C" gba_status gba_groupby_host(gba_context* ctx, const gba_query* q, con
     if (st == GBA_ERR_OUTPUT_CAPACITY)
       ctx->err = "output capacity " + std::to_string(out->capacity) + " < " + std::to_string(ng) + " groups";
     return st;
+  }
+  if (k.sort_output && ng > 1) {
+    const SortJob j = gba_sort_job(q, &dout, ng);
+    st = gba_sort_groups(ctx, &j, 1, s);
+    if (st != GBA_OK) return st;
   }
   GBA_CUDA_TRY(ctx, cudaMemcpyAsync(out->keys, dout.keys, size_t(ng) * kb, cudaMemcpyDeviceToHost, s));
   for (int a = 0; a < q->n_aggs; ++a)

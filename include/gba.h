@@ -49,9 +49,8 @@ typedef enum gba_type { GBA_I32 = 0, GBA_I64 = 1, GBA_F32 = 2, GBA_U32 = 3 } gba
 /* Aggregates.  SUM/COUNT/MIN/MAX of integer columns accumulate in int64 and are
  * exact (SUM wraps mod 2^64); SUM of an F32 column accumulates in fp64.  AVG
  * (gba_groupby and gba_groupby_batch; the other entry points return
- * GBA_ERR_UNSUPPORTED) is the
- * double SUM / COUNT of the group: the int64 sum (fp64 for an F32 column)
- * rounded to double, divided by the row count.  The reference computes SUM
+ * GBA_ERR_UNSUPPORTED) is the double SUM / COUNT of the group: the int64 sum
+ * (fp64 for an F32 column) rounded to double, divided by the row count.  The reference computes SUM
  * only, in u32 (kernel.cu:48,152,334). */
 typedef enum gba_op { GBA_SUM = 0, GBA_COUNT = 1, GBA_MIN = 2, GBA_MAX = 3, GBA_AVG = 4 } gba_op;
 
@@ -119,6 +118,10 @@ typedef struct gba_knobs {
   double learned_load;    /* learned sizing: HBM table load at the predicted group count (0 = auto, 0.35) */
   int64_t learned_min_rows; /* single query, learned sizing: smaller queries are sized plainly
                                (0 = auto: while the plain table is <= 256 MB; -1 = always estimate) */
+  int32_t sort_output;    /* gba_groupby, gba_groupby_batch, gba_groupby_host: 1 = groups in ascending key
+                             order (signed for I32/I64 keys, unsigned for U32), sorted on the device;
+                             0 (default) = hash-table order.  No reference counterpart: its partitions
+                             hold their groups in table order (groupby_agg_intra_partition.cu:245-276). */
 } gba_knobs;
 
 /* What the last call on a context did. */
