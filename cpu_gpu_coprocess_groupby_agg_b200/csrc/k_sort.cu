@@ -6,29 +6,36 @@
 // it comes); key order is an option of this library, for callers that join or
 // merge the groups downstream.
 //
-//   k_sort_range    min and max of the order-normalised key (sign bit flipped
-//                   for signed keys): only the bits in which keys differ are
-//                   sorted, 8 per pass, on (key - min)
-//   per pass:
-//   k_sort_hist     digit counts of each 4096-key tile, digit-major
-//                   ([digit][tile]), so that one exclusive scan (k_scan_excl)
-//                   gives every (digit, tile) its output offset
-//   k_sort_scatter  each warp ranks its 512 keys in order, 32 at a time
-//                   (__match_any_sync peers + per-warp digit counters in shared
-//                   memory), the block adds the warps' prefix per digit, and
-//                   every key and its group index goes to its place; order
-//                   inside a digit is the input order, so the sort is stable
+// The pass structure is the single-sweep radix sort published by Adinets and
+// Merrill ("Onesweep", 2022): one upfront read of the keys counts every digit
+// position, and each pass is then one kernel that ranks its tile and finds its
+// global offsets by a decoupled look-back over earlier tiles, per digit.
+//
+//   k_sort_prep     counts of every 8-bit digit of the order-normalised key
+//                   (sign bit flipped for signed keys), all positions at once
+//   k_sort_mask     per job: the digit positions whose keys do not all share
+//                   one digit; only those passes run (one host round trip for
+//                   all jobs of a call)
+//   k_sort_pass     one per pass: a CTA takes the next 4096-key tile from a
+//                   counter, each warp ranks its 512 keys in order, 32 at a
+//                   time (peers of equal digit from 8 ballots; their leader adds them
+//                   to the warp's digit counter in shared memory), the tile publishes its digit counts and
+//                   looks back over earlier tiles for their running totals
+//                   (bounded spin; a timeout raises GBA_FLAG_WAIT_TIMEOUT),
+//                   the tile is staged in shared memory in digit order and
+//                   written out as contiguous runs, one per digit; order inside
+//                   a digit is the input order, so the sort is stable
 //   k_sort_gather   every aggregate column permuted by the sorted group index
 //
-// Bytes per group and pass: read the key twice (count, scatter) and the index
-// once, write key and index once; the gather reads and writes each aggregate
-// word twice (a copy to scratch, then the permuted write back).
+// Bytes per group: the key read once up front; per pass the key and its index
+// read and written once (the first pass reads no index); the gather reads the
+// index and copies each aggregate word to scratch and back through it.
 #include <algorithm>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "gba_internal.cuh"
-#include "part_kernels.h"
 #include "sort_kernels.h"
 
 namespace {
@@ -37,7 +44,12 @@ constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kSortSteps = 16;                        // 32-key steps per warp
 constexpr int kWarpSpan = 32 * kSortSteps;            // a warp's keys in a tile
-constexpr int kSortTile = kSortThreads * kSortSteps;  // 4096 keys per block
+constexpr int kSortTile = kSortThreads * kSortSteps;  // 4096 keys per tile
+constexpr unsigned long long kAggregate = 1ull << 62;  // look-back word: this tile's count
+constexpr unsigned long long kPrefix = 2ull << 62;     // look-back word: running total through this tile
+constexpr unsigned long long kValue = (1ull << 62) - 1;
+constexpr unsigned kSpinLimit = 1u << 24;   // look-back rounds without progress before giving up
+constexpr int kLookWindow = 8;              // predecessor tiles read per look-back round
 
 template <bool K64>
 __device__ __forceinline__ unsigned long long load_raw(const void* keys, int64_t i) {
@@ -51,105 +63,215 @@ __device__ __forceinline__ void store_raw(void* keys, int64_t i, unsigned long l
   else static_cast<unsigned*>(keys)[i] = unsigned(k);
 }
 
-__device__ __forceinline__ unsigned digit_of(unsigned long long raw, unsigned long long flip, unsigned long long lo,
-                                             int shift) {
-  return unsigned(((raw ^ flip) - lo) >> shift) & 255u;
+__device__ __forceinline__ unsigned digit_of(unsigned long long raw, unsigned long long flip, int shift) {
+  return unsigned((raw ^ flip) >> shift) & 255u;
 }
 
+// hist[p * 256 + d]: keys whose digit p is d.  A warp whose 32 keys share a
+// digit adds 32 once (the common case at the top of a narrow key range).
 template <bool K64>
-__global__ void __launch_bounds__(kSortThreads) k_sort_range(const void* keys, int64_t g, unsigned long long flip,
-                                                             unsigned long long* lo, unsigned long long* hi) {
-  unsigned long long mn = ~0ull, mx = 0;
-  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < g; i += int64_t(gridDim.x) * blockDim.x) {
-    const unsigned long long k = load_raw<K64>(keys, i) ^ flip;
-    mn = k < mn ? k : mn;
-    mx = k > mx ? k : mx;
-  }
+__global__ void __launch_bounds__(kSortThreads) k_sort_prep(const void* keys, int64_t g, unsigned long long flip,
+                                                            unsigned* hist) {
+  constexpr int P = K64 ? 8 : 4;
+  __shared__ unsigned h[P * 256];
+  for (int i = threadIdx.x; i < P * 256; i += kSortThreads) h[i] = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int64_t stride = int64_t(gridDim.x) * kSortThreads;
+  for (int64_t base = int64_t(blockIdx.x) * kSortThreads; base < g; base += stride) {
+    const int64_t i = base + threadIdx.x;
+    const bool ok = i < g;
+    const unsigned long long k = ok ? load_raw<K64>(keys, i) ^ flip : 0ull;
+    const unsigned active = __ballot_sync(~0u, ok);
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const unsigned long long a = __shfl_xor_sync(~0u, mn, o), b = __shfl_xor_sync(~0u, mx, o);
-    mn = a < mn ? a : mn;
-    mx = b > mx ? b : mx;
+    for (int p = 0; p < P; ++p) {
+      const unsigned d = unsigned(k >> (8 * p)) & 255u;
+      const unsigned d0 = __shfl_sync(~0u, d, 0);  // lane 0 is active whenever any lane is
+      if (__all_sync(~0u, !ok || d == d0)) {
+        if (lane == 0) atomicAdd(&h[p * 256 + d], unsigned(__popc(active)));
+      } else if (ok) {
+        atomicAdd(&h[p * 256 + d], 1u);
+      }
+    }
   }
-  if ((threadIdx.x & 31) == 0) {
-    atomicMin(lo, mn);
-    atomicMax(hi, mx);
-  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < P * 256; i += kSortThreads)
+    if (h[i]) atomicAdd(&hist[i], h[i]);
 }
 
-template <bool K64>
-__global__ void __launch_bounds__(kSortThreads) k_sort_hist(const void* keys, int64_t g, unsigned long long flip,
-                                                            unsigned long long lo, int shift, unsigned* counts,
-                                                            int64_t ntiles) {
-  __shared__ unsigned cnt[256];
-  cnt[threadIdx.x] = 0;
+// mask[j] bit p: pass p of job j moves keys (its digit is not the same for all)
+__global__ void __launch_bounds__(kSortThreads) k_sort_mask(const unsigned* hists, const int64_t* gs, int npos,
+                                                            unsigned* mask) {
+  __shared__ unsigned m;
+  if (threadIdx.x == 0) m = 0;
   __syncthreads();
+  const unsigned* h = hists + size_t(blockIdx.x) * 8 * 256;
+  const unsigned g = unsigned(gs[blockIdx.x]);
+  for (int p = 0; p < 8; ++p)
+    if (p < npos && h[p * 256 + threadIdx.x] == g) atomicOr(&m, 1u << p);  // one digit holds every key
+  __syncthreads();
+  if (threadIdx.x == 0) mask[blockIdx.x] = ~m & ((1u << npos) - 1u);
+}
+
+// The lanes whose 8-bit digit equals this lane's, among the lanes with ok set:
+// one ballot per digit bit (the same mask __match_any_sync gives, from plain
+// votes).
+__device__ __forceinline__ unsigned digit_peers(unsigned d, bool ok) {
+  unsigned m = __ballot_sync(~0u, ok);
+#pragma unroll
+  for (int b = 0; b < 8; ++b) {
+    const unsigned v = __ballot_sync(~0u, (d >> b) & 1u);
+    m &= (d >> b) & 1u ? v : ~v;
+  }
+  return m;
+}
+
+// exclusive prefix over the block's 256 threads (one value each)
+__device__ __forceinline__ unsigned long long block_excl256(unsigned long long v, unsigned long long* warp_tot) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int64_t base = int64_t(blockIdx.x) * kSortTile + int64_t(warp) * kWarpSpan + lane;
-#pragma unroll 4
-  for (int step = 0; step < kSortSteps; ++step) {
-    const int64_t i = base + step * 32;
-    const unsigned d = i < g ? digit_of(load_raw<K64>(keys, i), flip, lo, shift) : 256u;
-    const unsigned peers = __match_any_sync(~0u, d);
-    if (d < 256u && lane == __ffs(peers) - 1) atomicAdd(&cnt[d], unsigned(__popc(peers)));
+  unsigned long long x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long y = __shfl_up_sync(~0u, x, o);
+    if (lane >= o) x += y;
   }
+  if (lane == 31) warp_tot[warp] = x;
   __syncthreads();
-  counts[int64_t(threadIdx.x) * ntiles + blockIdx.x] = cnt[threadIdx.x];
+  unsigned long long before = 0;
+#pragma unroll
+  for (int w = 0; w < kSortWarps; ++w)
+    if (w < warp) before += warp_tot[w];
+  __syncthreads();
+  return before + x - v;
 }
 
+struct PassArgs {
+  const void* keys_in;
+  const unsigned* idx_in;   // null: the key's index is its position (first pass)
+  void* keys_out;
+  unsigned* idx_out;
+  int64_t g;
+  unsigned long long flip;
+  int shift;
+  const unsigned* hist;     // this pass's 256 digit counts over all keys
+  unsigned long long* look; // [tile][256] look-back words, zeroed
+  unsigned* tile_ctr;       // zeroed
+  unsigned* flags;
+};
+
 template <bool K64>
-__global__ void __launch_bounds__(kSortThreads) k_sort_scatter(const void* keys_in, const unsigned* idx_in,
-                                                               void* keys_out, unsigned* idx_out, int64_t g,
-                                                               unsigned long long flip, unsigned long long lo,
-                                                               int shift, const unsigned long long* offsets,
-                                                               int64_t ntiles) {
+__global__ void __launch_bounds__(kSortThreads, 3) k_sort_pass(PassArgs a) {
+  using KeyT = typename std::conditional<K64, unsigned long long, unsigned>::type;
+  extern __shared__ __align__(16) unsigned char stage[];
+  KeyT* skeys = reinterpret_cast<KeyT*>(stage);
+  unsigned* sidx = reinterpret_cast<unsigned*>(stage + sizeof(KeyT) * kSortTile);
   __shared__ unsigned wcnt[kSortWarps][256];
-  __shared__ unsigned long long dbase[256];
+  __shared__ unsigned dstart[256];
+  __shared__ unsigned long long gbase[256];
+  __shared__ unsigned long long warp_tot[kSortWarps];
+  __shared__ unsigned s_tile;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  if (t == 0) s_tile = atomicAdd(a.tile_ctr, 1u);
 #pragma unroll
-  for (int w = 0; w < kSortWarps; ++w) wcnt[w][threadIdx.x] = 0;
-  dbase[threadIdx.x] = offsets[int64_t(threadIdx.x) * ntiles + blockIdx.x];
+  for (int w = 0; w < kSortWarps; ++w) wcnt[w][t] = 0;
   __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t tile = s_tile;
+  const int64_t tile0 = tile * kSortTile;
+  const int tile_n = a.g - tile0 < kSortTile ? int(a.g - tile0) : kSortTile;
+
+  // rank every key among the tile's keys of the same digit, in input order
   const unsigned lt = (1u << lane) - 1u;
-  const int64_t base = int64_t(blockIdx.x) * kSortTile + int64_t(warp) * kWarpSpan + lane;
-  unsigned long long key[kSortSteps];
+  const int64_t base = tile0 + int64_t(warp) * kWarpSpan + lane;
+  KeyT key[kSortSteps];
   unsigned idx[kSortSteps], rank[kSortSteps];
 #pragma unroll
   for (int step = 0; step < kSortSteps; ++step) {
     const int64_t i = base + step * 32;
-    const bool ok = i < g;
-    key[step] = ok ? load_raw<K64>(keys_in, i) : 0ull;
-    idx[step] = ok ? (idx_in ? __ldg(idx_in + i) : unsigned(i)) : 0u;
+    const bool ok = i < a.g;
+    key[step] = ok ? KeyT(load_raw<K64>(a.keys_in, i)) : KeyT(0);
+    idx[step] = ok ? (a.idx_in ? __ldg(a.idx_in + i) : unsigned(i)) : 0u;
   }
 #pragma unroll
   for (int step = 0; step < kSortSteps; ++step) {
-    const bool ok = base + step * 32 < g;
-    const unsigned d = ok ? digit_of(key[step], flip, lo, shift) : 256u;
-    const unsigned peers = __match_any_sync(~0u, d);
-    const unsigned before = ok ? wcnt[warp][d] : 0u;
-    __syncwarp();
-    if (ok && lane == __ffs(peers) - 1) wcnt[warp][d] = before + unsigned(__popc(peers));
-    __syncwarp();
+    const bool ok = base + step * 32 < a.g;
+    const unsigned d = ok ? digit_of(key[step], a.flip, a.shift) : 0u;
+    const unsigned peers = digit_peers(d, ok);
+    const int leader = __ffs(peers) - 1;
+    // the leader's atomic returns the count before this step; steps do not
+    // wait on one another (the warp's counter row is touched by it alone)
+    unsigned before = 0;
+    if (ok && lane == leader) before = atomicAdd(&wcnt[warp][d], unsigned(__popc(peers)));
+    before = __shfl_sync(~0u, before, leader);
     rank[step] = before + unsigned(__popc(peers & lt));
   }
   __syncthreads();
-  {
-    unsigned run = 0;
+
+  // thread t owns digit t: warp prefix, tile count, publish, look back
+  unsigned total = 0;
 #pragma unroll
-    for (int w = 0; w < kSortWarps; ++w) {
-      const unsigned c = wcnt[w][threadIdx.x];
-      wcnt[w][threadIdx.x] = run;
-      run += c;
-    }
+  for (int w = 0; w < kSortWarps; ++w) {
+    const unsigned c = wcnt[w][t];
+    wcnt[w][t] = total;
+    total += c;
   }
+  unsigned long long* look = a.look + size_t(tile) * 256 + t;
+  if (tile == 0) atomicExch(look, kPrefix | total);
+  else atomicExch(look, kAggregate | total);
+  const unsigned long long gstart = block_excl256(a.hist[t], warp_tot);
+  dstart[t] = unsigned(block_excl256(total, warp_tot));
+  unsigned long long excl = 0;
+  if (tile > 0) {
+    // walk back kLookWindow tiles per round of independent loads (the tiles of
+    // the first wave all publish at once; one dependent load per tile would
+    // make their walks serial)
+    int64_t j = tile - 1;
+    unsigned spins = 0;
+    while (true) {
+      unsigned long long w[kLookWindow];
+#pragma unroll
+      for (int u = 0; u < kLookWindow; ++u)
+        w[u] = j - u >= 0 ? *reinterpret_cast<const volatile unsigned long long*>(a.look + size_t(j - u) * 256 + t)
+                          : kPrefix;  // before tile 0: a running total of zero
+      int used = 0;
+      bool done = false;
+#pragma unroll
+      for (int u = 0; u < kLookWindow; ++u) {
+        if (done || used < u) continue;        // stopped earlier in this window
+        const unsigned long long f = w[u] & ~kValue;
+        if (f == 0ull) continue;               // tile j - u has not published yet
+        excl += w[u] & kValue;
+        done = f == kPrefix;
+        used = u + 1;
+      }
+      if (done) break;
+      if (used == 0 && ++spins > kSpinLimit) {
+        atomicOr(a.flags, GBA_FLAG_WAIT_TIMEOUT);
+        break;
+      }
+      j -= used;
+    }
+    atomicExch(look, kPrefix | (excl + total));
+  }
+  gbase[t] = gstart + excl;
   __syncthreads();
+
+  // stage the tile in digit order, then write each digit's run contiguously
 #pragma unroll
   for (int step = 0; step < kSortSteps; ++step) {
-    if (base + step * 32 >= g) continue;
-    const unsigned d = digit_of(key[step], flip, lo, shift);
-    const int64_t pos = int64_t(dbase[d]) + wcnt[warp][d] + rank[step];
-    store_raw<K64>(keys_out, pos, key[step]);
-    idx_out[pos] = idx[step];
+    if (base + step * 32 >= a.g) continue;
+    const unsigned d = digit_of(key[step], a.flip, a.shift);
+    const unsigned pos = dstart[d] + wcnt[warp][d] + rank[step];
+    skeys[pos] = KeyT(key[step]);
+    sidx[pos] = idx[step];
+  }
+  __syncthreads();
+  for (int i = t; i < tile_n; i += kSortThreads) {
+    const unsigned long long k = skeys[i];
+    const unsigned d = digit_of(k, a.flip, a.shift);
+    const unsigned long long gpos = gbase[d] + unsigned(i - int(dstart[d]));
+    if (gpos >= (unsigned long long)a.g) continue;  // only after a timed-out look-back
+    store_raw<K64>(a.keys_out, int64_t(gpos), k);
+    a.idx_out[gpos] = sidx[i];
   }
 }
 
@@ -170,22 +292,21 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_gather(GatherCols c, cons
 
 size_t a256(size_t x) { return (x + 255) & ~size_t(255); }
 
+size_t stage_bytes(bool key64) { return size_t(kSortTile) * ((key64 ? 8 : 4) + 4); }
+
 struct SortLayout {
-  size_t keys_alt, idx0, idx1, counts, offsets, status, tile_ctr, aggs, bytes;
+  size_t keys_alt, idx0, idx1, look, ctr, aggs, bytes;
 };
 
 SortLayout layout_for(const SortJob& j, size_t base) {
   const int64_t ntiles = (j.g + kSortTile - 1) / kSortTile;
-  const size_t entries = size_t(ntiles) * 256;
   SortLayout L;
   size_t o = base;
   L.keys_alt = o;  o += a256(size_t(j.g) * (j.key64 ? 8 : 4));
   L.idx0 = o;      o += a256(size_t(j.g) * 4);
   L.idx1 = o;      o += a256(size_t(j.g) * 4);
-  L.counts = o;    o += a256(entries * 4);
-  L.offsets = o;   o += a256(entries * 8);
-  L.status = o;    o += a256((entries / 1024 + 2) * 8);  // look-back scan: one word per scan tile (>= 1024 entries)
-  L.tile_ctr = o;  o += 256;
+  L.look = o;      o += a256(size_t(ntiles) * 256 * 8);
+  L.ctr = o;       o += 256;  // one tile counter per pass
   L.aggs = o;      o += a256(size_t(j.g) * 8) * size_t(j.nagg);
   L.bytes = o - base;
   return L;
@@ -206,70 +327,88 @@ gba_status gba_sort_groups(gba_context* ctx, const SortJob* jobs, int njobs, cud
     per_job = std::max(per_job, layout_for(jobs[j], 0).bytes);
   }
   if (todo.empty()) return GBA_OK;
-  const size_t nt = todo.size();
-  const size_t ranges = a256(nt * 16);
-  gba_status st = gba_ws_reserve(ctx, ranges + per_job, s);
+  const int nt = int(todo.size());
+  // front of the workspace: every job's digit counts, group count and pass mask
+  const size_t o_hist = 0, o_g = a256(size_t(nt) * 8 * 256 * 4), o_mask = o_g + a256(size_t(nt) * 8);
+  const size_t front = o_mask + a256(size_t(nt) * 4);
+  gba_status st = gba_ws_reserve(ctx, front + per_job, s);
   if (st != GBA_OK) return st;
-  st = gba_small_reserve(ctx, std::max<size_t>(ctx->d_small_bytes, 64 + nt * 16));
+  st = gba_small_reserve(ctx, std::max<size_t>(ctx->d_small_bytes, 64 + size_t(nt) * 4));
   if (st != GBA_OK) return st;
+  static const cudaError_t smem_ok = [] {
+    cudaError_t e = gba_allow_max_smem(k_sort_pass<true>);
+    return e != cudaSuccess ? e : gba_allow_max_smem(k_sort_pass<false>);
+  }();
+  GBA_CUDA_TRY(ctx, smem_ok);
   unsigned char* W = static_cast<unsigned char*>(ctx->ws);
-  unsigned long long* d_lo = reinterpret_cast<unsigned long long*>(W);
-  unsigned long long* d_hi = d_lo + nt;
+  unsigned* d_hist = reinterpret_cast<unsigned*>(W + o_hist);
+  int64_t* d_g = reinterpret_cast<int64_t*>(W + o_g);
+  unsigned* d_mask = reinterpret_cast<unsigned*>(W + o_mask);
   unsigned* d_flags = reinterpret_cast<unsigned*>(ctx->d_small);
-  GBA_CUDA_TRY(ctx, cudaMemsetAsync(d_lo, 0xff, nt * 8, s));
-  GBA_CUDA_TRY(ctx, cudaMemsetAsync(d_hi, 0, nt * 8, s));
+  std::vector<int64_t> gs(nt);
+  for (int t = 0; t < nt; ++t) gs[t] = jobs[todo[t]].g;
+  GBA_CUDA_TRY(ctx, cudaMemsetAsync(d_hist, 0, size_t(nt) * 8 * 256 * 4, s));
+  GBA_CUDA_TRY(ctx, cudaMemcpyAsync(d_g, gs.data(), size_t(nt) * 8, cudaMemcpyHostToDevice, s));
   GBA_CUDA_TRY(ctx, cudaMemsetAsync(d_flags, 0, 4, s));
   int launches = 0;
-  for (size_t t = 0; t < nt; ++t) {
+  bool any64 = false;
+  for (int t = 0; t < nt; ++t) {
     const SortJob& j = jobs[todo[t]];
     const unsigned long long flip = j.key_signed ? (j.key64 ? 1ull << 63 : 1ull << 31) : 0ull;
     const int grid = int(std::min<int64_t>(int64_t(ctx->sms) * 4, (j.g + kSortThreads - 1) / kSortThreads));
-    if (j.key64) k_sort_range<true><<<grid, kSortThreads, 0, s>>>(j.keys, j.g, flip, d_lo + t, d_hi + t);
-    else k_sort_range<false><<<grid, kSortThreads, 0, s>>>(j.keys, j.g, flip, d_lo + t, d_hi + t);
+    if (j.key64) k_sort_prep<true><<<grid, kSortThreads, 0, s>>>(j.keys, j.g, flip, d_hist + size_t(t) * 2048);
+    else k_sort_prep<false><<<grid, kSortThreads, 0, s>>>(j.keys, j.g, flip, d_hist + size_t(t) * 2048);
     GBA_CUDA_TRY(ctx, cudaGetLastError());
+    any64 = any64 || j.key64;
     ++launches;
   }
-  GBA_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_small + 64, d_lo, nt * 16, cudaMemcpyDeviceToHost, s));
+  // 32-bit jobs count 4 positions, 64-bit ones 8: the mask kernel is told the
+  // larger and a 32-bit job's positions 4..7 hold zero counts (never "all")
+  k_sort_mask<<<nt, kSortThreads, 0, s>>>(d_hist, d_g, any64 ? 8 : 4, d_mask);
+  GBA_CUDA_TRY(ctx, cudaGetLastError());
+  ++launches;
+  GBA_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_small + 64, d_mask, size_t(nt) * 4, cudaMemcpyDeviceToHost, s));
   GBA_CUDA_TRY(ctx, cudaStreamSynchronize(s));
-  std::vector<unsigned long long> lo(nt), hi(nt);
-  std::memcpy(lo.data(), ctx->h_small + 64, nt * 8);
-  std::memcpy(hi.data(), ctx->h_small + 64 + nt * 8, nt * 8);
+  std::vector<unsigned> mask(nt);
+  std::memcpy(mask.data(), ctx->h_small + 64, size_t(nt) * 4);
 
-  for (size_t t = 0; t < nt; ++t) {
+  const size_t jb = front;
+  for (int t = 0; t < nt; ++t) {
     const SortJob& j = jobs[todo[t]];
-    const unsigned long long span = hi[t] - lo[t];
-    const int bits = span ? 64 - __builtin_clzll(span) : 0;
-    const int passes = (bits + 7) / 8;
-    if (passes == 0) continue;
+    const unsigned m = mask[t] & (j.key64 ? 0xffu : 0xfu);
+    if (m == 0) continue;
     const unsigned long long flip = j.key_signed ? (j.key64 ? 1ull << 63 : 1ull << 31) : 0ull;
-    const SortLayout L = layout_for(j, ranges);
+    const SortLayout L = layout_for(j, jb);
     const int64_t ntiles = (j.g + kSortTile - 1) / kSortTile;
     void* alt = W + L.keys_alt;
     unsigned* idxb[2] = {reinterpret_cast<unsigned*>(W + L.idx0), reinterpret_cast<unsigned*>(W + L.idx1)};
-    unsigned* counts = reinterpret_cast<unsigned*>(W + L.counts);
-    unsigned long long* offsets = reinterpret_cast<unsigned long long*>(W + L.offsets);
+    unsigned* ctr = reinterpret_cast<unsigned*>(W + L.ctr);
+    GBA_CUDA_TRY(ctx, cudaMemsetAsync(ctr, 0, 8 * 4, s));
     void* cur = j.keys;
     const unsigned* idx_cur = nullptr;
-    for (int p = 0; p < passes; ++p) {
-      const int shift = 8 * p;
-      void* out = cur == j.keys ? alt : j.keys;
-      unsigned* idx_out = idxb[p & 1];
-      if (j.key64) k_sort_hist<true><<<unsigned(ntiles), kSortThreads, 0, s>>>(cur, j.g, flip, lo[t], shift, counts, ntiles);
-      else k_sort_hist<false><<<unsigned(ntiles), kSortThreads, 0, s>>>(cur, j.g, flip, lo[t], shift, counts, ntiles);
+    int np = 0;
+    for (int p = 0; p < 8; ++p) {
+      if (!(m >> p & 1u)) continue;
+      PassArgs a;
+      a.keys_in = cur;
+      a.idx_in = idx_cur;
+      a.keys_out = cur == j.keys ? alt : j.keys;
+      a.idx_out = idxb[np & 1];
+      a.g = j.g;
+      a.flip = flip;
+      a.shift = 8 * p;
+      a.hist = d_hist + size_t(t) * 2048 + size_t(p) * 256;
+      a.look = reinterpret_cast<unsigned long long*>(W + L.look);
+      a.tile_ctr = ctr + p;
+      a.flags = d_flags;
+      GBA_CUDA_TRY(ctx, cudaMemsetAsync(a.look, 0, size_t(ntiles) * 256 * 8, s));
+      if (j.key64) k_sort_pass<true><<<unsigned(ntiles), kSortThreads, stage_bytes(true), s>>>(a);
+      else k_sort_pass<false><<<unsigned(ntiles), kSortThreads, stage_bytes(false), s>>>(a);
       GBA_CUDA_TRY(ctx, cudaGetLastError());
-      GBA_CUDA_TRY(ctx, gba_launch_scan_excl(counts, offsets, ntiles * 256,
-                                             reinterpret_cast<unsigned long long*>(W + L.status),
-                                             reinterpret_cast<unsigned*>(W + L.tile_ctr), d_flags, s));
-      if (j.key64)
-        k_sort_scatter<true><<<unsigned(ntiles), kSortThreads, 0, s>>>(cur, idx_cur, out, idx_out, j.g, flip, lo[t],
-                                                                       shift, offsets, ntiles);
-      else
-        k_sort_scatter<false><<<unsigned(ntiles), kSortThreads, 0, s>>>(cur, idx_cur, out, idx_out, j.g, flip,
-                                                                        lo[t], shift, offsets, ntiles);
-      GBA_CUDA_TRY(ctx, cudaGetLastError());
-      launches += 3;
-      cur = out;
-      idx_cur = idx_out;
+      ++launches;
+      ++np;
+      cur = a.keys_out;
+      idx_cur = a.idx_out;
     }
     if (cur != j.keys)
       GBA_CUDA_TRY(ctx, cudaMemcpyAsync(j.keys, cur, size_t(j.g) * (j.key64 ? 8 : 4), cudaMemcpyDeviceToDevice, s));
@@ -292,7 +431,7 @@ gba_status gba_sort_groups(gba_context* ctx, const SortJob* jobs, int njobs, cud
   GBA_CUDA_TRY(ctx, cudaStreamSynchronize(s));
   ctx->stats.kernel_launches += launches;
   if (*reinterpret_cast<unsigned*>(ctx->h_small) & GBA_FLAG_WAIT_TIMEOUT) {
-    ctx->err = "sort_output: a bounded scan wait timed out";
+    ctx->err = "sort_output: a bounded look-back wait timed out";
     return GBA_ERR_TIMEOUT;
   }
   return GBA_OK;
