@@ -21,7 +21,7 @@ GBA_EST_SAMPLE = 1024
 OK, ERR_INVALID_ARG, ERR_CUDA, ERR_OOM, ERR_OUTPUT_CAPACITY, ERR_TABLE_OVERFLOW, ERR_TIMEOUT, ERR_UNSUPPORTED, \
     ERR_BUDGET = range(9)
 # gba_type
-I32, I64, F32, U32 = 0, 1, 2, 3
+I32, I64, F32, U32, F64 = 0, 1, 2, 3, 4
 # gba_op
 SUM, COUNT, MIN, MAX, AVG = 0, 1, 2, 3, 4
 # gba_sizing

@@ -19,12 +19,12 @@ _OPS = {"sum": A.SUM, "count": A.COUNT, "min": A.MIN, "max": A.MAX, "avg": A.AVG
 
 def _np_type(a: np.ndarray) -> int:
     return {np.dtype(np.int32): A.I32, np.dtype(np.uint32): A.U32, np.dtype(np.int64): A.I64,
-            np.dtype(np.float32): A.F32}[a.dtype]
+            np.dtype(np.float32): A.F32, np.dtype(np.float64): A.F64}[a.dtype]
 
 
 def _torch_type(t, unsigned: bool = False) -> int:
     import torch
-    m = {torch.int32: A.U32 if unsigned else A.I32, torch.int64: A.I64, torch.float32: A.F32}
+    m = {torch.int32: A.U32 if unsigned else A.I32, torch.int64: A.I64, torch.float32: A.F32, torch.float64: A.F64}
     if t.dtype not in m:
         raise TypeError(f"unsupported column dtype {t.dtype}")
     return m[t.dtype]
@@ -41,7 +41,7 @@ def parse_aggs(aggs: Sequence) -> list[tuple[int, int]]:
 
 def agg_is_fp(op: int, col_type: int) -> bool:
     """Does the aggregate's output column hold doubles (else int64)?"""
-    return op == A.AVG or (op == A.SUM and col_type == A.F32)
+    return op == A.AVG or (op == A.SUM and col_type in (A.F32, A.F64))
 
 
 def make_knobs(**kw) -> A.Knobs:

@@ -232,7 +232,7 @@ gba_status gba_build_qdesc(gba_context* ctx, const gba_query* q, QDesc* d) {
   d->ncols = q->n_cols;
   for (int c = 0; c < q->n_cols; ++c) {
     const int t = q->cols[c].type;
-    if (t != GBA_I32 && t != GBA_U32 && t != GBA_I64 && t != GBA_F32) {
+    if (t != GBA_I32 && t != GBA_U32 && t != GBA_I64 && t != GBA_F32 && t != GBA_F64) {
       ctx->err = "bad column type";
       return GBA_ERR_INVALID_ARG;
     }
@@ -259,9 +259,9 @@ gba_status gba_build_qdesc(gba_context* ctx, const gba_query* q, QDesc* d) {
     const int t = q->cols[c].type;
     d->acc_col[a] = c;
     d->acc_ctype[a] = t;
-    if (t == GBA_F32 && op != GBA_AVG) {
+    if ((t == GBA_F32 || t == GBA_F64) && op != GBA_AVG) {
       if (op != GBA_SUM) {
-        ctx->err = "only SUM is supported on fp32 columns";
+        ctx->err = "only SUM (and AVG) are supported on fp32 and fp64 columns";
         return GBA_ERR_UNSUPPORTED;
       }
       d->acc_op[a] = ACC_ADD_F;
@@ -318,7 +318,7 @@ void gba_make_plan(const gba_context* ctx, const QDesc& q, const gba_knobs& k, d
   // peak with one CTA per SM (measured: 2 x 32 KB -> 6.9 TB/s, 3 x 32 KB ->
   // 7.3 TB/s, 2 x 16 KB -> 4.7 TB/s); tiles of at least 24 KB, 2-4 stages
   size_t rb = q.key64 ? 8 : 4;
-  for (int c = 0; c < q.ncols; ++c) rb += q.col_type[c] == GBA_I64 ? 8 : 4;
+  for (int c = 0; c < q.ncols; ++c) rb += gba_type_bytes(q.col_type[c]);
   // Tiles are long enough that the per-tile barriers stay a small share of the
   // work (measured with ncu on 2048-row tiles: barrier stalls dominated).
   int T = 2048;
@@ -541,7 +541,7 @@ static gba_status groupby_avg(gba_context* ctx, const gba_query* q, const gba_ou
     }
     qa.aggs[a].op = GBA_SUM;
     ad.col[ad.n] = static_cast<unsigned long long*>(out->aggs[a]);
-    ad.fp[ad.n] = q->cols[c].type == GBA_F32;
+    ad.fp[ad.n] = q->cols[c].type == GBA_F32 || q->cols[c].type == GBA_F64;
     ++ad.n;
   }
   if (cnt < 0) {

@@ -171,7 +171,7 @@ static gba_status batch_avg(gba_context* ctx, int32_t nq, const gba_query* qs, c
       }
       q2[i].aggs[a].op = GBA_SUM;
       fin[i].col[fin[i].n] = static_cast<unsigned long long*>(outs[i].aggs[a]);
-      fin[i].fp[fin[i].n] = qs[i].cols[c].type == GBA_F32;
+      fin[i].fp[fin[i].n] = qs[i].cols[c].type == GBA_F32 || qs[i].cols[c].type == GBA_F64;
       ++fin[i].n;
     }
     if (fin[i].n > 0 && cnt[i] < 0) {

@@ -15,7 +15,7 @@
 #include "gba_plan.h"
 #include "sort_kernels.h"
 
-static int tbytes(int t) { return t == GBA_I64 ? 8 : 4; }
+static int tbytes(int t) { return gba_type_bytes(t); }
 
 extern "C" gba_status gba_groupby_host(gba_context* ctx, const gba_query* q, const gba_output* out,
                                        const gba_knobs* knobs, void* stream, int64_t* n_groups) {

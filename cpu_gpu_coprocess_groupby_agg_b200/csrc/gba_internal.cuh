@@ -69,13 +69,13 @@ __device__ __forceinline__ uint64_t load_key_g(const QDesc& q, int64_t r) {
 
 // Contribution of row value `raw` (8 raw bytes as loaded) to accumulator a.
 // raw holds the column value bits: i32/u32 in the low word, f32 bits in the low
-// word, i64 in full.
+// word, i64 and f64 in full.
 __device__ __forceinline__ unsigned long long acc_contrib(int op, int ctype, unsigned long long raw) {
   switch (op) {
     case ACC_CNT: return 1ull;
     case ACC_ADD_F: {
-      double d = double(__uint_as_float(unsigned(raw)));
-      return __double_as_longlong(d);
+      if (ctype == GBA_F64) return raw;
+      return __double_as_longlong(double(__uint_as_float(unsigned(raw))));
     }
     default: {
       long long v;

@@ -14,8 +14,11 @@ enum AccOp : int {
   ACC_CNT = 1,    // COUNT, int64
   ACC_MIN_I = 2,  // MIN of an integer column, int64
   ACC_MAX_I = 3,  // MAX of an integer column, int64
-  ACC_ADD_F = 4,  // SUM of an fp32 column, accumulated in fp64
+  ACC_ADD_F = 4,  // SUM of an fp32 or fp64 column, accumulated in fp64
 };
+
+// bytes of one value of a column type
+__host__ __device__ inline int gba_type_bytes(int t) { return t == GBA_I64 || t == GBA_F64 ? 8 : 4; }
 
 // One query as the kernels see it (passed by value in the parameter space).
 struct QDesc {
@@ -30,7 +33,7 @@ struct QDesc {
   int acc_col[GBA_MAX_AGGS];    // source column (0 for COUNT)
   int acc_ctype[GBA_MAX_AGGS];  // type of the source column
   // shared-memory layout: accumulator a starts at word acc_woff[a] of a slot;
-  // fp32 SUM takes 3 words (128-bit exact fixed point + fp64 residual), the
+  // fp SUM takes 3 words (128-bit exact fixed point + fp64 residual), the
   // others 1; nwords = words per slot
   int acc_woff[GBA_MAX_AGGS];
   int nwords;

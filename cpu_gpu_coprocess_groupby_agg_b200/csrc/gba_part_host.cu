@@ -19,7 +19,7 @@
 namespace {
 
 constexpr size_t kAlign = 256;
-int tbytes(int t) { return t == GBA_I64 ? 8 : 4; }
+int tbytes(int t) { return gba_type_bytes(t); }
 
 struct Carver {
   size_t off = 0;

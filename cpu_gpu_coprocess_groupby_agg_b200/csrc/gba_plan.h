@@ -6,7 +6,7 @@
 // bytes of one input row: key + value columns
 inline size_t gba_row_bytes(const QDesc& q) {
   size_t b = q.key64 ? 8 : 4;
-  for (int c = 0; c < q.ncols; ++c) b += q.col_type[c] == GBA_I64 ? 8 : 4;
+  for (int c = 0; c < q.ncols; ++c) b += gba_type_bytes(q.col_type[c]);
   return b;
 }
 

@@ -35,7 +35,7 @@ struct PreaggParams {
 constexpr int kMaxStages = 4;
 
 __host__ __device__ inline int key_bytes(const QDesc& q) { return q.key64 ? 8 : 4; }
-__host__ __device__ inline int col_bytes(int t) { return t == GBA_I64 ? 8 : 4; }
+__host__ __device__ inline int col_bytes(int t) { return gba_type_bytes(t); }
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
 __host__ __device__ inline size_t stage_bytes(const QDesc& q, int T) {

@@ -27,7 +27,7 @@
 
 namespace {
 
-__host__ __device__ inline int col_bytes_t(int t) { return t == GBA_I64 ? 8 : 4; }
+__host__ __device__ inline int col_bytes_t(int t) { return gba_type_bytes(t); }
 
 // digit of a key for a pass: bits [32 - shift_hi - bits, 32 - shift_hi) of the hash
 template <bool K64>

@@ -218,7 +218,7 @@ __device__ __forceinline__ void stream_chunk(const BatchQ& bq, const SmemTable<K
         for (int c = 0; c < GBA_MAX_COLS; ++c) {
           if (c < Sig::ncols(q)) {
             unsigned long long cv[V];
-            if (Sig::coltype(q, c) == GBA_I64) ld_vec8<V>(static_cast<const unsigned long long*>(q.cols[c]) + r, cv);
+            if (gba_type_bytes(Sig::coltype(q, c)) == 8) ld_vec8<V>(static_cast<const unsigned long long*>(q.cols[c]) + r, cv);
             else ld_vec4<V>(static_cast<const unsigned*>(q.cols[c]) + r, cv);
 #pragma unroll
             for (int e = 0; e < V; ++e) raw[u * V + e][c] = cv[e];
@@ -240,7 +240,7 @@ __device__ __forceinline__ void stream_chunk(const BatchQ& bq, const SmemTable<K
 #pragma unroll
           for (int c = 0; c < GBA_MAX_COLS; ++c)
             if (c < Sig::ncols(q))
-              raw[i][c] = Sig::coltype(q, c) == GBA_I64 ? __ldcs(static_cast<const unsigned long long*>(q.cols[c]) + r)
+              raw[i][c] = gba_type_bytes(Sig::coltype(q, c)) == 8 ? __ldcs(static_cast<const unsigned long long*>(q.cols[c]) + r)
                                                         : __ldcs(static_cast<const unsigned*>(q.cols[c]) + r);
         }
       }

@@ -43,11 +43,13 @@ typedef enum gba_status {
 } gba_status;
 
 /* Column and key types.  GBA_U32 is the reference's key_type/val_type
- * (u_int32_t, tiled_groupby_agg_partition/include/util.cuh:6-7). */
-typedef enum gba_type { GBA_I32 = 0, GBA_I64 = 1, GBA_F32 = 2, GBA_U32 = 3 } gba_type;
+ * (u_int32_t, tiled_groupby_agg_partition/include/util.cuh:6-7).  Keys are
+ * I32, U32 or I64; F32 and F64 are value columns only. */
+typedef enum gba_type { GBA_I32 = 0, GBA_I64 = 1, GBA_F32 = 2, GBA_U32 = 3, GBA_F64 = 4 } gba_type;
 
 /* Aggregates.  SUM/COUNT/MIN/MAX of integer columns accumulate in int64 and are
- * exact (SUM wraps mod 2^64); SUM of an F32 column accumulates in fp64.  AVG
+ * exact (SUM wraps mod 2^64); SUM of an F32 or F64 column accumulates in fp64
+ * (F32 and F64 columns take SUM and AVG only).  AVG
  * (gba_groupby and gba_groupby_batch; the other entry points return
  * GBA_ERR_UNSUPPORTED) is the double SUM / COUNT of the group: the int64 sum
  * (fp64 for an F32 column) rounded to double, divided by the row count.  The reference computes SUM

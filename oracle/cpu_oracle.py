@@ -16,7 +16,7 @@ HERE = Path(__file__).resolve().parent
 LIB = HERE / "lib" / "liboracle.so"
 REF_DRIVER = HERE / "_ref" / "ref_driver"
 
-I32, I64, F32, U32 = 0, 1, 2, 3
+I32, I64, F32, U32, F64 = 0, 1, 2, 3, 4
 SUM, COUNT, MIN, MAX, SUMABS = 0, 1, 2, 3, 4
 _OPS = {"sum": SUM, "count": COUNT, "min": MIN, "max": MAX, "sumabs": SUMABS}
 
@@ -54,7 +54,7 @@ def lib() -> C.CDLL:
 
 def _type(a: np.ndarray) -> int:
     return {np.dtype(np.int32): I32, np.dtype(np.uint32): U32, np.dtype(np.int64): I64,
-            np.dtype(np.float32): F32}[a.dtype]
+            np.dtype(np.float32): F32, np.dtype(np.float64): F64}[a.dtype]
 
 
 def murmur3_32(data: bytes, seed: int = 0) -> int:
@@ -65,7 +65,7 @@ def murmur3_32(data: bytes, seed: int = 0) -> int:
 def groupby(keys: np.ndarray, cols=(), aggs=(("count", None),), nthreads: int = 1, sort: bool = True):
     """Exact GROUP BY; returns (keys, [agg arrays]) sorted by key.
 
-    Integer aggregates are int64; SUM (and SUMABS) of fp32 columns are float64.
+    Integer aggregates are int64; SUM (and SUMABS) of fp32 and fp64 columns are float64.
     """
     keys = np.ascontiguousarray(keys)
     cols = [np.ascontiguousarray(c) for c in cols]
@@ -76,7 +76,7 @@ def groupby(keys: np.ndarray, cols=(), aggs=(("count", None),), nthreads: int = 
     out_keys = np.empty(max(n, 1), dtype=keys.dtype)
     outs = []
     for o, c in zip(ops, acols):
-        fp = o in (SUM, SUMABS) and o != COUNT and len(cols) > c and ctypes_[c] == F32
+        fp = o in (SUM, SUMABS) and o != COUNT and len(cols) > c and ctypes_[c] in (F32, F64)
         outs.append(np.empty(max(n, 1), dtype=np.float64 if fp else np.int64))
     na = len(ops)
     ct = (C.c_int * max(len(cols), 1))(*ctypes_)

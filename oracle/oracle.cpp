@@ -16,7 +16,7 @@
 //                        result of phase 1 + phase 2 together: kernel.cu:9-186 (per tile)
 //                        and kernel.cu:294-406 (per partition) both compute an exact
 //                        per-key SUM; the reference accumulates u32 (wrapping), this
-//                        oracle accumulates int64 (and fp64 for fp32 columns) so nothing
+//                        oracle accumulates int64 (and fp64 for fp32 and fp64 columns) so nothing
 //                        overflows, which is the contract of the new implementation.
 //  * orc_tile_partition_counts
 //                        the reference's phase-1 partition layout: each tile of
@@ -43,7 +43,7 @@
 
 extern "C" {
 
-enum { ORC_I32 = 0, ORC_I64 = 1, ORC_F32 = 2, ORC_U32 = 3 };
+enum { ORC_I32 = 0, ORC_I64 = 1, ORC_F32 = 2, ORC_U32 = 3, ORC_F64 = 4 };
 enum { ORC_SUM = 0, ORC_COUNT = 1, ORC_MIN = 2, ORC_MAX = 3, ORC_SUMABS = 4 };
 
 // ---------------------------------------------------------------------------
@@ -124,7 +124,8 @@ struct AggSpec {
 inline bool agg_is_fp(const AggSpec& s, int a) {
   const int op = s.ops[a];
   if (op == ORC_COUNT) return false;
-  return s.col_types[s.cols[a]] == ORC_F32 && (op == ORC_SUM || op == ORC_SUMABS);
+  const int t = s.col_types[s.cols[a]];
+  return (t == ORC_F32 || t == ORC_F64) && (op == ORC_SUM || op == ORC_SUMABS);
 }
 
 union Acc {
@@ -153,8 +154,10 @@ inline void agg_update(const AggSpec& s, int a, Acc& acc, int64_t row) {
   const int c = s.cols[a];
   const void* col = s.cols_data[c];
   switch (s.col_types[c]) {
-    case ORC_F32: {
-      const double x = static_cast<const float*>(col)[row];
+    case ORC_F32:
+    case ORC_F64: {
+      const double x = s.col_types[c] == ORC_F64 ? static_cast<const double*>(col)[row]
+                                                 : double(static_cast<const float*>(col)[row]);
       if (op == ORC_SUM) acc.f += x;
       else if (op == ORC_SUMABS) acc.f += std::fabs(x);
       else if (op == ORC_MIN) { /* fp MIN/MAX are not part of the contract */ }
@@ -237,7 +240,7 @@ extern "C" {
 // columns of col_types.  Aggregate a is ops[a] over column agg_cols[a]
 // (ignored for COUNT).  Output (capacity n rows): out_keys in key_type,
 // out_accs[a] an array of int64 (integer aggregates, COUNT) or double (SUM /
-// SUMABS over fp32).  Rows are written sorted by key when sort_output != 0.
+// SUMABS over fp32 or fp64).  Rows are written sorted by key when sort_output != 0.
 // nthreads <= 1 runs single-threaded; more threads run a partitioned
 // aggregation (radix partition on hash bits, then one table per partition).
 // Returns the number of groups.

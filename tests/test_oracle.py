@@ -89,6 +89,21 @@ def test_groupby_edge_cases():
     assert list(k) == [7, 0xFFFFFFFF] and list(outs[0]) == [3, 3]
 
 
+def test_f64_sum_matches_fsum():
+    """fp64 value columns: each group's SUM within a few roundings of the
+    correctly rounded sum (math.fsum), SUMABS likewise."""
+    import math
+    rng = np.random.default_rng(3)
+    n = 50_000
+    keys = rng.integers(0, 300, size=n).astype(np.int64)
+    v = rng.standard_normal(n) * 10.0 ** rng.integers(-20, 20, size=n)
+    k, (s, a) = O.groupby(keys, [v], [("sum", 0), ("sumabs", 0)], nthreads=4)
+    for i, key in enumerate(k):
+        x = v[keys == key]
+        assert abs(s[i] - math.fsum(x)) <= 1e-12 * math.fsum(np.abs(x))
+        assert abs(a[i] - math.fsum(np.abs(x))) <= 1e-12 * math.fsum(np.abs(x))
+
+
 def test_sum_wraps_mod_2_64():
     keys = np.zeros(3, dtype=np.int64)
     v = np.array([np.iinfo(np.int64).max, 1, 1], dtype=np.int64)
