@@ -48,11 +48,13 @@ class Query(C.Structure):
         ("cols", Column * GBA_MAX_COLS),
         ("n_aggs", C.c_int32),
         ("aggs", Agg * GBA_MAX_AGGS),
+        ("key2", Column),
     ]
 
 
 class Output(C.Structure):
-    _fields_ = [("keys", C.c_void_p), ("aggs", C.c_void_p * GBA_MAX_AGGS), ("capacity", C.c_int64)]
+    _fields_ = [("keys", C.c_void_p), ("aggs", C.c_void_p * GBA_MAX_AGGS), ("capacity", C.c_int64),
+                ("keys2", C.c_void_p)]
 
 
 class Knobs(C.Structure):

@@ -56,12 +56,44 @@ def make_knobs(**kw) -> A.Knobs:
     return k
 
 
+def _split_keys(keys, unsigned_keys):
+    """(first key, second key or None, unsigned flags of both): keys is a tensor
+    or, for a composite key, a pair of 32-bit tensors."""
+    if isinstance(keys, (tuple, list)):
+        k1, k2 = keys
+        u = tuple(unsigned_keys) if isinstance(unsigned_keys, (tuple, list)) else (bool(unsigned_keys),) * 2
+        return k1, k2, u
+    return keys, None, (bool(unsigned_keys), False)
+
+
+def _empty_like_keys(keys, cap):
+    import torch
+    if isinstance(keys, (tuple, list)):
+        return tuple(torch.empty(cap, dtype=k.dtype, device=k.device) for k in keys)
+    return torch.empty(cap, dtype=keys.dtype, device=keys.device)
+
+
+def _set_out_keys(o: A.Output, okeys) -> int:
+    """Points o at the output key column(s); returns the capacity."""
+    if isinstance(okeys, (tuple, list)):
+        o.keys, o.keys2 = okeys[0].data_ptr(), okeys[1].data_ptr()
+        return min(okeys[0].numel(), okeys[1].numel())
+    o.keys = okeys.data_ptr()
+    return okeys.numel()
+
+
+def _head(okeys, g):
+    return tuple(k[:g] for k in okeys) if isinstance(okeys, (tuple, list)) else okeys[:g]
+
+
 def build_query(n: int, key_ptr: int, key_type: int, cols: Sequence[tuple[int, int]],
-                aggs: Sequence[tuple[int, int]]) -> A.Query:
+                aggs: Sequence[tuple[int, int]], key2: tuple[int, int] | None = None) -> A.Query:
     q = A.Query()
     q.n_rows = n
     q.key.type = key_type
     q.key.data = key_ptr
+    if key2 is not None:
+        q.key2.data, q.key2.type = key2
     q.n_cols = len(cols)
     for i, (ptr, t) in enumerate(cols):
         q.cols[i].type = t
@@ -127,37 +159,39 @@ class Context:
                 capacity: int | None = None, unsigned_keys: bool = False, stream=None, out=None,
                 unsigned_cols: Sequence[bool] = ()) -> Result:
         """torch has no general uint32 dtype: pass uint32 data as int32 tensors
-        and mark them with unsigned_keys / unsigned_cols[i]."""
+        and mark them with unsigned_keys / unsigned_cols[i].  A composite key is
+        a pair of 32-bit tensors (unsigned_keys may then be a pair of flags);
+        the result's keys are then a pair too."""
         import torch
-        if not keys.is_cuda:
+        k1, k2, uk = _split_keys(keys, unsigned_keys)
+        if not k1.is_cuda:
             raise ValueError("groupby() takes device tensors; use groupby_host() for host arrays")
-        n = keys.numel()
+        n = k1.numel()
         aggs_p = parse_aggs(aggs)
         uc = list(unsigned_cols) + [False] * (len(cols) - len(unsigned_cols))
         col_specs = [(c.data_ptr(), _torch_type(c, u)) for c, u in zip(cols, uc)]
-        ktype = _torch_type(keys, unsigned_keys)
-        q = build_query(n, keys.data_ptr(), ktype, col_specs, aggs_p)
+        q = build_query(n, k1.data_ptr(), _torch_type(k1, uk[0]), col_specs, aggs_p,
+                        None if k2 is None else (k2.data_ptr(), _torch_type(k2, uk[1])))
         if out is None:
             cap = capacity if capacity is not None else max(n, 1) + 1
-            okeys = torch.empty(cap, dtype=keys.dtype, device=keys.device)
+            okeys = _empty_like_keys(keys, cap)
             oaggs = [torch.empty(cap, dtype=torch.float64 if agg_is_fp(op, col_specs[col][1] if op != A.COUNT else 0)
-                                 else torch.int64, device=keys.device) for op, col in aggs_p]
+                                 else torch.int64, device=k1.device) for op, col in aggs_p]
         else:
             okeys, oaggs = out
-            cap = okeys.numel()
         o = A.Output()
-        o.keys = okeys.data_ptr()
+        cap = _set_out_keys(o, okeys)
         for i, t in enumerate(oaggs):
             o.aggs[i] = t.data_ptr()
         o.capacity = cap
         kn = knobs if isinstance(knobs, A.Knobs) else make_knobs(**(knobs or {}))
         ng = C.c_int64(0)
-        s = stream if stream is not None else torch.cuda.current_stream(keys.device)
+        s = stream if stream is not None else torch.cuda.current_stream(k1.device)
         st = self._lib.gba_groupby(self._h, C.byref(q), C.byref(o), C.byref(kn), C.c_void_p(s.cuda_stream),
                                    C.byref(ng))
         A.check(st, self._h)
         g = ng.value
-        return Result(okeys[:g], [t[:g] for t in oaggs], g, self.stats())
+        return Result(_head(okeys, g), [t[:g] for t in oaggs], g, self.stats())
 
     def batch_outputs(self, queries: Sequence, capacity: Sequence[int] | None = None) -> list:
         """Device output buffers (keys, aggs) for each query of a batch; reusable
@@ -170,10 +204,11 @@ class Context:
             uc = list(q[4]) if len(q) > 4 else []
             uc += [False] * (len(cols) - len(uc))
             ctypes_ = [_torch_type(c, u) for c, u in zip(cols, uc)]
-            cap = capacity[i] if capacity is not None else max(keys.numel(), 1) + 1
-            okeys = torch.empty(cap, dtype=keys.dtype, device=keys.device)
+            k1 = _split_keys(keys, False)[0]
+            cap = capacity[i] if capacity is not None else max(k1.numel(), 1) + 1
+            okeys = _empty_like_keys(keys, cap)
             oaggs = [torch.empty(cap, dtype=torch.float64 if agg_is_fp(op, ctypes_[col] if op != A.COUNT else 0)
-                                 else torch.int64, device=keys.device) for op, col in aggs_p]
+                                 else torch.int64, device=k1.device) for op, col in aggs_p]
             outs.append((okeys, oaggs))
         return outs
 
@@ -183,18 +218,18 @@ class Context:
         oarr = (A.Output * max(nq, 1))()
         for i, q in enumerate(queries):
             keys, cols, aggs = q[0], q[1], q[2]
-            uk = bool(q[3]) if len(q) > 3 else False
+            k1, k2, uk = _split_keys(keys, q[3] if len(q) > 3 else False)
             uc = list(q[4]) if len(q) > 4 else []
             uc += [False] * (len(cols) - len(uc))
-            if not keys.is_cuda:
+            if not k1.is_cuda:
                 raise ValueError("device tensors expected")
             col_specs = [(c.data_ptr(), _torch_type(c, u)) for c, u in zip(cols, uc)]
-            qarr[i] = build_query(keys.numel(), keys.data_ptr(), _torch_type(keys, uk), col_specs, parse_aggs(aggs))
+            qarr[i] = build_query(k1.numel(), k1.data_ptr(), _torch_type(k1, uk[0]), col_specs, parse_aggs(aggs),
+                                  None if k2 is None else (k2.data_ptr(), _torch_type(k2, uk[1])))
             okeys, oaggs = outs[i]
-            oarr[i].keys = okeys.data_ptr()
             for a, t in enumerate(oaggs):
                 oarr[i].aggs[a] = t.data_ptr()
-            oarr[i].capacity = okeys.numel()
+            oarr[i].capacity = _set_out_keys(oarr[i], okeys)
         return qarr, oarr
 
     def prepare_batch(self, queries: Sequence, outs=None) -> "PreparedBatch":
@@ -212,7 +247,7 @@ class Context:
         pb.outs[i][0][:n], [a[:n] for a in pb.outs[i][1]]."""
         import torch
         kn = knobs if isinstance(knobs, A.Knobs) else make_knobs(**(knobs or {}))
-        s = stream if stream is not None else torch.cuda.current_stream(pb.queries[0][0].device)
+        s = stream if stream is not None else torch.cuda.current_stream(_split_keys(pb.queries[0][0], False)[0].device)
         A.check(self._lib.gba_groupby_batch(self._h, len(pb.queries), pb.qarr, pb.oarr, C.byref(kn),
                                             C.c_void_p(s.cuda_stream), pb.ng), self._h)
         return np.ctypeslib.as_array(pb.ng)[:len(pb.queries)].copy()
@@ -227,7 +262,7 @@ class Context:
         kn = knobs if isinstance(knobs, A.Knobs) else make_knobs(**(knobs or {}))
         best = A.Knobs()
         ms = C.c_double(0)
-        s = stream if stream is not None else torch.cuda.current_stream(queries[0][0].device)
+        s = stream if stream is not None else torch.cuda.current_stream(_split_keys(queries[0][0], False)[0].device)
         A.check(self._lib.gba_autotune(self._h, len(queries), qarr, oarr, C.byref(kn), C.c_void_p(s.cuda_stream),
                                        reps, C.byref(best), C.byref(ms)), self._h)
         return best, ms.value
@@ -236,7 +271,8 @@ class Context:
         """Many independent queries in one call (gba_groupby_batch).
 
         queries: sequence of (keys, cols, aggs[, unsigned_keys[, unsigned_cols]])
-        with device tensors; outs: batch_outputs() buffers (allocated when None).
+        with device tensors (keys: a tensor, or a pair of 32-bit tensors for a
+        composite key); outs: batch_outputs() buffers (allocated when None).
         Returns one Result per query (views into the output buffers)."""
         import torch
         nq = len(queries)
@@ -245,7 +281,7 @@ class Context:
         qarr, oarr = self._batch_arrays(queries, outs)
         kn = knobs if isinstance(knobs, A.Knobs) else make_knobs(**(knobs or {}))
         ng = (C.c_int64 * max(nq, 1))()
-        dev = queries[0][0].device if nq else torch.device("cuda", 0)
+        dev = _split_keys(queries[0][0], False)[0].device if nq else torch.device("cuda", 0)
         s = stream if stream is not None else torch.cuda.current_stream(dev)
         A.check(self._lib.gba_groupby_batch(self._h, nq, qarr, oarr, C.byref(kn), C.c_void_p(s.cuda_stream), ng),
                 self._h)
@@ -254,7 +290,7 @@ class Context:
         for i in range(nq):
             g = ng[i]
             okeys, oaggs = outs[i]
-            res.append(Result(okeys[:g], [t[:g] for t in oaggs], g, st))
+            res.append(Result(_head(okeys, g), [t[:g] for t in oaggs], g, st))
         return res
 
     # ---- learned cardinality estimator ---------------------------------------
@@ -438,15 +474,17 @@ class Server:
                                  f"({self._lib.gba_server_last_error(self._h).decode()})")
 
     def submit(self, keys, cols, aggs, out, unsigned_keys: bool = False) -> int:
-        """out = (keys_out, [agg_out, ...]) device tensors; returns the ticket."""
+        """out = (keys_out, [agg_out, ...]) device tensors (keys and keys_out
+        pairs for a composite key); returns the ticket."""
         col_specs = [(c.data_ptr(), _torch_type(c)) for c in cols]
-        q = build_query(keys.numel(), keys.data_ptr(), _torch_type(keys, unsigned_keys), col_specs, parse_aggs(aggs))
+        k1, k2, uk = _split_keys(keys, unsigned_keys)
+        q = build_query(k1.numel(), k1.data_ptr(), _torch_type(k1, uk[0]), col_specs, parse_aggs(aggs),
+                        None if k2 is None else (k2.data_ptr(), _torch_type(k2, uk[1])))
         okeys, oaggs = out
         o = A.Output()
-        o.keys = okeys.data_ptr()
         for i, t in enumerate(oaggs):
             o.aggs[i] = t.data_ptr()
-        o.capacity = okeys.numel()
+        o.capacity = _set_out_keys(o, okeys)
         t = C.c_int64(0)
         self._check(self._lib.gba_server_submit(self._h, C.byref(q), C.byref(o), C.byref(t)))
         return t.value

@@ -13,6 +13,7 @@
 
 #include "gba_context.h"
 #include "gba_plan.h"
+#include "composite.h"
 #include "sort_kernels.h"
 
 size_t gba_round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
@@ -94,6 +95,7 @@ extern "C" gba_status gba_destroy(gba_context* ctx) {
   if (ctx->h_batch) cudaFreeHost(ctx->h_batch);
   if (ctx->rp_buf) cudaFree(ctx->rp_buf);
   if (ctx->avg_buf) cudaFree(ctx->avg_buf);
+  if (ctx->ck_buf) cudaFree(ctx->ck_buf);
   delete ctx;
   return GBA_OK;
 }
@@ -225,6 +227,10 @@ gba_status gba_build_qdesc(gba_context* ctx, const gba_query* q, QDesc* d) {
   if (q->n_rows > 0 && !q->key.data) {
     ctx->err = "null key column";
     return GBA_ERR_INVALID_ARG;
+  }
+  if (q->key2.data) {
+    ctx->err = "composite keys are supported by gba_groupby and gba_groupby_batch only";
+    return GBA_ERR_UNSUPPORTED;
   }
   d->keys = q->key.data;
   d->n = q->n_rows;
@@ -506,13 +512,31 @@ static gba_status groupby_device(gba_context* ctx, const gba_query* q, const gba
 static gba_status groupby_avg(gba_context* ctx, const gba_query* q, const gba_output* out,
                               const gba_knobs* knobs, void* stream, int64_t* n_groups);
 
-// Key order (knobs->sort_output) is a device sort of the finished groups.
+// Composite keys are packed into one 64-bit key around the call; key order
+// (knobs->sort_output) is a device sort of the finished groups.
 extern "C" gba_status gba_groupby(gba_context* ctx, const gba_query* q, const gba_output* out,
                                   const gba_knobs* knobs, void* stream, int64_t* n_groups) {
-  gba_status st = groupby_avg(ctx, q, out, knobs, stream, n_groups);
-  if (st != GBA_OK || !knobs || !knobs->sort_output) return st;
-  const SortJob j = gba_sort_job(q, out, std::min<int64_t>(*n_groups, out->capacity));
-  return gba_sort_groups(ctx, &j, 1, static_cast<cudaStream_t>(stream));
+  if (!ctx || !q || !n_groups) return GBA_ERR_INVALID_ARG;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  gba_query qq = *q;
+  gba_output oo = out ? *out : gba_output{};
+  std::vector<CompositeJob> cj;
+  if (q->key2.data) {
+    if (!out) return GBA_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    gba_status st = gba_composite_prepare(ctx, 1, q, out, &qq, &oo, &cj, s);
+    if (st != GBA_OK) return st;
+  }
+  gba_status st = groupby_avg(ctx, &qq, out ? &oo : nullptr, knobs, stream, n_groups);
+  if (st != GBA_OK) return st;
+  if (knobs && knobs->sort_output) {
+    SortJob j = gba_sort_job(&qq, &oo, std::min<int64_t>(*n_groups, oo.capacity));
+    if (!cj.empty()) j.key_signed = 0;  // the packed pair orders as an unsigned word
+    st = gba_sort_groups(ctx, &j, 1, s);
+    if (st != GBA_OK) return st;
+  }
+  if (!cj.empty()) return gba_composite_finish(ctx, cj, out, n_groups, s);
+  return GBA_OK;
 }
 
 // AVG: the query runs with each AVG as a SUM into the caller's column and one

@@ -31,6 +31,7 @@
 #include "est_kernels.h"
 #include "gba_context.h"
 #include "gba_plan.h"
+#include "composite.h"
 #include "sort_kernels.h"
 
 namespace {
@@ -130,15 +131,40 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
 static gba_status batch_avg(gba_context* ctx, int32_t nq, const gba_query* qs, const gba_output* outs,
                             const gba_knobs* knobs, void* stream, int64_t* n_groups);
 
-// Key order (knobs->sort_output): every query's groups sorted on the device
-// after the batch, one query after another.
+// Composite keys are packed into 64-bit keys around the batch; key order
+// (knobs->sort_output) sorts every query's groups on the device after it, one
+// query after another.
 extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_query* qs, const gba_output* outs,
                                         const gba_knobs* knobs, void* stream, int64_t* n_groups) {
-  gba_status st = batch_avg(ctx, nq, qs, outs, knobs, stream, n_groups);
-  if (st != GBA_OK || !knobs || !knobs->sort_output) return st;
-  std::vector<SortJob> jobs(nq);
-  for (int i = 0; i < nq; ++i) jobs[i] = gba_sort_job(&qs[i], &outs[i], std::min<int64_t>(n_groups[i], outs[i].capacity));
-  return gba_sort_groups(ctx, jobs.data(), nq, static_cast<cudaStream_t>(stream));
+  if (!ctx || nq < 0 || (nq > 0 && (!qs || !outs || !n_groups))) return GBA_ERR_INVALID_ARG;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  bool composite = false;
+  for (int i = 0; i < nq && !composite; ++i) composite = qs[i].key2.data != nullptr;
+  std::vector<gba_query> q2;
+  std::vector<gba_output> o2;
+  std::vector<CompositeJob> cj;
+  if (composite) {
+    GBA_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    q2.assign(qs, qs + nq);
+    o2.assign(outs, outs + nq);
+    gba_status st = gba_composite_prepare(ctx, nq, qs, outs, q2.data(), o2.data(), &cj, s);
+    if (st != GBA_OK) return st;
+  }
+  const gba_query* qa = composite ? q2.data() : qs;
+  const gba_output* oa = composite ? o2.data() : outs;
+  gba_status st = batch_avg(ctx, nq, qa, oa, knobs, stream, n_groups);
+  if (st != GBA_OK) return st;
+  if (knobs && knobs->sort_output) {
+    std::vector<SortJob> jobs(nq);
+    for (int i = 0; i < nq; ++i) {
+      jobs[i] = gba_sort_job(&qa[i], &oa[i], std::min<int64_t>(n_groups[i], oa[i].capacity));
+      if (qs[i].key2.data) jobs[i].key_signed = 0;  // the packed pair orders as an unsigned word
+    }
+    st = gba_sort_groups(ctx, jobs.data(), nq, s);
+    if (st != GBA_OK) return st;
+  }
+  if (!cj.empty()) return gba_composite_finish(ctx, cj, outs, n_groups, s);
+  return GBA_OK;
 }
 
 // AVG, as in gba_groupby: every AVG runs as a SUM into the caller's column,

@@ -48,6 +48,9 @@ struct gba_context {
   // AVG without a COUNT in the query: the added COUNT's output column
   void* avg_buf = nullptr;
   size_t avg_bytes = 0;
+  // composite keys: packed input and output keys of a call's queries
+  void* ck_buf = nullptr;
+  size_t ck_bytes = 0;
   std::string err;
   gba_stats stats{};
 };

@@ -73,6 +73,12 @@ typedef struct gba_query {
   gba_column cols[GBA_MAX_COLS];
   int32_t n_aggs;
   gba_agg aggs[GBA_MAX_AGGS];
+  /* Composite key (gba_groupby and gba_groupby_batch; the other entry points
+   * return GBA_ERR_UNSUPPORTED): when key2.data is set the query groups by the
+   * pair (key, key2), both GBA_I32 or GBA_U32, and gba_output.keys2 receives
+   * the second key of every group.  No reference counterpart: the reference
+   * groups by one u32 key (tiled_groupby_agg_partition/include/util.cuh:6). */
+  gba_column key2;
 } gba_query;
 
 /* Output columns: one row per distinct key, in no particular order.  aggs[a]
@@ -82,6 +88,7 @@ typedef struct gba_output {
   void* keys;
   void* aggs[GBA_MAX_AGGS];
   int64_t capacity;
+  void* keys2; /* composite keys only: capacity second keys */
 } gba_output;
 
 typedef enum gba_sizing {
