@@ -23,7 +23,7 @@ OK, ERR_INVALID_ARG, ERR_CUDA, ERR_OOM, ERR_OUTPUT_CAPACITY, ERR_TABLE_OVERFLOW,
 # gba_type
 I32, I64, F32, U32, F64 = 0, 1, 2, 3, 4
 # gba_op
-SUM, COUNT, MIN, MAX, AVG = 0, 1, 2, 3, 4
+SUM, COUNT, MIN, MAX, AVG, COUNT_VALID = 0, 1, 2, 3, 4, 5
 # gba_sizing
 SIZING_PLAIN, SIZING_LEARNED, SIZING_FIXED = 0, 1, 2
 # gba_strategy
@@ -33,7 +33,7 @@ GEN_UNIFORM_I32, GEN_UNIFORM_I64, GEN_NORMAL_F32, GEN_ONES_I32 = 0, 1, 2, 3
 
 
 class Column(C.Structure):
-    _fields_ = [("type", C.c_int32), ("data", C.c_void_p)]
+    _fields_ = [("type", C.c_int32), ("data", C.c_void_p), ("valid", C.c_void_p)]
 
 
 class Agg(C.Structure):
@@ -54,7 +54,7 @@ class Query(C.Structure):
 
 class Output(C.Structure):
     _fields_ = [("keys", C.c_void_p), ("aggs", C.c_void_p * GBA_MAX_AGGS), ("capacity", C.c_int64),
-                ("keys2", C.c_void_p)]
+                ("keys2", C.c_void_p), ("agg_valid", C.c_void_p * GBA_MAX_AGGS)]
 
 
 class Knobs(C.Structure):

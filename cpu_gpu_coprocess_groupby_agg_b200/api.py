@@ -14,7 +14,7 @@ import numpy as np
 
 from . import _abi as A
 
-_OPS = {"sum": A.SUM, "count": A.COUNT, "min": A.MIN, "max": A.MAX, "avg": A.AVG}
+_OPS = {"sum": A.SUM, "count": A.COUNT, "min": A.MIN, "max": A.MAX, "avg": A.AVG, "count_valid": A.COUNT_VALID}
 
 
 def _np_type(a: np.ndarray) -> int:
@@ -95,9 +95,10 @@ def build_query(n: int, key_ptr: int, key_type: int, cols: Sequence[tuple[int, i
     if key2 is not None:
         q.key2.data, q.key2.type = key2
     q.n_cols = len(cols)
-    for i, (ptr, t) in enumerate(cols):
-        q.cols[i].type = t
-        q.cols[i].data = ptr
+    for i, spec in enumerate(cols):  # (data pointer, type[, validity bitmap pointer])
+        q.cols[i].data, q.cols[i].type = spec[0], spec[1]
+        if len(spec) > 2 and spec[2]:
+            q.cols[i].valid = spec[2]
     q.n_aggs = len(aggs)
     for i, (op, col) in enumerate(aggs):
         q.aggs[i].op = op
@@ -120,6 +121,7 @@ class Result:
     aggs: list
     n_groups: int
     stats: dict = field(default_factory=dict)
+    valid: list | None = None  # per aggregate, uint8 per group (when requested)
 
 
 class Context:
@@ -157,11 +159,13 @@ class Context:
     # ---- device-resident ---------------------------------------------------
     def groupby(self, keys, cols: Sequence = (), aggs: Sequence = (("count", None),), knobs=None,
                 capacity: int | None = None, unsigned_keys: bool = False, stream=None, out=None,
-                unsigned_cols: Sequence[bool] = ()) -> Result:
+                unsigned_cols: Sequence[bool] = (), col_valid: Sequence = (), agg_valid: bool = False) -> Result:
         """torch has no general uint32 dtype: pass uint32 data as int32 tensors
         and mark them with unsigned_keys / unsigned_cols[i].  A composite key is
         a pair of 32-bit tensors (unsigned_keys may then be a pair of flags);
-        the result's keys are then a pair too."""
+        the result's keys are then a pair too.  col_valid[i]: a uint8 device
+        tensor holding column i's validity bitmap (Arrow layout), or None;
+        agg_valid: also return one validity byte per group and aggregate."""
         import torch
         k1, k2, uk = _split_keys(keys, unsigned_keys)
         if not k1.is_cuda:
@@ -169,7 +173,9 @@ class Context:
         n = k1.numel()
         aggs_p = parse_aggs(aggs)
         uc = list(unsigned_cols) + [False] * (len(cols) - len(unsigned_cols))
-        col_specs = [(c.data_ptr(), _torch_type(c, u)) for c, u in zip(cols, uc)]
+        cv = list(col_valid) + [None] * (len(cols) - len(col_valid))
+        col_specs = [(c.data_ptr(), _torch_type(c, u), 0 if v is None else v.data_ptr())
+                     for c, u, v in zip(cols, uc, cv)]
         q = build_query(n, k1.data_ptr(), _torch_type(k1, uk[0]), col_specs, aggs_p,
                         None if k2 is None else (k2.data_ptr(), _torch_type(k2, uk[1])))
         if out is None:
@@ -184,6 +190,11 @@ class Context:
         for i, t in enumerate(oaggs):
             o.aggs[i] = t.data_ptr()
         o.capacity = cap
+        ovalid = None
+        if agg_valid:
+            ovalid = [torch.empty(cap, dtype=torch.uint8, device=k1.device) for _ in aggs_p]
+            for i, t in enumerate(ovalid):
+                o.agg_valid[i] = t.data_ptr()
         kn = knobs if isinstance(knobs, A.Knobs) else make_knobs(**(knobs or {}))
         ng = C.c_int64(0)
         s = stream if stream is not None else torch.cuda.current_stream(k1.device)
@@ -191,7 +202,8 @@ class Context:
                                    C.byref(ng))
         A.check(st, self._h)
         g = ng.value
-        return Result(_head(okeys, g), [t[:g] for t in oaggs], g, self.stats())
+        return Result(_head(okeys, g), [t[:g] for t in oaggs], g, self.stats(),
+                      None if ovalid is None else [t[:g] for t in ovalid])
 
     def batch_outputs(self, queries: Sequence, capacity: Sequence[int] | None = None) -> list:
         """Device output buffers (keys, aggs) for each query of a batch; reusable
@@ -223,12 +235,18 @@ class Context:
             uc += [False] * (len(cols) - len(uc))
             if not k1.is_cuda:
                 raise ValueError("device tensors expected")
-            col_specs = [(c.data_ptr(), _torch_type(c, u)) for c, u in zip(cols, uc)]
+            cv = list(q[5]) if len(q) > 5 else []
+            cv += [None] * (len(cols) - len(cv))
+            col_specs = [(c.data_ptr(), _torch_type(c, u), 0 if v is None else v.data_ptr())
+                         for c, u, v in zip(cols, uc, cv)]
             qarr[i] = build_query(k1.numel(), k1.data_ptr(), _torch_type(k1, uk[0]), col_specs, parse_aggs(aggs),
                                   None if k2 is None else (k2.data_ptr(), _torch_type(k2, uk[1])))
-            okeys, oaggs = outs[i]
+            okeys, oaggs = outs[i][0], outs[i][1]
             for a, t in enumerate(oaggs):
                 oarr[i].aggs[a] = t.data_ptr()
+            if len(outs[i]) > 2 and outs[i][2] is not None:  # validity bytes per aggregate
+                for a, t in enumerate(outs[i][2]):
+                    oarr[i].agg_valid[a] = t.data_ptr()
             oarr[i].capacity = _set_out_keys(oarr[i], okeys)
         return qarr, oarr
 
@@ -270,9 +288,11 @@ class Context:
     def groupby_batch(self, queries: Sequence, knobs=None, stream=None, outs=None) -> list:
         """Many independent queries in one call (gba_groupby_batch).
 
-        queries: sequence of (keys, cols, aggs[, unsigned_keys[, unsigned_cols]])
-        with device tensors (keys: a tensor, or a pair of 32-bit tensors for a
-        composite key); outs: batch_outputs() buffers (allocated when None).
+        queries: sequence of (keys, cols, aggs[, unsigned_keys[, unsigned_cols[,
+        col_valid]]]) with device tensors (keys: a tensor, or a pair of 32-bit
+        tensors for a composite key; col_valid: validity bitmaps or None per
+        column); outs: batch_outputs() buffers (allocated when None), each
+        (keys, aggs[, validity bytes per aggregate]).
         Returns one Result per query (views into the output buffers)."""
         import torch
         nq = len(queries)
@@ -289,8 +309,10 @@ class Context:
         res = []
         for i in range(nq):
             g = ng[i]
-            okeys, oaggs = outs[i]
-            res.append(Result(_head(okeys, g), [t[:g] for t in oaggs], g, st))
+            okeys, oaggs = outs[i][0], outs[i][1]
+            ov = outs[i][2] if len(outs[i]) > 2 else None
+            res.append(Result(_head(okeys, g), [t[:g] for t in oaggs], g, st,
+                              None if ov is None else [t[:g] for t in ov]))
         return res
 
     # ---- learned cardinality estimator ---------------------------------------

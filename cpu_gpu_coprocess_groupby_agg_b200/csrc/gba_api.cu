@@ -14,6 +14,7 @@
 #include "gba_context.h"
 #include "gba_plan.h"
 #include "composite.h"
+#include "nulls.h"
 #include "sort_kernels.h"
 
 size_t gba_round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
@@ -96,6 +97,7 @@ extern "C" gba_status gba_destroy(gba_context* ctx) {
   if (ctx->rp_buf) cudaFree(ctx->rp_buf);
   if (ctx->avg_buf) cudaFree(ctx->avg_buf);
   if (ctx->ck_buf) cudaFree(ctx->ck_buf);
+  if (ctx->null_buf) cudaFree(ctx->null_buf);
   delete ctx;
   return GBA_OK;
 }
@@ -230,6 +232,13 @@ gba_status gba_build_qdesc(gba_context* ctx, const gba_query* q, QDesc* d) {
   }
   if (q->key2.data) {
     ctx->err = "composite keys are supported by gba_groupby and gba_groupby_batch only";
+    return GBA_ERR_UNSUPPORTED;
+  }
+  bool nullable = q->key.valid != nullptr;
+  for (int c = 0; c < q->n_cols && c < GBA_MAX_COLS; ++c) nullable = nullable || q->cols[c].valid != nullptr;
+  for (int a = 0; a < q->n_aggs && a < GBA_MAX_AGGS; ++a) nullable = nullable || q->aggs[a].op == GBA_COUNT_VALID;
+  if (nullable) {
+    ctx->err = "nullable columns and COUNT(col) are supported by gba_groupby and gba_groupby_batch only";
     return GBA_ERR_UNSUPPORTED;
   }
   d->keys = q->key.data;
@@ -518,13 +527,23 @@ extern "C" gba_status gba_groupby(gba_context* ctx, const gba_query* q, const gb
                                   const gba_knobs* knobs, void* stream, int64_t* n_groups) {
   if (!ctx || !q || !n_groups) return GBA_ERR_INVALID_ARG;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  gba_query qq = *q;
-  gba_output oo = out ? *out : gba_output{};
+  // nullable columns: rewritten columns and aggregates (qn, on)
+  gba_query qn = *q;
+  gba_output on = out ? *out : gba_output{};
+  std::vector<NullPlan> np;
+  if (out && gba_nulls_needed(*q, *out)) {
+    cudaSetDevice(ctx->device);
+    gba_status st = gba_nulls_prepare(ctx, 1, q, out, &qn, &on, &np, s);
+    if (st != GBA_OK) return st;
+  }
+  // composite keys: packed key columns (qq, oo)
+  gba_query qq = qn;
+  gba_output oo = on;
   std::vector<CompositeJob> cj;
-  if (q->key2.data) {
+  if (qn.key2.data) {
     if (!out) return GBA_ERR_INVALID_ARG;
     cudaSetDevice(ctx->device);
-    gba_status st = gba_composite_prepare(ctx, 1, q, out, &qq, &oo, &cj, s);
+    gba_status st = gba_composite_prepare(ctx, 1, &qn, &on, &qq, &oo, &cj, s);
     if (st != GBA_OK) return st;
   }
   gba_status st = groupby_avg(ctx, &qq, out ? &oo : nullptr, knobs, stream, n_groups);
@@ -535,7 +554,11 @@ extern "C" gba_status gba_groupby(gba_context* ctx, const gba_query* q, const gb
     st = gba_sort_groups(ctx, &j, 1, s);
     if (st != GBA_OK) return st;
   }
-  if (!cj.empty()) return gba_composite_finish(ctx, cj, out, n_groups, s);
+  if (!cj.empty()) {
+    st = gba_composite_finish(ctx, cj, &on, n_groups, s);
+    if (st != GBA_OK) return st;
+  }
+  if (!np.empty()) return gba_nulls_finish(ctx, np, q, out, &on, n_groups, s);
   return GBA_OK;
 }
 

@@ -32,6 +32,7 @@
 #include "gba_context.h"
 #include "gba_plan.h"
 #include "composite.h"
+#include "nulls.h"
 #include "sort_kernels.h"
 
 namespace {
@@ -138,20 +139,36 @@ extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_
                                         const gba_knobs* knobs, void* stream, int64_t* n_groups) {
   if (!ctx || nq < 0 || (nq > 0 && (!qs || !outs || !n_groups))) return GBA_ERR_INVALID_ARG;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // nullable columns: rewritten columns and aggregates (qn, on)
+  bool nulls = false;
+  for (int i = 0; i < nq && !nulls; ++i) nulls = gba_nulls_needed(qs[i], outs[i]);
+  std::vector<gba_query> qn;
+  std::vector<gba_output> on;
+  std::vector<NullPlan> np;
+  if (nulls) {
+    GBA_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    qn.assign(qs, qs + nq);
+    on.assign(outs, outs + nq);
+    gba_status st = gba_nulls_prepare(ctx, nq, qs, outs, qn.data(), on.data(), &np, s);
+    if (st != GBA_OK) return st;
+  }
+  const gba_query* qb = nulls ? qn.data() : qs;
+  const gba_output* ob = nulls ? on.data() : outs;
+  // composite keys: packed key columns
   bool composite = false;
-  for (int i = 0; i < nq && !composite; ++i) composite = qs[i].key2.data != nullptr;
+  for (int i = 0; i < nq && !composite; ++i) composite = qb[i].key2.data != nullptr;
   std::vector<gba_query> q2;
   std::vector<gba_output> o2;
   std::vector<CompositeJob> cj;
   if (composite) {
     GBA_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
-    q2.assign(qs, qs + nq);
-    o2.assign(outs, outs + nq);
-    gba_status st = gba_composite_prepare(ctx, nq, qs, outs, q2.data(), o2.data(), &cj, s);
+    q2.assign(qb, qb + nq);
+    o2.assign(ob, ob + nq);
+    gba_status st = gba_composite_prepare(ctx, nq, qb, ob, q2.data(), o2.data(), &cj, s);
     if (st != GBA_OK) return st;
   }
-  const gba_query* qa = composite ? q2.data() : qs;
-  const gba_output* oa = composite ? o2.data() : outs;
+  const gba_query* qa = composite ? q2.data() : qb;
+  const gba_output* oa = composite ? o2.data() : ob;
   gba_status st = batch_avg(ctx, nq, qa, oa, knobs, stream, n_groups);
   if (st != GBA_OK) return st;
   if (knobs && knobs->sort_output) {
@@ -163,7 +180,11 @@ extern "C" gba_status gba_groupby_batch(gba_context* ctx, int32_t nq, const gba_
     st = gba_sort_groups(ctx, jobs.data(), nq, s);
     if (st != GBA_OK) return st;
   }
-  if (!cj.empty()) return gba_composite_finish(ctx, cj, outs, n_groups, s);
+  if (!cj.empty()) {
+    st = gba_composite_finish(ctx, cj, ob, n_groups, s);
+    if (st != GBA_OK) return st;
+  }
+  if (!np.empty()) return gba_nulls_finish(ctx, np, qs, outs, ob, n_groups, s);
   return GBA_OK;
 }
 

@@ -51,6 +51,9 @@ struct gba_context {
   // composite keys: packed input and output keys of a call's queries
   void* ck_buf = nullptr;
   size_t ck_bytes = 0;
+  // nullable columns: identity-filled copies, presence columns, hidden counts
+  void* null_buf = nullptr;
+  size_t null_bytes = 0;
   std::string err;
   gba_stats stats{};
 };

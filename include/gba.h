@@ -54,11 +54,20 @@ typedef enum gba_type { GBA_I32 = 0, GBA_I64 = 1, GBA_F32 = 2, GBA_U32 = 3, GBA_
  * GBA_ERR_UNSUPPORTED) is the double SUM / COUNT of the group: the int64 sum
  * (fp64 for an F32 column) rounded to double, divided by the row count.  The reference computes SUM
  * only, in u32 (kernel.cu:48,152,334). */
-typedef enum gba_op { GBA_SUM = 0, GBA_COUNT = 1, GBA_MIN = 2, GBA_MAX = 3, GBA_AVG = 4 } gba_op;
+/* GBA_COUNT counts rows (COUNT(*)); GBA_COUNT_VALID counts the rows whose
+ * column value is present (COUNT(col); gba_groupby and gba_groupby_batch). */
+typedef enum gba_op { GBA_SUM = 0, GBA_COUNT = 1, GBA_MIN = 2, GBA_MAX = 3, GBA_AVG = 4, GBA_COUNT_VALID = 5 } gba_op;
 
 typedef struct gba_column {
   int32_t type;     /* gba_type */
   const void* data; /* n_rows elements, device (or host for *_host calls) */
+  /* Nullable value columns (gba_groupby and gba_groupby_batch; elsewhere, and
+   * on keys, GBA_ERR_UNSUPPORTED): a validity bitmap in device memory, bit
+   * (i & 7) of byte i >> 3 set when row i's value is present (the Arrow
+   * layout); null = every value present.  SUM, MIN, MAX and AVG skip absent
+   * values; a group with none gets SUM 0, MIN the type's largest value, MAX
+   * its smallest, AVG NaN, and validity 0 in gba_output.agg_valid. */
+  const uint8_t* valid;
 } gba_column;
 
 typedef struct gba_agg {
@@ -89,6 +98,10 @@ typedef struct gba_output {
   void* aggs[GBA_MAX_AGGS];
   int64_t capacity;
   void* keys2; /* composite keys only: capacity second keys */
+  /* optional (gba_groupby and gba_groupby_batch): one byte per group for
+   * aggregate a, 1 when it saw a present value (always 1 for COUNT and for
+   * columns without a validity bitmap) */
+  uint8_t* agg_valid[GBA_MAX_AGGS];
 } gba_output;
 
 typedef enum gba_sizing {
