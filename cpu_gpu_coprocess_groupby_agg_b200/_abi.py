@@ -156,6 +156,7 @@ SIGNATURES = {
                                     C.POINTER(C.c_int64)]),
     "gba_groupby_noalloc": (C.c_int, [_P, C.POINTER(Query), C.POINTER(Output), _P, C.POINTER(C.c_int64)]),
     "gba_groupby_partition_u32": (C.c_int, [_P, _P, _P, C.c_int64, C.c_int32, _P, _P, _P, _P]),
+    "gba_avg_divide": (C.c_int, [_P, C.c_int32, _P, C.POINTER(C.c_int32), _P, C.c_int64, _P]),
     "gba_autotune": (C.c_int, [_P, C.c_int32, C.POINTER(Query), C.POINTER(Output), C.POINTER(Knobs), _P, C.c_int32,
                                C.POINTER(Knobs), C.POINTER(C.c_double)]),
     "gba_server_default_config": (None, [C.POINTER(ServerConfig)]),

@@ -242,6 +242,15 @@ gba_status gba_groupby_partition_u32(gba_context* ctx, const uint32_t* keys, con
                                      int32_t P, uint32_t* out_keys, uint32_t* out_vals, uint64_t* part_offsets,
                                      void* stream);
 
+/* Sharded GROUP BY across ranks (one process per GPU; the exchange is
+ * torch.distributed's all-to-all in the Python package): gba_avg_divide turns
+ * each of n_cols device columns of n group SUMs (int64, or double where
+ * sum_is_fp[i]) into the double SUM / counts[i] in place, for AVGs merged from
+ * partial SUMs and COUNTs.  Synchronises `stream`.  No reference counterpart:
+ * the reference runs on one device (test/test.cu:35). */
+gba_status gba_avg_divide(gba_context* ctx, int32_t n_cols, void* const* sums, const int32_t* sum_is_fp,
+                          const int64_t* counts, int64_t n, void* stream);
+
 /* Autotuner: times the caller's own queries (device columns, as gba_groupby /
  * gba_groupby_batch take them) under candidate knobs by coordinate descent
  * from `base` and writes the fastest setting to *best (and its mean time per

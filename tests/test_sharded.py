@@ -1,0 +1,91 @@
+"""Sharded GROUP BY across ranks on CPU: gloo, world size 2.
+
+The range cuts, owner runs, exchange and merge logic of
+cpu_gpu_coprocess_groupby_agg_b200.sharded run for real over gloo all-reduces
+and all-to-alls; its device steps (local partial aggregation in key order,
+merge, AVG division) are stood in for by the oracle, so that the multi-rank
+path is covered without a GPU.  The union of the
+ranks' groups must equal the oracle over all rows, with each key on exactly one
+rank."""
+import os
+import sys
+from pathlib import Path
+
+import numpy as np
+import torch.multiprocessing as mp
+
+ROOT = Path(__file__).resolve().parents[1]
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "oracle"))
+
+AGGS = [("sum", 0), ("count", None), ("min", 0), ("max", 0), ("avg", 0), ("sum", 1), ("avg", 1)]
+
+
+class OracleOps:
+    """The sharded path's device steps, restated on the CPU oracle."""
+
+    def local(self, keys, cols, partials, unsigned_keys=False, unsigned_cols=(), knobs=None):
+        """Partial groups in key order."""
+        import torch
+        import cpu_oracle as O
+        k, outs = O.groupby(keys.numpy(), [c.numpy() for c in cols], list(partials), nthreads=2)
+        return torch.from_numpy(k), [torch.from_numpy(o) for o in outs]
+
+    def merge(self, keys, cols, merge_aggs, unsigned_keys=False):
+        return self.local(keys, cols, merge_aggs)
+
+    def avg_divide(self, sums, fp, count):
+        return [s.double() / count.double() for s in sums]
+
+
+def _data(seed=5, n=20_000):
+    rng = np.random.default_rng(seed)
+    dom = rng.integers(-(1 << 50), 1 << 50, size=3_000, dtype=np.int64)
+    keys = dom[rng.integers(0, len(dom), size=n)]
+    cols = [rng.integers(-(1 << 30), 1 << 30, size=n, dtype=np.int64), rng.standard_normal(n).astype(np.float32)]
+    return keys, cols
+
+
+def _worker(rank, world, port, q):
+    import torch
+    import torch.distributed as dist
+    from cpu_gpu_coprocess_groupby_agg_b200.sharded import groupby_sharded
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    keys, cols = _data()
+    mine = slice(rank, None, world)
+    r = groupby_sharded(None, torch.from_numpy(keys[mine].copy()), [torch.from_numpy(c[mine].copy()) for c in cols],
+                        AGGS, ops=OracleOps())
+    q.put((rank, r.keys.numpy(), [a.numpy() for a in r.aggs]))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_sharded_groupby_gloo():
+    import cpu_oracle as O
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 28000 + os.getpid() % 1000
+    ps = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    got = dict((r, (k, a)) for r, k, a in (q.get(timeout=120) for _ in range(2)))
+    for p in ps:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    k0, k1 = got[0][0], got[1][0]
+    assert len(np.intersect1d(k0, k1)) == 0, "a key on two ranks"
+    assert len(k0) > 0 and len(k1) > 0
+    gk = np.concatenate([k0, k1])
+    ga = [np.concatenate([got[0][1][i], got[1][1][i]]) for i in range(len(AGGS))]
+    order = np.argsort(gk)
+    gk, ga = gk[order], [a[order] for a in ga]
+    keys, cols = _data()
+    ek, (s0, c, mn, mx, s1, a1) = O.groupby(keys, cols, [("sum", 0), ("count", None), ("min", 0), ("max", 0),
+                                                        ("sum", 1), ("sumabs", 1)], nthreads=2)
+    np.testing.assert_array_equal(gk, ek)
+    for g, e in zip(ga[:4], (s0, c, mn, mx)):
+        np.testing.assert_array_equal(g, e)
+    np.testing.assert_array_equal(ga[4], s0.astype(np.float64) / c)
+    assert (np.abs(ga[5] - s1) <= 1e-6 * np.abs(s1) + 1e-12 * a1).all()
+    assert (np.abs(ga[6] - s1 / c) <= 1e-6 * np.abs(s1 / c) + 1e-12 * a1 / c).all()
