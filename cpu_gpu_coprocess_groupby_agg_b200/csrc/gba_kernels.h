@@ -17,8 +17,9 @@ enum AccOp : int {
   ACC_ADD_F = 4,  // SUM of an fp32 or fp64 column, accumulated in fp64
 };
 
-// bytes of one value of a column type
-__host__ __device__ inline int gba_type_bytes(int t) { return t == GBA_I64 || t == GBA_F64 ? 8 : 4; }
+// bytes of one value of a column type (I64 = 1 and F64 = 4 are the 8-byte
+// types: bits 1 and 4 of 0x12; one shift instead of two compares in row loops)
+__host__ __device__ inline int gba_type_bytes(int t) { return (0x12u >> t) & 1u ? 8 : 4; }
 
 // One query as the kernels see it (passed by value in the parameter space).
 struct QDesc {

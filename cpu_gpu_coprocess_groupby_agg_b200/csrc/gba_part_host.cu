@@ -172,6 +172,10 @@ gba_status gba_run_partition(gba_context* ctx, const QDesc& q, const gba_output*
       GBA_CUDA_TRY(ctx, cudaMemcpyAsync(W + o_snch, snch.data(), 4 * snch.size(), cudaMemcpyHostToDevice, s));
       PartPass pp;
       pp.in = in;
+      // the passes only move bytes: an fp64 column travels as I64, which keeps
+      // the scatter's column-width test the single compare it is tuned for
+      for (int c = 0; c < pp.in.ncols; ++c)
+        if (pp.in.col_type[c] == GBA_F64) pp.in.col_type[c] = GBA_I64;
       pp.out = outq;
       pp.chunks = reinterpret_cast<const PartChunk*>(W + o_chunks);
       pp.nchunks = int(chunks.size());

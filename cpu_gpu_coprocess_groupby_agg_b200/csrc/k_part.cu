@@ -27,7 +27,9 @@
 
 namespace {
 
-__host__ __device__ inline int col_bytes_t(int t) { return gba_type_bytes(t); }
+// width of a column in the partition passes, which see fp64 columns as I64
+// (gba_part_host.cu relabels them; the passes only move bytes)
+__host__ __device__ inline int col_bytes_t(int t) { return t == GBA_I64 ? 8 : 4; }
 
 // digit of a key for a pass: bits [32 - shift_hi - bits, 32 - shift_hi) of the hash
 template <bool K64>
@@ -322,7 +324,7 @@ __global__ void __launch_bounds__(1024, 1) k_part_agg(PartAgg a) {
 #pragma unroll
             for (int c = 0; c < GBA_MAX_COLS; ++c)
               if (c < Sig::ncols(q))
-                raw[u][c] = col_bytes_t(Sig::coltype(q, c)) == 8
+                raw[u][c] = gba_type_bytes(Sig::coltype(q, c)) == 8
                                 ? __ldg(static_cast<const unsigned long long*>(q.cols[c]) + r)
                                 : __ldg(static_cast<const unsigned*>(q.cols[c]) + r);
           }
