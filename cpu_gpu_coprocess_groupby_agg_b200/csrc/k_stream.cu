@@ -386,6 +386,7 @@ int gba_stream_rows_per_chunk(const QDesc& q, int minb) {
   int r = 0;
   gba_dispatch_sig(q, [&](auto, auto sig) -> cudaError_t {
     r = 32 * (minb == 4   ? stream_rows_per_lane<decltype(sig), 4>()
+              : minb == 3 ? stream_rows_per_lane<decltype(sig), 3>()
               : minb == 2 ? stream_rows_per_lane<decltype(sig), 2>()
                           : stream_rows_per_lane<decltype(sig), 1>());
     return cudaSuccess;
@@ -400,6 +401,7 @@ cudaError_t gba_prepare_stream_agg(const QDesc& proto, int minb) {
     constexpr bool k64 = decltype(K)::value;
     using Sig = decltype(sig);
     return minb == 4   ? gba_allow_max_smem(k_stream_agg<k64, Sig, 4>)
+           : minb == 3 ? gba_allow_max_smem(k_stream_agg<k64, Sig, 3>)
            : minb == 2 ? gba_allow_max_smem(k_stream_agg<k64, Sig, 2>)
                        : gba_allow_max_smem(k_stream_agg<k64, Sig, 1>);
   });
@@ -413,6 +415,8 @@ cudaError_t gba_launch_stream_agg(const QDesc& proto, int minb, const BatchQ* d_
     constexpr bool k64 = decltype(K)::value;
     using Sig = decltype(sig);
     if (minb == 4) k_stream_agg<k64, Sig, 4><<<grid, 512, smem, s>>>(d_qs, d_spans, nspans, nitems, item_ctr, sprobe);
+    else if (minb == 3)
+      k_stream_agg<k64, Sig, 3><<<grid, 512, smem, s>>>(d_qs, d_spans, nspans, nitems, item_ctr, sprobe);
     else if (minb == 2)
       k_stream_agg<k64, Sig, 2><<<grid, 512, smem, s>>>(d_qs, d_spans, nspans, nitems, item_ctr, sprobe);
     else k_stream_agg<k64, Sig, 1><<<grid, 512, smem, s>>>(d_qs, d_spans, nspans, nitems, item_ctr, sprobe);
