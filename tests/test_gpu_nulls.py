@@ -195,3 +195,46 @@ def test_nullable_refusals(ctx):
     st = lib.gba_groupby_host(ctx._h, C.byref(q), C.byref(o), C.byref(kn), C.c_void_p(0), C.byref(ng))
     assert st == A.ERR_UNSUPPORTED
     torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("batch", [False, True])
+def test_nullable_composite_sorted_together(ctx, batch):
+    """The rewrites stacked: a nullable column, a composite key, AVG and key
+    order in one query (alone and through the batch entry point)."""
+    import torch
+    rng = np.random.default_rng(12)
+    n = 60_000
+    k1 = rng.integers(-40, 40, size=n).astype(np.int32)
+    k2 = rng.integers(0, 50, size=n).astype(np.int32)
+    v = rng.integers(-1000, 1000, size=n, dtype=np.int64)
+    valid = rng.random(n) >= 0.4
+    valid[(k1 == 7) & (k2 == 3)] = False  # one group with no present value
+    aggs = [("avg", 0), ("count_valid", 0), ("count", None)]
+    dk = (to_device(k1), to_device(k2))
+    bm = [to_device(_bitmap(valid))]
+    if batch:
+        q = [(dk, [to_device(v)], aggs, False, [], bm)]
+        outs = ctx.batch_outputs(q)
+        outs[0] = (outs[0][0], outs[0][1], [torch.empty(n + 1, dtype=torch.uint8, device="cuda") for _ in aggs])
+        r = ctx.groupby_batch(q, outs=outs, knobs=dict(sort_output=1))[0]
+    else:
+        r = ctx.groupby(dk, [to_device(v)], aggs, col_valid=bm, agg_valid=True, knobs=dict(sort_output=1))
+    g1, g2 = (t.cpu().numpy() for t in r.keys)
+    # expected, in (k1, k2) order: the oracle on a 64-bit key that orders like the pair
+    comb = (k1.astype(np.int64) << 32) | (k2.astype(np.int64) & 0xFFFFFFFF)
+    ek, (cnt,) = O.groupby(comb, [v], [("count", None)], nthreads=8)
+    pk, (s, c) = O.groupby(comb[valid], [v[valid]], [("sum", 0), ("count", None)], nthreads=8)
+    pos = np.searchsorted(ek, pk)
+    avg = np.full(len(ek), np.nan)
+    avg[pos] = s.astype(np.float64) / c
+    cv = np.zeros(len(ek), dtype=np.int64)
+    cv[pos] = c
+    present = np.zeros(len(ek), dtype=np.uint8)
+    present[pos] = 1
+    np.testing.assert_array_equal(g1, (ek >> 32).astype(np.int32))
+    np.testing.assert_array_equal(g2, (ek & 0xFFFFFFFF).astype(np.int32))
+    np.testing.assert_array_equal(r.aggs[0].cpu().numpy(), avg)
+    np.testing.assert_array_equal(r.aggs[1].cpu().numpy(), cv)
+    np.testing.assert_array_equal(r.aggs[2].cpu().numpy(), cnt)
+    np.testing.assert_array_equal(r.valid[0].cpu().numpy(), present)
+    assert present.min() == 0  # the all-absent group is there
