@@ -174,13 +174,20 @@ __device__ __forceinline__ void smem_apply_rows(const SmemTable<K64>& t, const Q
   }
 }
 
+// A row's accumulator contributions, passed by value to the out-of-line slow
+// path: a reference to one row of the caller's v[R][NA] would take the array's
+// address and move all of it to local memory for the whole chunk.
+template <int NA>
+struct AccVals {
+  unsigned long long x[NA];
+};
+
 // HBM-table insert that did not find its key in the home slot (first
 // occurrence, or a displaced key): out of line, like bucket_find_or_insert.
 template <bool K64, typename Sig>
 __device__ __noinline__ void gtable_insert_slow(const GTable gt, const QDesc& q, uint64_t key, uint64_t home,
-                                                unsigned long long cur, const unsigned long long (&v)[Sig::NA],
-                                                unsigned* flags) {
-  gtable_finish<K64, Sig>(gt, q, key, home, cur, v, flags);
+                                                unsigned long long cur, const AccVals<Sig::NA> v, unsigned* flags) {
+  gtable_finish<K64, Sig>(gt, q, key, home, cur, v.x, flags);
 }
 
 template <bool K64, typename Sig, int R>
@@ -317,7 +324,10 @@ __device__ __forceinline__ void stream_chunk(const BatchQ& bq, const SmemTable<K
 #pragma unroll
       for (int a = 0; a < NA; ++a) global_acc(Sig::op(q, a), sp + 1 + a, v[i][a]);
     } else {
-      gtable_insert_slow<K64, Sig>(bq.gt, q, key[i], home[i], cur[i], v[i], bq.flags);
+      AccVals<NA> vv;
+#pragma unroll
+      for (int a = 0; a < NA; ++a) vv.x[a] = v[i][a];
+      gtable_insert_slow<K64, Sig>(bq.gt, q, key[i], home[i], cur[i], vv, bq.flags);
     }
   }
 }
