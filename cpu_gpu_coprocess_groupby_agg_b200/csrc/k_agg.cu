@@ -294,23 +294,26 @@ __global__ void __launch_bounds__(1024, 1) k_preagg(PreaggParams P) {
   smem_flush_to_gtable<K64, Sig>(q, P.gt, st, P.flags);
 }
 
-__global__ void k_table_init(GTable t, int naccs, QDesc q) {
+// Slots first, first + step, ... <= cap (cap is the all-ones key's side slot,
+// whose key word is its presence flag) get their key word and identities, one
+// slot per iteration (no division of a word index by the slot stride).
+__device__ __forceinline__ void init_slots(const GTable& t, int naccs, const unsigned long long (&id)[GBA_MAX_AGGS],
+                                           uint64_t first, uint64_t step) {
   const int stride = 1 + naccs;
-  const uint64_t total = (t.cap + 1) * stride;
-  for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < total;
-       i += uint64_t(gridDim.x) * blockDim.x) {
-    const uint64_t slot = i / stride;
-    const int w = int(i - slot * stride);
-    unsigned long long v;
-    if (w == 0) v = slot == t.cap ? 0ull : EMPTY64;
-    else {
-      v = 0ull;
+  for (uint64_t slot = first; slot <= t.cap; slot += step) {
+    unsigned long long* p = t.base + slot * stride;
+    p[0] = slot == t.cap ? 0ull : EMPTY64;
 #pragma unroll
-      for (int a = 0; a < GBA_MAX_AGGS; ++a)
-        if (a == w - 1) v = acc_identity(q.acc_op[a]);
-    }
-    t.base[i] = v;
+    for (int a = 0; a < GBA_MAX_AGGS; ++a)
+      if (a < naccs) p[1 + a] = id[a];
   }
+}
+
+__global__ void k_table_init(GTable t, int naccs, QDesc q) {
+  unsigned long long id[GBA_MAX_AGGS];
+#pragma unroll
+  for (int a = 0; a < GBA_MAX_AGGS; ++a) id[a] = a < naccs ? acc_identity(q.acc_op[a]) : 0ull;
+  init_slots(t, naccs, id, blockIdx.x * uint64_t(blockDim.x) + threadIdx.x, uint64_t(gridDim.x) * blockDim.x);
 }
 
 // Compaction of table slots [lo, hi) (hi - lo <= 2048) by a whole CTA of 256
@@ -409,24 +412,10 @@ __global__ void __launch_bounds__(256) k_batch_init(const BatchQ* qs, const int6
   const int64_t nb = blk_prefix[qi + 1] - blk_prefix[qi];
   const GTable t = qs[qi].gt;
   const QDesc& q = qs[qi].q;
-  const int stride = 1 + q.naccs;
   unsigned long long id[GBA_MAX_AGGS];
 #pragma unroll
   for (int a = 0; a < GBA_MAX_AGGS; ++a) id[a] = a < q.naccs ? acc_identity(q.acc_op[a]) : 0ull;
-  const uint64_t total = (t.cap + 1) * stride;
-  for (uint64_t i = uint64_t(b) * blockDim.x + threadIdx.x; i < total; i += uint64_t(nb) * blockDim.x) {
-    const uint64_t slot = i / stride;
-    const int w = int(i - slot * stride);
-    unsigned long long v;
-    if (w == 0) v = slot == t.cap ? 0ull : EMPTY64;
-    else {
-      v = 0ull;
-#pragma unroll
-      for (int a = 0; a < GBA_MAX_AGGS; ++a)
-        if (a == w - 1) v = id[a];
-    }
-    t.base[i] = v;
-  }
+  init_slots(t, q.naccs, id, uint64_t(b) * blockDim.x + threadIdx.x, uint64_t(nb) * blockDim.x);
 }
 
 // compaction of every query of a batch into its own output (blocks dealt as
