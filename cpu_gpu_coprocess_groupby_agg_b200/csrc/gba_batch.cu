@@ -314,13 +314,13 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   }
   // work items are cut at multiples of T rows (vector loads need aligned starts)
   const int T = 2048;
-  // CTAs per SM of the streaming kernel (1 to 4; automatic: 4).  More CTAs
+  // CTAs per SM of the streaming kernel (1 to 4; automatic: 3).  More CTAs
   // split each SM's shared memory and registers into smaller tables and fewer
   // rows per lane, but keep more warps and L2 requests in flight: measured on
   // the 256-query batch, the kernel takes 16.4 ms at 1, 11.1-12.3 ms at 2 and
-  // 10.3 ms at 4 (where registers spill); 3 (40 registers, few spills) is about
-  // 1% faster than 4 and is what the autotuner picks there.
-  const int bps = k.blocks_per_sm >= 1 && k.blocks_per_sm <= 3 ? k.blocks_per_sm : 4;
+  // 10.3 ms at 4 (where registers spill); 3 (40 registers, few spills) is 1-2%
+  // faster than 4 and is what the autotuner picks there.
+  const int bps = k.blocks_per_sm >= 1 && k.blocks_per_sm <= 4 ? k.blocks_per_sm : 3;
   // buckets probed in a shared table before a row goes to the HBM table
   const int sprobe = k.smem_probe_cap > 0 ? k.smem_probe_cap : 2;
   for (int i = 0; i < nq; ++i) {

@@ -217,9 +217,9 @@ extern "C" gba_status gba_server_create(gba_server** out, const gba_server_confi
   // thread must not meet another lane's workspace growth, whose cudaFree
   // synchronises the device.
   c.knobs.use_graph = 0;
-  // Lanes' batch kernels share the GPU: at the batch default of 4 CTAs per SM
-  // one lane's launch fills every SM and the others queue behind it; at 2 two
-  // lanes' launches fit side by side.
+  // Lanes' batch kernels share the GPU: at 3 or 4 CTAs per SM one lane's
+  // launch fills every SM and the others queue behind it; at 2 two lanes'
+  // launches fit side by side.
   if (c.knobs.blocks_per_sm == 0) c.knobs.blocks_per_sm = 2;
   gba_server* sv = new gba_server();
   sv->cfg = c;

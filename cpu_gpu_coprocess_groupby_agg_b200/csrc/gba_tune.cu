@@ -94,7 +94,7 @@ extern "C" gba_status gba_autotune(gba_context* ctx, int32_t nq, const gba_query
                       }});
     axes.push_back({"load", {nan, 0.25, 0.5, 0.7}, set_load});
   } else {
-    axes.push_back({"blocks_per_sm", {nan, 1, 2, 3}, [](gba_knobs& k, double v) {
+    axes.push_back({"blocks_per_sm", {nan, 1, 2, 4}, [](gba_knobs& k, double v) {
                       k.blocks_per_sm = std::isnan(v) ? 0 : int32_t(v);
                     }});
     axes.push_back({"load", {nan, 0.25, 0.5}, set_load});

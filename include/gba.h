@@ -125,7 +125,7 @@ typedef struct gba_knobs {
   int32_t preagg;         /* -1 auto, 0 off, 1 on */
   int32_t smem_slots;     /* shared-memory table slots per CTA */
   int32_t partition_bits; /* radix fan-out 2^bits */
-  int32_t blocks_per_sm;  /* single query: CTAs per SM of the pre-aggregation grid; batch: 1, 2, 3 or 4 (0 = 4) */
+  int32_t blocks_per_sm;  /* single query: CTAs per SM of the pre-aggregation grid; batch: 1, 2, 3 or 4 (0 = 3) */
   int32_t block_threads;
   int32_t tile_rows;
   int32_t nstages;        /* TMA pipeline depth */
