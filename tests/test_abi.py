@@ -69,3 +69,14 @@ def test_dropin_cxx_entry_points_exported():
     assert driver.exists()
     ldd = subprocess.run(["ldd", str(driver)], capture_output=True, text=True).stdout
     assert "libgba.so" in ldd and "not found" not in ldd.split("libgba.so")[1].splitlines()[0]
+
+
+def test_c_caller_compiles_and_links(tmp_path):
+    """include/gba.h is plain C11: a C caller using every struct field the
+    guide shows compiles without warnings and links against libgba.so."""
+    src = ROOT / "tests" / "drivers" / "c_caller.c"
+    out = tmp_path / "c_caller.so"
+    r = subprocess.run(["gcc", "-std=c11", "-Wall", "-Wextra", "-Wno-missing-field-initializers", "-Werror",
+                        "-I", str(ROOT / "include"), "-shared", "-fPIC", str(src), "-o", str(out),
+                        "-L", str(A.LIB_PATH.parent), "-lgba"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
