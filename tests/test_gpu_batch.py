@@ -91,10 +91,11 @@ def test_batch_overflow_reruns_query_alone(ctx):
 
 def test_batch_with_partition_members(ctx):
     qs = _queries(6, seed=11)
-    # plain sizing: 4M rows -> a 137 MB table, past the L2-resident bound -> partition
+    # plain sizing at load 0.055: 4M rows -> 2^27 slots, a 3.2 GB table, past the batch's
+    # 2 GB bound -> partition; the small queries stay on the table strategy
     keys, cols = _data(4_000_000, np.int64, 2_000_000, seed=99)
     qs.insert(3, (keys, cols, [("sum", 0), ("count", None)]))
-    res = ctx.groupby_batch(_device(qs))
+    res = ctx.groupby_batch(_device(qs), knobs=dict(load_factor=0.055))
     _check(qs, res, "mixed strategies")
     assert res[0].stats["strategy"] == A.STRATEGY_AUTO  # both kinds ran
 
