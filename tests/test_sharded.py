@@ -89,3 +89,29 @@ def test_sharded_groupby_gloo():
     np.testing.assert_array_equal(ga[4], s0.astype(np.float64) / c)
     assert (np.abs(ga[5] - s1) <= 1e-6 * np.abs(s1) + 1e-12 * a1).all()
     assert (np.abs(ga[6] - s1 / c) <= 1e-6 * np.abs(s1 / c) + 1e-12 * a1 / c).all()
+
+
+def test_range_cuts_and_owner_runs():
+    """The range cuts split [lo, hi] into nparts nonempty ranges that cover it;
+    the owner runs of a key-ordered shard follow them, u32 keys read unsigned."""
+    import torch
+    from cpu_gpu_coprocess_groupby_agg_b200.sharded import key_range, owner_counts, range_cuts
+    for lo, hi, p in [(0, 0, 1), (5, 5, 4), (-10, 10, 3), (-(1 << 63), (1 << 63) - 1, 8), (0, (1 << 32) - 1, 5)]:
+        cuts = range_cuts(lo, hi, p)
+        assert len(cuts) == p - 1
+        edges = [lo] + cuts + [hi + 1]
+        assert all(a <= b for a, b in zip(edges, edges[1:])) and edges[0] == lo and edges[-1] == hi + 1
+        if hi - lo + 1 >= p:
+            assert all(a < b for a, b in zip(edges, edges[1:])), (lo, hi, p)
+    # a key-ordered shard of signed keys
+    k = torch.tensor([-9, -3, 0, 2, 7, 10], dtype=torch.int64)
+    assert key_range(k) == (-9, 10)
+    cuts = range_cuts(-10, 10, 3)  # owners own [-10,-3), [-3,4), [4,10]
+    assert owner_counts(k, cuts) == [1, 3, 2]
+    # u32 keys held in an int32 tensor, in unsigned order (0x80000000 and up last)
+    u = torch.tensor([1, 2, 0x7FFFFFFF, -0x80000000, -1], dtype=torch.int32)
+    assert key_range(u, True) == (1, 0xFFFFFFFF)
+    assert owner_counts(u, range_cuts(0, 0xFFFFFFFF, 2), True) == [3, 2]
+    # an empty shard still reports one run per owner
+    assert key_range(torch.empty(0, dtype=torch.int64)) is None
+    assert owner_counts(torch.empty(0, dtype=torch.int64), [1, 2]) == [0, 0, 0]
