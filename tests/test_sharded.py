@@ -115,3 +115,16 @@ def test_range_cuts_and_owner_runs():
     # an empty shard still reports one run per owner
     assert key_range(torch.empty(0, dtype=torch.int64)) is None
     assert owner_counts(torch.empty(0, dtype=torch.int64), [1, 2]) == [0, 0, 0]
+
+
+def test_plan_partials_shares_partials():
+    """AVG becomes SUM and COUNT partials shared with the caller's own SUM and
+    COUNT; ops without a partial merge are refused."""
+    import pytest
+    from cpu_gpu_coprocess_groupby_agg_b200 import _abi as A
+    from cpu_gpu_coprocess_groupby_agg_b200.sharded import plan_partials
+    p = plan_partials([("sum", 0), ("avg", 0), ("count", None), ("avg", 1), ("max", 1)])
+    assert p.partials == [(A.SUM, 0), (A.COUNT, 0), (A.SUM, 1), (A.MAX, 1)]
+    assert p.final == [("col", 0), ("avg", 0, 1), ("col", 1), ("avg", 2, 1), ("col", 3)]
+    with pytest.raises(ValueError):
+        plan_partials([("count_valid", 0)])
