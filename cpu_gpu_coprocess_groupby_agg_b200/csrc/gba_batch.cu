@@ -334,7 +334,16 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
     ctx->est_skew = skew[i];
     gba_make_plan(ctx, qd[i], k, pred[i], &qi[i].p);
     qi[i].pred = pred[i];
-    const double table_bytes = double(qi[i].p.table_slots + 1) * 8.0 * double(1 + qd[i].naccs);
+    double table_bytes = double(qi[i].p.table_slots + 1) * 8.0 * double(1 + qd[i].naccs);
+    // A learned-sized table that cannot stay in L2 at the batch's load anyway
+    // (above twice its 126 MB) is sized at load 0.5: half the DRAM footprint for
+    // its inserts, at the cost of longer probes (an under-estimate still regrows).
+    if (k.sizing == GBA_SIZING_LEARNED && pred[i] > 0 && table_bytes > 256.0 * double(1 << 20)) {
+      const double g = std::min(double(std::max<int64_t>(qd[i].n, 1)), pred[i] * 1.25 + 64.0);
+      const uint64_t at_half = uint64_t(g / 0.5) + 1;
+      if (at_half < qi[i].p.table_slots) qi[i].p.table_slots = at_half;
+      table_bytes = double(qi[i].p.table_slots + 1) * 8.0 * double(1 + qd[i].naccs);
+    }
     qi[i].strategy = k.strategy != GBA_STRATEGY_AUTO ? k.strategy
                      : table_bytes <= kBatchTableMax ? GBA_STRATEGY_TABLE
                                                      : gba_choose_strategy(ctx, qd[i], k, pred[i], qi[i].p);
