@@ -138,35 +138,61 @@ def cpu_sample_rows(w) -> int:
     return min(w.n, 1 << 24)
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (first /proc/cpuinfo entry)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
 def run_reference(args, ws, rank):
-    """The reference arm: CPU restatement of the path on all host cores."""
+    """The reference arm: the CPU restatement of the path (the reference has no
+    CPU aggregation path of its own) on all host cores.  For the batch every
+    step is the WHOLE 256-query batch, the GPU arm's workload; inputs come
+    from the oracle's copy of the seeded generator, so this process never
+    loads the library.  A single-thread time over the batch's first queries is
+    reported beside it."""
     if rank != 0:
         return 0
     sys.path.insert(0, str(ROOT / "oracle"))
-    import numpy as np
     import cpu_oracle as O
-    from cpu_gpu_coprocess_groupby_agg_b200 import gen_host
+    from cpu_gpu_coprocess_groupby_agg_b200 import workloads as W  # generator specs only; no library load
     cores = os.cpu_count() or 1
     if args.workload == "batch":
-        from cpu_gpu_coprocess_groupby_agg_b200 import workloads as W
         allq = W.batch_queries()
-        sample, m = batch_cpu_sample(allq)
-        data = [gen_host(q.spec, q.n, nthreads=cores) for q in sample]
-        name, total_rows, aggs = BATCH_NAME, sum(q.n for q in allq), sample[0].aggs
+        name = BATCH_NAME
+        if args.ndv_range:
+            lo, hi = (float(x) for x in args.ndv_range.split(":"))
+            allq = [q for q in allq if lo <= q.meta["ndv"] < hi]
+            name = f"{BATCH_NAME}[ndv {args.ndv_range}]"
+        data = [O.gen(q.spec, q.n, nthreads=cores) for q in allq]
+        total_rows = m = sum(q.n for q in allq)
+        aggs = allq[0].aggs
 
-        def one():
-            for q, (k, c) in zip(sample, data):
-                O.groupby(k, c, q.aggs, nthreads=cores, sort=False)
-        what = f"the first {len(sample)} of the 256 queries ({m} rows) per step"
+        def one(threads=cores, upto=None):
+            for q, (k, c) in list(zip(allq, data))[:upto]:
+                O.groupby(k, c, q.aggs, nthreads=threads, sort=False)
+        what = f"all {len(allq)} queries of the batch ({m} rows) per step, the GPU arm's workload"
+        sample, m1 = batch_cpu_sample(allq)
+        single = (len(sample), m1)
+        same = True
     else:
         w = get_workload(args.workload)
         m = cpu_sample_rows(w)
-        keys, cols = gen_host(w.spec, m, nthreads=cores)
+        keys, cols = O.gen(w.spec, m, nthreads=cores)
         name, total_rows, aggs = w.name, w.n, w.aggs
 
-        def one():
-            O.groupby(keys, cols, w.aggs, nthreads=cores, sort=False)
+        def one(threads=cores, upto=None):
+            O.groupby(keys, cols, w.aggs, nthreads=threads, sort=False)
         what = f"first {m} rows of the workload per step"
+        single = (1, m)
+        same = m == w.n
     for _ in range(args.warmup):
         one()
     t0 = time.perf_counter()
@@ -174,16 +200,23 @@ def run_reference(args, ws, rank):
         one()
     dt = (time.perf_counter() - t0) / args.steps
     value = m / dt / 1e9
+    # one thread, over a bounded sample (the leading queries of the batch)
+    t1 = time.perf_counter()
+    one(threads=1, upto=single[0])
+    st_value = single[1] / (time.perf_counter() - t1) / 1e9
     line = {
         "impl": "reference", "metric": "groupby_rows_per_s", "value": round(value, 6), "unit": "G rows/s",
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
-        "data": "synthetic (seeded PCG32 generator)",
-        "config": {"workload": name, "rows": total_rows, "sample_rows_per_step": m,
+        "data": "synthetic (seeded PCG32 generator; the oracle's copy, bit-identical to the GPU arm's)",
+        "config": {"workload": name, "rows": total_rows, "rows_per_step": m, "same_config": same,
                    "aggs": [list(map(str, a)) for a in aggs]},
         "cpu_baseline": {"value": round(value, 6), "unit": "G rows/s", "cores": cores, "kind": "port",
+                         "cpu_model": cpu_model(),
                          "sample": f"{what} (partitioned hash aggregation, {cores} threads); the reference "
-                                   f"itself has no CPU aggregation path"},
+                                   f"itself has no CPU aggregation path",
+                         "single_thread": {"value": round(st_value, 6), "unit": "G rows/s", "cores": 1,
+                                           "sample": f"the first {single[0]} queries ({single[1]} rows), one pass"}},
         "e2e": {"value": round(value, 6), "unit": "G rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -461,20 +494,28 @@ def run_batch(args, ws, rank, local, pg):
     if not args.no_e2e and rank == 0:
         line["e2e"] = batch_e2e(ctx, allq, dq, outs, knobs_for(args.sizing), args)
     if not args.no_cpu_baseline and rank == 0 and ws == 1:
+        # the oracle over the whole batch (one pass, all host cores), and on
+        # one thread over the batch's leading queries
         sys.path.insert(0, str(ROOT / "oracle"))
         import cpu_oracle as O
-        sample, m = batch_cpu_sample(allq)
-        host = [(dq[i][0].cpu().numpy(), [c.cpu().numpy() for c in dq[i][1]]) for i in range(len(sample))]
+        host = [(k.cpu().numpy(), [c.cpu().numpy() for c in cs]) for k, cs, _ in dq]
         cores = os.cpu_count() or 1
-        for (k, c), q in zip(host, sample):
-            O.groupby(k, c, q.aggs, nthreads=cores, sort=False)
         t0 = time.perf_counter()
-        for (k, c), q in zip(host, sample):
+        for (k, c), q in zip(host, allq):
             O.groupby(k, c, q.aggs, nthreads=cores, sort=False)
         dt = time.perf_counter() - t0
-        line["cpu_baseline"] = {"value": round(m / dt / 1e9, 6), "unit": "G rows/s", "cores": cores, "kind": "port",
-                                "sample": f"the first {len(sample)} of the 256 queries ({m} rows), partitioned "
-                                          f"hash aggregation on {cores} threads"}
+        sample, m1 = batch_cpu_sample(allq)
+        t1 = time.perf_counter()
+        for (k, c), q in zip(host, sample):
+            O.groupby(k, c, q.aggs, nthreads=1, sort=False)
+        dt1 = time.perf_counter() - t1
+        del host
+        line["cpu_baseline"] = {"value": round(total_rows / dt / 1e9, 6), "unit": "G rows/s", "cores": cores,
+                                "kind": "port", "cpu_model": cpu_model(),
+                                "sample": f"all {len(allq)} queries ({total_rows} rows), one pass, partitioned "
+                                          f"hash aggregation on {cores} threads",
+                                "single_thread": {"value": round(m1 / dt1 / 1e9, 6), "unit": "G rows/s", "cores": 1,
+                                                  "sample": f"the first {len(sample)} queries ({m1} rows), one pass"}}
     if rank == 0:
         print(json.dumps(line), flush=True)
     del outs, dq
@@ -670,9 +711,16 @@ def cpu_baseline(w, keys, cols):
     for _ in range(reps):
         O.groupby(hk, hc, w.aggs, nthreads=cores, sort=False)
     dt = (time.perf_counter() - t0) / reps
+    m1 = min(m, 1 << 22)
+    t1 = time.perf_counter()
+    O.groupby(hk[:m1], [c[:m1] for c in hc], w.aggs, nthreads=1, sort=False)
+    dt1 = time.perf_counter() - t1
     return {"value": round(m / dt / 1e9, 6), "unit": "G rows/s", "cores": cores, "kind": "port",
+            "cpu_model": cpu_model(),
             "sample": f"first {m} rows of the workload, partitioned hash aggregation on {cores} threads, "
-                      f"mean of {reps} runs"}
+                      f"mean of {reps} runs",
+            "single_thread": {"value": round(m1 / dt1 / 1e9, 6), "unit": "G rows/s", "cores": 1,
+                              "sample": f"first {m1} rows, one pass"}}
 
 
 if __name__ == "__main__":

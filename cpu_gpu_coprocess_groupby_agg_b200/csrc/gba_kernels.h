@@ -64,6 +64,7 @@ enum : unsigned {
   GBA_FLAG_TABLE_OVERFLOW = 1u,  // an HBM-table insert ran out of probes
   GBA_FLAG_WAIT_TIMEOUT = 2u,    // a bounded mbarrier wait gave up
   GBA_FLAG_PART_OVERFLOW = 4u,   // a partition outgrew its shared table
+  GBA_FLAG_DRAIN_TIMEOUT = 8u,   // after an abort, a copy still in flight did not land in time
 };
 
 struct PreaggCfg {

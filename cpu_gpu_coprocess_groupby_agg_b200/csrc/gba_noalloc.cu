@@ -25,6 +25,7 @@
 
 #include "gba_context.h"
 #include "gba_plan.h"
+#include "nulls.h"
 
 // The fixed scratch: 16 MiB, 256-byte aligned.
 static constexpr size_t kNoallocScratchBytes = size_t(16) << 20;
@@ -39,7 +40,9 @@ void* g_noalloc_ptr[kMaxDevices] = {};
 
 // Address of this device's scratch, looked up once per device with that device
 // current (the caller has made it current).  The first lookup may make the
-// runtime load the library's device code.
+// runtime load the library's device code.  The address is kept for the life of
+// the process: a caller that resets the device (cudaDeviceReset) unloads the
+// module that holds the array, and must not call this entry point afterwards.
 gba_status noalloc_scratch(gba_context* ctx, unsigned char** out) {
   const int dev = ctx->device;
   if (dev < 0 || dev >= kMaxDevices) {
@@ -69,6 +72,13 @@ extern "C" gba_status gba_groupby_noalloc(gba_context* ctx, const gba_query* q_i
   GBA_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   ctx->stats = gba_stats{};
   ctx->stats.predicted_groups = -1;
+  // per-aggregate validity outputs and a second key output belong to the
+  // nullable-column and composite-key rewrites, which need scratch of their own
+  if (gba_nulls_needed(*q_in, *out) || out->keys2 || q_in->key2.data) {
+    ctx->err = "gba_groupby_noalloc: nullable columns, validity outputs (gba_output.agg_valid), COUNT(col) and "
+               "composite keys are supported by gba_groupby and gba_groupby_batch only";
+    return GBA_ERR_UNSUPPORTED;
+  }
   gba_query qc;
   gba_compact_query(q_in, &qc);
   QDesc q;

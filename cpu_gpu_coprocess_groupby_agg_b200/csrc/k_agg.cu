@@ -241,15 +241,19 @@ __global__ void __launch_bounds__(1024, 1) k_preagg(PreaggParams P) {
   };
 
   // prologue: fill the pipeline
+  unsigned pending = 0;  // (thread 0) bit s: stage s has a copy in flight
   if (P.use_tma && tid == 0) {
     for (int s = 0; s < P.nstages; ++s) {
       const int64_t tile = blockIdx.x + int64_t(s) * gridDim.x;
-      if (tile < nfull) issue(tile, s);
+      if (tile < nfull) {
+        issue(tile, s);
+        pending |= 1u << s;
+      }
     }
   }
 
   const unsigned lane = lane_id();
-  unsigned phase = 0;  // bit s = parity to wait for on stage s
+  unsigned phase = 0;  // bit s = parity to wait for on stage s (flipped only once that phase completed)
   int64_t it = 0;
   for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
     const int s = int(it % P.nstages);
@@ -257,8 +261,12 @@ __global__ void __launch_bounds__(1024, 1) k_preagg(PreaggParams P) {
     const int rows = int(n - r0 < int64_t(T) ? n - r0 : int64_t(T));
     const bool via_tma = P.use_tma && tile < nfull;
     if (via_tma) {
-      if (!mbar_wait_bounded(&bars[s], (phase >> s) & 1u, P.flags)) s_abort = 1;
-      phase ^= 1u << s;
+      if (mbar_wait_bounded(&bars[s], (phase >> s) & 1u, P.flags)) {
+        phase ^= 1u << s;
+        pending &= ~(1u << s);
+      } else {
+        s_abort = 1;
+      }
     }
     __syncthreads();
     if (s_abort) break;
@@ -274,17 +282,22 @@ __global__ void __launch_bounds__(1024, 1) k_preagg(PreaggParams P) {
         if (nxt < nfull) {
           fence_proxy_async_smem();
           issue(nxt, s);
+          pending |= 1u << s;
         }
       }
     }
   }
 
   if (s_abort) {
-    // drain: wait (bounded) for copies this CTA still has in flight
+    // drain: wait (bounded) for every copy this CTA still has in flight, the
+    // one whose wait gave up included (its phase bit was not flipped, so the
+    // wait is for the same phase), before the CTA's shared memory is released
     if (tid == 0 && P.use_tma) {
       for (int s = 0; s < P.nstages; ++s) {
-        for (unsigned k = 0; k < (1u << 20); ++k)
-          if (mbar_try_wait(&bars[s], (phase >> s) & 1u)) break;
+        if (!(pending >> s & 1u)) continue;
+        bool landed = false;
+        for (unsigned k = 0; k < (1u << 22) && !landed; ++k) landed = mbar_try_wait(&bars[s], (phase >> s) & 1u);
+        if (!landed) atomicOr(P.flags, GBA_FLAG_DRAIN_TIMEOUT);
       }
     }
     return;

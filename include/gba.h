@@ -220,7 +220,10 @@ gba_status gba_groupby_batch(gba_context* ctx, int32_t n_queries, const gba_quer
  * (about 349,000 rows with 2 aggregates); larger queries return
  * GBA_ERR_INVALID_ARG with the limit in gba_last_error and launch nothing.
  * The first call on a device looks up the scratch's address, which may load
- * the library's device code: make it before any stream capture begins.  Every
+ * the library's device code: make it before any stream capture begins.  The
+ * address is kept until the process exits, so do not call this entry point
+ * after resetting the device (cudaDeviceReset).  Nullable columns, validity
+ * outputs and composite keys return GBA_ERR_UNSUPPORTED.  Every
  * call clears the scratch's status and counter words and initialises its table
  * itself.  All calls on one device share the scratch: calls that overlap in
  * time on one device race; serialise them.  Synchronises `stream`. */

@@ -46,6 +46,8 @@ def lib() -> C.CDLL:
         L.orc_partition_of_u32.argtypes = [C.c_uint32, C.c_uint32]
         L.orc_partition_u32_array.restype = None
         L.orc_partition_u32_array.argtypes = [C.c_void_p, C.c_int64, C.c_uint32, C.c_void_p]
+        L.orc_gen.restype = C.c_int
+        L.orc_gen.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.POINTER(C.c_void_p), C.c_int]
         L.orc_merge_partitions.restype = C.c_int64
         L.orc_merge_partitions.argtypes = [C.c_void_p, C.c_int64, C.c_uint64, C.c_void_p, C.c_void_p]
         _lib = L
@@ -132,3 +134,19 @@ def digest_pairs(keys: np.ndarray, vals: np.ndarray) -> str:
     z = (keys.astype(np.uint32).astype(np.uint64) << np.uint64(32)) | vals.astype(np.uint32).astype(np.uint64)
     with np.errstate(over="ignore"):
         return f"{int(_mix64(z).sum(dtype=np.uint64)):016x}"
+
+
+_GEN_DTYPES = {0: np.int32, 1: np.int64, 2: np.float32, 3: np.int32}  # column kinds of datagen.h
+
+
+def gen(spec, n: int, row0: int = 0, nthreads: int = 1, key_unsigned: bool = False):
+    """Rows [row0, row0 + n) of a seeded generator spec (a ctypes structure with
+    the layout of datagen.h's gba_gen_spec) as numpy (keys, [columns])."""
+    kd = np.int64 if spec.key_bits == 64 else (np.uint32 if key_unsigned else np.int32)
+    keys = np.empty(n, dtype=kd)
+    cols = [np.empty(n, dtype=_GEN_DTYPES[spec.col_kind[i]]) for i in range(spec.ncols)]
+    ptrs = (C.c_void_p * 4)(*([c.ctypes.data for c in cols] + [None] * (4 - len(cols))))
+    rc = lib().orc_gen(C.addressof(spec), row0, n, keys.ctypes.data, ptrs, nthreads)
+    if rc != 0:
+        raise ValueError("orc_gen: bad generator spec")
+    return keys, cols

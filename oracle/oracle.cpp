@@ -27,6 +27,10 @@
 //                        the greedy min-heap merge of small partitions
 //                        (groupby_agg_intra_partition.cu:13-48) and the resulting
 //                        par_kv_begin prefix (groupby_agg_intra_partition.cu:303-311).
+//  * orc_gen             the benchmark's seeded input columns, from the same
+//                        generator header the library's own generator uses
+//                        (datagen.h), so the CPU arm of the benchmark produces
+//                        the GPU arm's inputs without loading the library.
 //
 // Parity with the reference itself is pinned by tests/golden/ fixtures produced by
 // running the unmodified reference (built by oracle/Makefile into oracle/_ref).
@@ -40,6 +44,8 @@
 #include <queue>
 #include <thread>
 #include <vector>
+
+#include "datagen.h"
 
 extern "C" {
 
@@ -406,6 +412,42 @@ int64_t orc_merge_partitions(const uint32_t* sizes, int64_t P, uint64_t K, int64
     H.pop();
   }
   return m;
+}
+
+// ---------------------------------------------------------------------------
+// Input generator: rows [row0, row0 + n) of a seeded spec, on nthreads threads
+// (every row is an independent PCG32 stream, so any split gives the same
+// columns).  keys: 4- or 8-byte column; cols[c]: int32, int64 or fp32 as the
+// spec's column kind says.  Returns 0, or -1 for a bad spec.
+int orc_gen(const gba_gen_spec* sp, int64_t row0, int64_t n, void* keys, void* const* cols, int nthreads) {
+  if (!sp || (sp->key_bits != 32 && sp->key_bits != 64) || sp->ndv < 1 || sp->ncols < 0 ||
+      sp->ncols > GBA_GEN_MAX_COLS || sp->zipf_s < 0 || n < 0)
+    return -1;
+  const gba_zipf z = gba_zipf_make(sp->ndv, sp->zipf_s > 0 ? sp->zipf_s : 1.0);
+  auto work = [&](int64_t lo, int64_t hi) {
+    for (int64_t i = lo; i < hi; ++i) {
+      uint64_t key;
+      int64_t iv[GBA_GEN_MAX_COLS];
+      float fv[GBA_GEN_MAX_COLS];
+      gba_gen_row(sp, &z, uint64_t(row0 + i), &key, iv, fv);
+      if (sp->key_bits == 64) static_cast<uint64_t*>(keys)[i] = key;
+      else static_cast<uint32_t*>(keys)[i] = uint32_t(key);
+      for (int c = 0; c < sp->ncols; ++c) {
+        if (sp->col_kind[c] == GBA_GEN_UNIFORM_I64) static_cast<int64_t*>(cols[c])[i] = iv[c];
+        else if (sp->col_kind[c] == GBA_GEN_NORMAL_F32) static_cast<float*>(cols[c])[i] = fv[c];
+        else static_cast<int32_t*>(cols[c])[i] = int32_t(iv[c]);
+      }
+    }
+  };
+  const int T = std::max(1, std::min(nthreads, 256));
+  if (T == 1 || n < 65536) {
+    work(0, n);
+  } else {
+    std::vector<std::thread> th;
+    for (int t = 0; t < T; ++t) th.emplace_back(work, n * t / T, n * (t + 1) / T);
+    for (auto& x : th) x.join();
+  }
+  return 0;
 }
 
 }  // extern "C"

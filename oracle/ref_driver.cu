@@ -11,6 +11,10 @@
 //   <out>.json  phase-1 partition sizes and pair digests, merged layout, timings
 //   <out>.bin   for every merged partition i: par_result_kv_num[i] (u64) then
 //               that many u32 keys and u32 sums from its result range
+// An optional 7th argument R runs both phases R times on the same input (the
+// pinned buffers are refilled from a copy before each run, outside the timed
+// region; the reference overwrites them in phase 1) and records every run's
+// times; the outputs are those of the last run.
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -48,6 +52,7 @@ int main(int argc, char** argv) {
   const size_t P = std::strtoull(argv[4], nullptr, 10);
   const size_t nstreams = std::strtoull(argv[5], nullptr, 10);
   const size_t Capacity = std::strtoull(argv[6], nullptr, 10);
+  const int repeat = argc > 7 ? std::max(1, std::atoi(argv[7])) : 1;
   FILE* f = std::fopen(in.c_str(), "rb");
   if (!f) return 3;
   int64_t n = 0;
@@ -56,19 +61,35 @@ int main(int argc, char** argv) {
   u_int32_t *keys, *vals;
   cudaMallocHost(&keys, sizeof(u_int32_t) * n);
   cudaMallocHost(&vals, sizeof(u_int32_t) * n);
-  if (std::fread(keys, 4, n, f) != size_t(n) || std::fread(vals, 4, n, f) != size_t(n)) return 3;
+  std::vector<u_int32_t> keys0(n), vals0(n);
+  if (std::fread(keys0.data(), 4, n, f) != size_t(n) || std::fread(vals0.data(), 4, n, f) != size_t(n)) return 3;
   std::fclose(f);
   cudaFree(nullptr);
 
-  std::vector<par_result> par_result_vec(P);
+  auto sec = [](auto a, auto z) { return std::chrono::duration<double>(z - a).count(); };
+  std::vector<double> p1_all, p2_all;
+  std::vector<par_result> par_result_vec;
+  key_type* out_keys = nullptr;
+  val_type* out_vals = nullptr;
+  std::vector<size_t> par_kv_begin, par_result_kv_num;
+  std::vector<uint32_t> p1_size(P);
+  std::vector<uint64_t> p1_digest(P);
+  for (int rep = 0; rep < repeat; ++rep) {
+  std::copy(keys0.begin(), keys0.end(), keys);
+  std::copy(vals0.begin(), vals0.end(), vals);
+  if (out_keys) cudaFreeHost(out_keys);
+  if (out_vals) cudaFreeHost(out_vals);
+  out_keys = nullptr;
+  out_vals = nullptr;
+  par_kv_begin.clear();
+  par_result_kv_num.clear();
+  par_result_vec.assign(P, par_result());
   auto t0 = std::chrono::steady_clock::now();
   groupby_agg_partition<u_int32_t, u_int32_t>(keys, vals, n, tile_len, P, par_result_vec, nstreams);
   cudaDeviceSynchronize();
   auto t1 = std::chrono::steady_clock::now();
 
   // phase-1 result: per partition, the multiset of (key, per-tile sum) pairs
-  std::vector<uint32_t> p1_size(P);
-  std::vector<uint64_t> p1_digest(P);
   for (size_t p = 0; p < P; ++p) {
     std::vector<std::pair<uint32_t, uint32_t>> pairs;
     auto& pr = par_result_vec[p];
@@ -78,14 +99,14 @@ int main(int argc, char** argv) {
     p1_digest[p] = digest_pairs(pairs);
   }
 
-  key_type* out_keys;
-  val_type* out_vals;
-  std::vector<size_t> par_kv_begin, par_result_kv_num;
   auto t2 = std::chrono::steady_clock::now();
   groupby_agg_intra_partition(par_result_vec, out_keys, out_vals, Capacity, Capacity * 3 / 5, Capacity * 4 / 5,
                               nstreams, par_kv_begin, par_result_kv_num);
   cudaDeviceSynchronize();
   auto t3 = std::chrono::steady_clock::now();
+  p1_all.push_back(sec(t0, t1));
+  p2_all.push_back(sec(t2, t3));
+  }
 
   FILE* b = std::fopen((outp + ".bin").c_str(), "wb");
   for (size_t i = 0; i < par_kv_begin.size(); ++i) {
@@ -97,10 +118,14 @@ int main(int argc, char** argv) {
   std::fclose(b);
 
   FILE* j = std::fopen((outp + ".json").c_str(), "w");
-  auto sec = [](auto a, auto z) { return std::chrono::duration<double>(z - a).count(); };
   std::fprintf(j, "{\"n\": %lld, \"tile_len\": %zu, \"P\": %zu, \"nstreams\": %zu, \"capacity\": %zu,\n",
                (long long)n, tile_len, P, nstreams, Capacity);
-  std::fprintf(j, " \"phase1_s\": %.6f, \"phase2_s\": %.6f,\n", sec(t0, t1), sec(t2, t3));
+  std::fprintf(j, " \"phase1_s\": %.6f, \"phase2_s\": %.6f,\n", p1_all.back(), p2_all.back());
+  std::fprintf(j, " \"phase1_s_all\": [");
+  for (size_t r = 0; r < p1_all.size(); ++r) std::fprintf(j, "%s%.6f", r ? ", " : "", p1_all[r]);
+  std::fprintf(j, "],\n \"phase2_s_all\": [");
+  for (size_t r = 0; r < p2_all.size(); ++r) std::fprintf(j, "%s%.6f", r ? ", " : "", p2_all[r]);
+  std::fprintf(j, "],\n");
   std::fprintf(j, " \"phase1_sizes\": [");
   for (size_t p = 0; p < P; ++p) std::fprintf(j, "%s%u", p ? ", " : "", p1_size[p]);
   std::fprintf(j, "],\n \"phase1_digests\": [");

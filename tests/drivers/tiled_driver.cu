@@ -12,6 +12,11 @@
 //               in the caller's buffers, timings
 //   <out>.bin   per merged partition i: par_result_kv_num[i] (u64), then that
 //               many u32 keys and u32 sums
+// An optional 7th argument R runs both phases R times on the same input (the
+// pinned buffers are refilled from a copy before each run, outside the timed
+// region, since phase 1 overwrites them) and records every run's times; the
+// outputs are those of the last run.
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -40,6 +45,7 @@ int main(int argc, char** argv) {
   const size_t P = std::strtoull(argv[4], nullptr, 10);
   const size_t nstreams = std::strtoull(argv[5], nullptr, 10);
   const size_t Capacity = std::strtoull(argv[6], nullptr, 10);
+  const int repeat = argc > 7 ? std::max(1, std::atoi(argv[7])) : 1;
   FILE* f = std::fopen(in.c_str(), "rb");
   if (!f) return 3;
   int64_t n = 0;
@@ -49,10 +55,35 @@ int main(int argc, char** argv) {
   val_type* vals = nullptr;
   cudaMallocHost(&keys, sizeof(key_type) * (n > 0 ? n : 1));
   cudaMallocHost(&vals, sizeof(val_type) * (n > 0 ? n : 1));
-  if (std::fread(keys, 4, n, f) != size_t(n) || std::fread(vals, 4, n, f) != size_t(n)) return 3;
+  std::vector<key_type> keys0(n);
+  std::vector<val_type> vals0(n);
+  if (std::fread(keys0.data(), 4, n, f) != size_t(n) || std::fread(vals0.data(), 4, n, f) != size_t(n)) return 3;
   std::fclose(f);
+  cudaFree(nullptr);
 
-  std::vector<par_result> par_result_vec(P);
+  auto sec = [](auto a, auto z) { return std::chrono::duration<double>(z - a).count(); };
+  std::vector<double> p1_all, p2_all;
+  std::vector<par_result> par_result_vec;
+  key_type* out_keys = nullptr;
+  val_type* out_vals = nullptr;
+  std::vector<size_t> par_kv_begin, par_result_kv_num;
+  std::vector<uint32_t> p1_size(P);
+  std::vector<uint64_t> p1_digest(P);
+  bool in_place = true;
+  const size_t tiles = tile_len ? (size_t(n) + tile_len - 1) / tile_len : 0;
+  std::vector<uint64_t> tile_fill(tiles, 0);
+  for (int rep = 0; rep < repeat; ++rep) {
+  std::copy(keys0.begin(), keys0.end(), keys);
+  std::copy(vals0.begin(), vals0.end(), vals);
+  if (out_keys) cudaFreeHost(out_keys);
+  if (out_vals) cudaFreeHost(out_vals);
+  out_keys = nullptr;
+  out_vals = nullptr;
+  par_kv_begin.clear();
+  par_result_kv_num.clear();
+  par_result_vec.assign(P, par_result());
+  in_place = true;
+  std::fill(tile_fill.begin(), tile_fill.end(), 0);
   auto t0 = std::chrono::steady_clock::now();
   try {
     groupby_agg_partition<key_type, val_type>(keys, vals, size_t(n), tile_len, P, par_result_vec, nstreams);
@@ -62,11 +93,6 @@ int main(int argc, char** argv) {
   }
   auto t1 = std::chrono::steady_clock::now();
 
-  std::vector<uint32_t> p1_size(P);
-  std::vector<uint64_t> p1_digest(P);
-  bool in_place = true;
-  const size_t tiles = tile_len ? (size_t(n) + tile_len - 1) / tile_len : 0;
-  std::vector<uint64_t> tile_fill(tiles, 0);
   for (size_t p = 0; p < P; ++p) {
     const par_result& pr = par_result_vec[p];
     uint64_t h = 0;
@@ -82,9 +108,6 @@ int main(int argc, char** argv) {
     p1_digest[p] = h;
   }
 
-  key_type* out_keys = nullptr;
-  val_type* out_vals = nullptr;
-  std::vector<size_t> par_kv_begin, par_result_kv_num;
   auto t2 = std::chrono::steady_clock::now();
   try {
     groupby_agg_intra_partition(par_result_vec, out_keys, out_vals, Capacity, Capacity * 3 / 5, Capacity * 4 / 5,
@@ -94,6 +117,9 @@ int main(int argc, char** argv) {
     return 6;
   }
   auto t3 = std::chrono::steady_clock::now();
+  p1_all.push_back(sec(t0, t1));
+  p2_all.push_back(sec(t2, t3));
+  }
 
   FILE* b = std::fopen((outp + ".bin").c_str(), "wb");
   for (size_t i = 0; i < par_kv_begin.size(); ++i) {
@@ -105,11 +131,15 @@ int main(int argc, char** argv) {
   std::fclose(b);
 
   FILE* j = std::fopen((outp + ".json").c_str(), "w");
-  auto sec = [](auto a, auto z) { return std::chrono::duration<double>(z - a).count(); };
   std::fprintf(j, "{\"n\": %lld, \"tile_len\": %zu, \"P\": %zu, \"nstreams\": %zu, \"capacity\": %zu,\n",
                (long long)n, tile_len, P, nstreams, Capacity);
-  std::fprintf(j, " \"phase1_s\": %.6f, \"phase2_s\": %.6f, \"segments_in_place\": %s,\n", sec(t0, t1), sec(t2, t3),
-               in_place ? "true" : "false");
+  std::fprintf(j, " \"phase1_s\": %.6f, \"phase2_s\": %.6f, \"segments_in_place\": %s,\n", p1_all.back(),
+               p2_all.back(), in_place ? "true" : "false");
+  std::fprintf(j, " \"phase1_s_all\": [");
+  for (size_t r = 0; r < p1_all.size(); ++r) std::fprintf(j, "%s%.6f", r ? ", " : "", p1_all[r]);
+  std::fprintf(j, "],\n \"phase2_s_all\": [");
+  for (size_t r = 0; r < p2_all.size(); ++r) std::fprintf(j, "%s%.6f", r ? ", " : "", p2_all[r]);
+  std::fprintf(j, "],\n");
   std::fprintf(j, " \"tile_groups\": [");
   for (size_t t = 0; t < tiles; ++t) std::fprintf(j, "%s%llu", t ? ", " : "", (unsigned long long)tile_fill[t]);
   std::fprintf(j, "],\n \"phase1_sizes\": [");

@@ -3,8 +3,8 @@
 Integer columns: the oracle's exact int64 sum rounded to double and divided by
 the count is the same IEEE computation the kernel does, so the result is
 bit-exact.  fp32 columns: the sums are fp64 in different orders, so the
-averages agree to the fp32-SUM tolerance (1e-6 relative, plus the sum's
-condition-number floor).  AVG is checked with and without a COUNT of its own in
+averages agree to the fp32-SUM tolerance (1e-6 relative, plus the FP64
+oracle's own rounding bound for nearly cancelling sums; tests/gpu_util.py).  AVG is checked with and without a COUNT of its own in
 the query, on the table and the partition strategy, with learned sizing, and through the
 batch entry point."""
 import numpy as np
@@ -12,17 +12,19 @@ import pytest
 
 import cpu_oracle as O
 from cpu_gpu_coprocess_groupby_agg_b200 import estimator as E
-from gpu_util import FP_ABS_PER_ABSSUM, FP_RTOL, run_gpu, sort_result, to_device
+from gpu_util import fp_bound, run_gpu, sort_result, to_device
 from test_gpu_parity import _data
 
 pytestmark = pytest.mark.gpu
 
 
 def _expected(keys, cols, col):
+    """(group keys, expected AVG, allowed error or None when bit-exact)."""
     ok, (s, c) = O.groupby(keys, cols, [("sum", col), ("count", None)], nthreads=8)
     if s.dtype == np.float64:
         _, (a,) = O.groupby(keys, cols, [("sumabs", col)], nthreads=8)
-        return ok, s / c.astype(np.float64), a / c.astype(np.float64)
+        avg = s / c.astype(np.float64)
+        return ok, avg, fp_bound(avg, a / c.astype(np.float64), c)
     return ok, s.astype(np.float64) / c.astype(np.float64), None
 
 
@@ -34,13 +36,12 @@ def test_avg_matches_oracle(ctx, strategy, kdt):
     gk, ga, res = run_gpu(ctx, keys, cols, aggs, knobs=dict(strategy=strategy))
     gk, ga = sort_result(gk, ga, False)
     for ai, col in ((0, 0), (2, 2), (3, 1)):
-        ok, avg, abs_avg = _expected(keys, cols, col)
+        ok, avg, bound = _expected(keys, cols, col)
         np.testing.assert_array_equal(gk, ok)
         assert ga[ai].dtype == np.float64
-        if abs_avg is None:
+        if bound is None:
             np.testing.assert_array_equal(ga[ai], avg, err_msg=f"avg of column {col}")
         else:
-            bound = FP_RTOL * np.abs(avg) + FP_ABS_PER_ABSSUM * abs_avg
             assert (np.abs(ga[ai] - avg) <= bound).all(), f"avg of fp32 column {col}"
     ok, (s2, mx) = O.groupby(keys, cols, [("sum", 2), ("max", 0)], nthreads=8)
     np.testing.assert_array_equal(ga[1], s2)
@@ -81,19 +82,18 @@ def test_avg_in_batch(ctx):
         for ai, (op, col) in enumerate(aggs):
             msg = f"query {qi} aggregate {ai} ({op})"
             if op == "avg":
-                ok, avg, abs_avg = _expected(keys, cols, col)
+                ok, avg, bound = _expected(keys, cols, col)
                 np.testing.assert_array_equal(gk, ok, err_msg=msg)
                 assert ga[ai].dtype == np.float64, msg
-                if abs_avg is None:
+                if bound is None:
                     np.testing.assert_array_equal(ga[ai], avg, err_msg=msg)
                 else:
-                    bound = FP_RTOL * np.abs(avg) + FP_ABS_PER_ABSSUM * abs_avg
                     assert (np.abs(ga[ai] - avg) <= bound).all(), msg
             else:
                 ok, (e,) = O.groupby(keys, cols, [(op, col)], nthreads=8)
                 np.testing.assert_array_equal(gk, ok, err_msg=msg)
                 if e.dtype == np.float64:
-                    _, (a,) = O.groupby(keys, cols, [("sumabs", col)], nthreads=8)
-                    assert (np.abs(ga[ai] - e) <= FP_RTOL * np.abs(e) + FP_ABS_PER_ABSSUM * a).all(), msg
+                    _, (a, cnt) = O.groupby(keys, cols, [("sumabs", col), ("count", None)], nthreads=8)
+                    assert (np.abs(ga[ai] - e) <= fp_bound(e, a, cnt)).all(), msg
                 else:
                     np.testing.assert_array_equal(ga[ai], e, err_msg=msg)

@@ -16,7 +16,7 @@ import pytest
 import cpu_oracle as O
 from cpu_gpu_coprocess_groupby_agg_b200 import _abi as A
 from cpu_gpu_coprocess_groupby_agg_b200.api import build_query, parse_aggs
-from gpu_util import FP_ABS_PER_ABSSUM, FP_RTOL, sort_result, to_device
+from gpu_util import fp_bound, sort_result, to_device
 
 pytestmark = pytest.mark.gpu
 
@@ -56,7 +56,7 @@ def _expected(keys, cols, valid, op, c):
         if cols[c].dtype == np.float32:
             _, (a,) = O.groupby(keys[m], [x[m] for x in cols], [("sumabs", c)], nthreads=8)
             absum = np.zeros(len(gk))
-            absum[pos] = a / pc if op == "avg" else a
+            absum[pos] = fp_bound(out[pos], a / pc if op == "avg" else a, pc)  # the allowed error
     else:
         info = np.iinfo(cols[c].dtype)
         fill = {"sum": 0, "min": int(info.max), "max": int(info.min)}[op]
@@ -84,8 +84,7 @@ def _check(res, keys, cols, valid, aggs, label, presorted=False):
         np.testing.assert_array_equal(gk, ek, err_msg=msg)
         np.testing.assert_array_equal(gv[i], ev, err_msg=msg + " validity")
         if absum is not None:
-            ok = np.isclose(ga[i], e, rtol=0, atol=0, equal_nan=True) | (
-                np.abs(ga[i] - e) <= FP_RTOL * np.abs(e) + FP_ABS_PER_ABSSUM * absum)
+            ok = np.isclose(ga[i], e, rtol=0, atol=0, equal_nan=True) | (np.abs(ga[i] - e) <= absum)
             assert ok.all(), msg
         else:
             np.testing.assert_array_equal(ga[i], e, err_msg=msg)

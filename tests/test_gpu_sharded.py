@@ -17,7 +17,7 @@ import pytest
 import cpu_oracle as O
 from cpu_gpu_coprocess_groupby_agg_b200.sharded import (DeviceOps, groupby_sharded, key_range, merge_partials,
                                                         owner_counts, plan_partials, range_cuts)
-from gpu_util import FP_ABS_PER_ABSSUM, FP_RTOL, to_device
+from gpu_util import fp_bound, to_device
 
 pytestmark = pytest.mark.gpu
 
@@ -42,8 +42,8 @@ def _check(gk, ga, keys, cols, label):
     for g, e in zip(ga[:4], (s0, c, mn, mx)):
         np.testing.assert_array_equal(g, e, err_msg=label)
     np.testing.assert_array_equal(ga[4], s0.astype(np.float64) / c, err_msg=label)
-    assert (np.abs(ga[5] - s1) <= FP_RTOL * np.abs(s1) + FP_ABS_PER_ABSSUM * a1).all(), label
-    assert (np.abs(ga[6] - s1 / c) <= FP_RTOL * np.abs(s1 / c) + FP_ABS_PER_ABSSUM * a1 / c).all(), label
+    assert (np.abs(ga[5] - s1) <= fp_bound(s1, a1, c)).all(), label
+    assert (np.abs(ga[6] - s1 / c) <= fp_bound(s1 / c, a1 / c, c)).all(), label
 
 
 @pytest.mark.parametrize("kdt", [np.int32, np.int64, np.uint32])

@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 import cpu_oracle as O
-from gpu_util import FP_ABS_PER_ABSSUM, FP_RTOL, run_gpu, to_device
+from gpu_util import fp_bound, run_gpu, to_device
 from test_gpu_parity import _data
 
 pytestmark = pytest.mark.gpu
@@ -25,8 +25,8 @@ def _check_ordered(gk, ga, keys, cols, aggs, label):
     np.testing.assert_array_equal(gk, ok, err_msg=f"{label}: keys out of order or wrong")
     for i, ((op, col), g, o) in enumerate(zip(aggs, ga, oa)):
         if o.dtype == np.float64:
-            _, (a,) = O.groupby(keys, cols, [("sumabs", col)], nthreads=8)
-            assert (np.abs(g - o) <= FP_RTOL * np.abs(o) + FP_ABS_PER_ABSSUM * a).all(), f"{label}: agg {i}"
+            _, (a, cnt) = O.groupby(keys, cols, [("sumabs", col), ("count", None)], nthreads=8)
+            assert (np.abs(g - o) <= fp_bound(o, a, cnt)).all(), f"{label}: agg {i}"
         else:
             np.testing.assert_array_equal(g, o, err_msg=f"{label}: agg {i} ({op})")
 

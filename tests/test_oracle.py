@@ -156,3 +156,23 @@ def test_generator_properties():
     sp = gen_spec(1, 32, 1024, 0.0, [("i32", 0, 1000)], avoid_all_ones=True)
     k, _ = gen_host(sp, 1 << 16, key_unsigned=True)
     assert len(np.unique(k)) == 1024 and not (k == 0xFFFFFFFF).any()
+
+
+def test_oracle_generator_matches_the_library_generator():
+    """The reference arm of the benchmark generates its inputs with the
+    oracle's copy of the generator (it must not load the library); both must
+    give the same bytes."""
+    from cpu_gpu_coprocess_groupby_agg_b200 import gen_host, gen_spec, workloads as W
+    specs = [gen_spec(11, 64, 1000, 1.0, [("i64", -5, 5), ("normal",), ("i32", 0, 1000)], permute_ids=False),
+             gen_spec(1, 32, 1024, 0.0, [("i32", 0, 1000)], avoid_all_ones=True),
+             gen_spec(7, 32, 300_000, 1.45, [("i64", 0, 1 << 31)])]
+    specs += [q.spec for q in W.batch_queries()[:6]]
+    for sp in specs:
+        for row0, n, th in ((0, 70_000, 4), (123_457, 5000, 1)):
+            k1, c1 = gen_host(sp, n, row0=row0, nthreads=th)
+            k2, c2 = O.gen(sp, n, row0=row0, nthreads=3)
+            assert k1.dtype == k2.dtype
+            np.testing.assert_array_equal(k1, k2)
+            for a, b in zip(c1, c2):
+                assert a.dtype == b.dtype
+                np.testing.assert_array_equal(a, b)

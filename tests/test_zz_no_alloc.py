@@ -1,6 +1,7 @@
 """gba_groupby_noalloc (fixed static scratch, no device allocation) through the
-C ABI: the same groups and aggregates as gba_groupby on two calls in a row, in
-this process after the other tests and in a fresh process of its own."""
+C ABI: the same groups and aggregates as gba_groupby and as the CPU oracle on
+two calls in a row, in this process after the other tests and in a fresh
+process of its own."""
 import ctypes as C
 import os
 import subprocess
@@ -9,6 +10,8 @@ from pathlib import Path
 
 import numpy as np
 import pytest
+
+import cpu_oracle as O
 
 from cpu_gpu_coprocess_groupby_agg_b200 import _abi as A
 from cpu_gpu_coprocess_groupby_agg_b200.api import build_query, parse_aggs
@@ -30,8 +33,9 @@ def _data(n, kdt, ndv, seed):
     return keys, cols
 
 
-def _noalloc(ctx, dk, dcols, aggs, unsigned_keys=False):
-    """Calls gba_groupby_noalloc directly through ctypes; returns (status, keys, aggs)."""
+def _noalloc(ctx, dk, dcols, aggs, unsigned_keys=False, valid_out=False):
+    """Calls gba_groupby_noalloc directly through ctypes; returns (status, keys, aggs).
+    valid_out: also pass a per-aggregate validity output (not supported)."""
     import torch
     n = dk.numel()
     kt = A.U32 if unsigned_keys else {torch.int32: A.I32, torch.int64: A.I64}[dk.dtype]
@@ -47,6 +51,9 @@ def _noalloc(ctx, dk, dcols, aggs, unsigned_keys=False):
     for i, t in enumerate(oaggs):
         o.aggs[i] = t.data_ptr()
     o.capacity = cap
+    if valid_out:
+        vbuf = torch.empty(cap, dtype=torch.uint8, device=dk.device)
+        o.agg_valid[0] = vbuf.data_ptr()
     ng = C.c_int64(-1)
     s = torch.cuda.current_stream(dk.device)
     st = ctx._lib.gba_groupby_noalloc(ctx._h, C.byref(q), C.byref(o), C.c_void_p(s.cuda_stream), C.byref(ng))
@@ -63,8 +70,8 @@ def _sorted(keys, aggs, unsigned):
 
 
 def _check_same(ctx, keys, cols, aggs):
-    """noalloc twice in a row == gba_groupby (integers bit-exact, fp32 sums
-    within 1e-6 relative)."""
+    """noalloc twice in a row == gba_groupby and == the oracle (integers
+    bit-exact, fp32 sums within 1e-6 relative of the FP64 oracle)."""
     import torch
     unsigned = keys.dtype == np.uint32
     dk = torch.from_numpy(keys.view(np.int32) if unsigned else keys).cuda()
@@ -72,6 +79,7 @@ def _check_same(ctx, keys, cols, aggs):
     ref = ctx.groupby(dk, dcols, aggs, unsigned_keys=unsigned)
     rk = ref.keys.cpu().numpy()
     rk, ra = _sorted(rk, [a.cpu().numpy() for a in ref.aggs], unsigned)
+    ok, oa = O.groupby(keys, cols, aggs, nthreads=8)
     for call in range(2):
         st, k, a = _noalloc(ctx, dk, dcols, aggs, unsigned_keys=unsigned)
         assert st == A.OK, (call, st, ctx._lib.gba_last_error(ctx._h))
@@ -82,6 +90,12 @@ def _check_same(ctx, keys, cols, aggs):
                 np.testing.assert_allclose(x, y, rtol=1e-6, atol=0, err_msg=f"call {call}: agg {aggs[i]}")
             else:
                 np.testing.assert_array_equal(x, y, err_msg=f"call {call}: agg {aggs[i]}")
+        np.testing.assert_array_equal(k, ok, err_msg=f"call {call}: keys vs oracle")
+        for i, (x, y) in enumerate(zip(a, oa)):
+            if x.dtype == np.float64:
+                np.testing.assert_allclose(x, y, rtol=1e-6, atol=0, err_msg=f"call {call}: agg {aggs[i]} vs oracle")
+            else:
+                np.testing.assert_array_equal(x, y, err_msg=f"call {call}: agg {aggs[i]} vs oracle")
 
 
 # 5 aggregates: at most 174,727 rows fit the 16 MiB scratch
@@ -118,10 +132,21 @@ def test_noalloc_rejects_queries_beyond_the_scratch(ctx):
     assert str(SCRATCH_BYTES) in msg and "rows" in msg, msg
 
 
+def test_noalloc_rejects_validity_outputs(ctx):
+    import torch
+    keys, cols = _data(1000, np.int64, 50, seed=3)
+    dk = torch.from_numpy(keys).cuda()
+    dcols = [torch.from_numpy(c).cuda() for c in cols]
+    st, _, _ = _noalloc(ctx, dk, dcols, AGGS, valid_out=True)
+    assert st == A.ERR_UNSUPPORTED
+    assert "agg_valid" in ctx._lib.gba_last_error(ctx._h).decode()
+
+
 _FRESH = r"""
 import sys
 sys.path.insert(0, {root!r})
 sys.path.insert(0, {tests!r})
+sys.path.insert(0, {oracle!r})
 import numpy as np
 from cpu_gpu_coprocess_groupby_agg_b200 import Context
 import test_zz_no_alloc as T
@@ -139,7 +164,7 @@ print("FRESH-OK")
 
 
 def test_noalloc_in_a_fresh_process():
-    code = _FRESH.format(root=str(ROOT), tests=str(ROOT / "tests"))
+    code = _FRESH.format(root=str(ROOT), tests=str(ROOT / "tests"), oracle=str(ROOT / "oracle"))
     env = dict(os.environ)
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600, env=env,
                        cwd=str(ROOT))
