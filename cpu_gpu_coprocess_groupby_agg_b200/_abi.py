@@ -25,7 +25,7 @@ I32, I64, F32, U32, F64 = 0, 1, 2, 3, 4
 # gba_op
 SUM, COUNT, MIN, MAX, AVG, COUNT_VALID = 0, 1, 2, 3, 4, 5
 # gba_sizing
-SIZING_PLAIN, SIZING_LEARNED, SIZING_FIXED = 0, 1, 2
+SIZING_PLAIN, SIZING_LEARNED, SIZING_FIXED, SIZING_GROW = 0, 1, 2, 3
 # gba_strategy
 STRATEGY_AUTO, STRATEGY_TABLE, STRATEGY_PARTITION = 0, 1, 2
 # generator column kinds (csrc/datagen.h)
@@ -81,6 +81,7 @@ class Knobs(C.Structure):
         ("learned_load", C.c_double),
         ("learned_min_rows", C.c_int64),
         ("sort_output", C.c_int32),
+        ("cluster_ctas", C.c_int32),
     ]
 
 

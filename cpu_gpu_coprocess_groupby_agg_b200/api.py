@@ -49,7 +49,8 @@ def make_knobs(**kw) -> A.Knobs:
     A.lib().gba_default_knobs(C.byref(k))
     for name, val in kw.items():
         if name == "sizing" and isinstance(val, str):
-            val = {"plain": A.SIZING_PLAIN, "learned": A.SIZING_LEARNED, "fixed": A.SIZING_FIXED}[val]
+            val = {"plain": A.SIZING_PLAIN, "learned": A.SIZING_LEARNED, "fixed": A.SIZING_FIXED,
+                   "grow": A.SIZING_GROW}[val]
         if name == "strategy" and isinstance(val, str):
             val = {"auto": A.STRATEGY_AUTO, "table": A.STRATEGY_TABLE, "partition": A.STRATEGY_PARTITION}[val]
         setattr(k, name, val)

@@ -364,7 +364,13 @@ void gba_make_plan(const gba_context* ctx, const QDesc& q, const gba_knobs& k, d
   const double lf = (k.load_factor > 0.05 && k.load_factor < 0.95) ? k.load_factor : 0.5;
   const double llf = (k.learned_load > 0.05 && k.learned_load < 0.95) ? k.learned_load : 0.35;
   uint64_t cap;
+  // GROW: the plain capacity, capped at a modest start (table_slots, default
+  // 2^16 slots); a table that overflows regrows 4x per rerun, the estimator-free
+  // alternative to sizing by the row count.
   if (k.sizing == GBA_SIZING_FIXED && k.table_slots > 0) cap = uint64_t(k.table_slots);
+  else if (k.sizing == GBA_SIZING_GROW)
+    cap = std::min<uint64_t>(gba_pow2_ceil(uint64_t(double(std::max<int64_t>(q.n, 1)) / lf)),
+                             k.table_slots > 0 ? uint64_t(k.table_slots) : (uint64_t(1) << 16));
   else if (k.sizing == GBA_SIZING_LEARNED && predicted_groups > 0)
     cap = uint64_t(std::min(double(std::max<int64_t>(q.n, 1)), predicted_groups * 1.25 + 64.0) / llf) + 1;
   else cap = gba_pow2_ceil(uint64_t(double(std::max<int64_t>(q.n, 1)) / lf));

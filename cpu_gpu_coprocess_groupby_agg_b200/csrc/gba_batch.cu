@@ -62,7 +62,8 @@ struct QInfo {
   GbaPlan p;
   double pred = -1;
   int strategy = GBA_STRATEGY_TABLE;
-  int S = 0;         // shared-table slots in the batch kernel
+  int S = 0;         // shared-table slots in the batch kernel (per CTA)
+  int cl = 1;        // CTAs of the cluster whose tables form the query's shared table
   int slot = -1;     // index among the table-strategy queries
 };
 
@@ -71,6 +72,9 @@ struct Group {
   QDesc proto;
   std::vector<int> members;  // indices into the batch's queries
   size_t smem = 0;           // dynamic shared memory of the group's launch
+  size_t stage_bytes = 0;    // bulk-copy kernel: bytes of one ring slot
+  int cluster = 1;           // bulk-copy kernel: CTAs per cluster
+  int minb = 1;              // CTAs per SM of the launch
   int64_t item_begin = 0, nitems = 0;  // item_begin: index of the group's first span
   int nspans = 0;
   int grid = 0;
@@ -117,6 +121,19 @@ int batch_smem_slots(const gba_context* ctx, const QDesc& q, int bps) {
   // between the CTAs, each losing 1 KB to the system)
   const size_t budget = (size_t(ctx->max_smem_optin) + 1024) / size_t(bps) - 1024;
   const size_t fixed = gba_stream_smem_bytes(q, 0) + gba_batch_static_smem() + 1024;
+  if (budget <= fixed) return 0;
+  const size_t slot = (q.key64 ? 8 : 4) + 8 * size_t(q.nwords);
+  const int S = int(std::min<size_t>(16384, (budget - fixed) / slot));
+  return S < 32 ? 0 : S;
+}
+
+// Shared-table slots of a query in the bulk-copy streaming kernel with `minb`
+// CTAs per SM: what a CTA's share of the SM's shared memory holds beside its
+// warps' copy rings (`nst` slots of `slot_bytes` each) and its static part
+// (barriers, chunk starts: 2 KB at most).
+int tma_smem_slots(const gba_context* ctx, const QDesc& q, int minb, int nst, size_t slot_bytes) {
+  const size_t budget = (size_t(ctx->max_smem_optin) + 1024) / size_t(minb) - 1024;
+  const size_t fixed = gba_stream_tma_smem_bytes(q, 0, nst, slot_bytes) + gba_batch_static_smem() + 2048;
   if (budget <= fixed) return 0;
   const size_t slot = (q.key64 ? 8 : 4) + 8 * size_t(q.nwords);
   const int S = int(std::min<size_t>(16384, (budget - fixed) / slot));
@@ -320,7 +337,14 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   // the 256-query batch, the kernel takes 16.4 ms at 1, 11.1-12.3 ms at 2 and
   // 10.3 ms at 4 (where registers spill); 3 (40 registers, few spills) is 1-2%
   // faster than 4 and is what the autotuner picks there.
-  const int bps = k.blocks_per_sm >= 1 && k.blocks_per_sm <= 4 ? k.blocks_per_sm : 3;
+  // The streaming kernel: by default the bulk-copy one (k_stream_tma: 1 or 2
+  // CTAs per SM, automatic 2, each warp staging its rows through a ring of
+  // `nst` slots); knobs.use_tma = 0 selects the register-loading one
+  // (k_stream_agg, 1 to 4 CTAs per SM).
+  const bool tma_kernel = k.use_tma != 0;
+  const int nst = k.nstages >= 1 && k.nstages <= 4 ? k.nstages : 3;
+  const int bps = tma_kernel ? (k.blocks_per_sm == 1 ? 1 : 2)
+                             : (k.blocks_per_sm >= 1 && k.blocks_per_sm <= 4 ? k.blocks_per_sm : 3);
   // buckets probed in a shared table before a row goes to the HBM table
   const int sprobe = k.smem_probe_cap > 0 ? k.smem_probe_cap : 2;
   // Strategy: a query alone leaves the HBM-table strategy once its table
@@ -349,24 +373,56 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
                                                      : gba_choose_strategy(ctx, qd[i], k, pred[i], qi[i].p);
   }
 
-  // ---- group the table-strategy queries by aggregate signature ----
+  // ---- cluster tables ----
+  // A query whose predicted groups outgrow one CTA's shared table (more than
+  // half its slots) but fit the tables of a cluster of 2-16 CTAs at load 0.7
+  // gets such a cluster (the smallest that fits): its rows then meet a
+  // shared-memory table spread over the cluster instead of the HBM table.
+  // Learned sizing only (the group count is needed); integer SUM/COUNT
+  // signatures only.
+  const int maxcl = k.cluster_ctas == 1 ? 1 : (k.cluster_ctas >= 2 && k.cluster_ctas <= 16 ? k.cluster_ctas : 8);
+  for (int i = 0; i < nq && tma_kernel && maxcl > 1; ++i) {
+    if (qi[i].strategy != GBA_STRATEGY_TABLE || !qi[i].p.preagg || qi[i].pred <= 0 || k.smem_slots > 0 ||
+        !gba_stream_tma_cluster_ok(qd[i]))
+      continue;
+    const double S1 = tma_smem_slots(ctx, qd[i], 1, nst, gba_stream_tma_slot_bytes(qd[i], 1));
+    if (S1 <= 0 || qi[i].pred <= 0.5 * S1) continue;
+    for (int c = 2; c <= maxcl; c *= 2)
+      if (qi[i].pred <= 0.7 * c * S1) {
+        qi[i].cl = c;
+        break;
+      }
+  }
+
+  // ---- group the table-strategy queries by aggregate signature (and cluster) ----
   std::vector<Group> groups;
   std::vector<int> tq;  // table-strategy queries, group by group
   for (int i = 0; i < nq; ++i) {
     if (qi[i].strategy != GBA_STRATEGY_TABLE) continue;
-    const int sig = 2 * gba_batch_sig_id(qd[i]) + (qd[i].key64 ? 1 : 0);  // one launch per signature and key width
+    // one launch per signature, key width and cluster size
+    const int sig = (2 * gba_batch_sig_id(qd[i]) + (qd[i].key64 ? 1 : 0)) * 32 + qi[i].cl;
     auto it = std::find_if(groups.begin(), groups.end(), [&](const Group& g) { return g.sig == sig; });
     if (it == groups.end()) {
       groups.push_back(Group{sig, qd[i], {}});
+      groups.back().cluster = qi[i].cl;
       it = groups.end() - 1;
     }
     it->members.push_back(i);
   }
   for (auto& g : groups) {
     g.smem = gba_stream_smem_bytes(g.proto, 0);
+    g.minb = g.cluster > 1 ? 1 : bps;
+    if (tma_kernel) {
+      // one ring slot holds a chunk of any member (run-time signatures may
+      // differ in columns per member)
+      for (int i : g.members) g.stage_bytes = std::max(g.stage_bytes, gba_stream_tma_slot_bytes(qd[i], g.minb));
+      g.smem = gba_stream_tma_smem_bytes(g.proto, 0, nst, g.stage_bytes);
+    }
     for (int i : g.members) {
       // run-time signatures may differ in accumulator words per member
-      int S = qi[i].p.preagg ? batch_smem_slots(ctx, qd[i], bps) : 0;
+      int S = !qi[i].p.preagg ? 0
+              : tma_kernel    ? tma_smem_slots(ctx, qd[i], g.minb, nst, g.stage_bytes)
+                              : batch_smem_slots(ctx, qd[i], bps);
       if (k.smem_slots > 0) S = std::min(S, k.smem_slots);
       // a known-small group count needs only a small shared table (cheaper
       // to clear and flush per work item)
@@ -374,9 +430,23 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
       if (S > 0 && qi[i].pred > 0) S = std::min<int64_t>(S, std::max<int64_t>(256, int64_t(qi[i].pred * 4.0 + 31) / 32 * 32));
       S = S / 4 * 4;  // whole 16-byte buckets
       qi[i].S = S;
-      g.smem = std::max(g.smem, gba_stream_smem_bytes(qd[i], S));
+      g.smem = std::max(g.smem, tma_kernel ? gba_stream_tma_smem_bytes(qd[i], S, nst, g.stage_bytes)
+                                           : gba_stream_smem_bytes(qd[i], S));
       qi[i].slot = int(tq.size());
       tq.push_back(i);
+    }
+    // a cluster launch fills as many clusters as can be resident at once;
+    // where none can, its queries run as single CTAs (smaller tables, same
+    // results)
+    g.grid = ctx->sms * g.minb;
+    if (g.cluster > 1) {
+      GBA_CUDA_TRY(ctx, gba_prepare_stream_tma(g.proto, g.cluster, 1));
+      const int cg = gba_stream_tma_cluster_grid(g.proto, g.cluster, g.smem, ctx->sms);
+      if (cg >= g.cluster) g.grid = cg;
+      else {
+        g.cluster = 1;
+        for (int i : g.members) qi[i].cl = 1;
+      }
     }
   }
   const int nt = int(tq.size());
@@ -389,7 +459,6 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   // and the random table updates spilled from L2 to DRAM).  A query's rows
   // are cut into about one item per CTA (at least one tile, at most
   // item_rows or 2^20 rows), so one query occupies the whole grid.
-  const int grid_max = ctx->sms * bps;
   const int64_t item_cap = k.item_rows > 0 ? std::max<int64_t>(T, int64_t(k.item_rows)) : (int64_t(1) << 20);
   std::vector<BatchSpan> spans;
   for (auto& g : groups) {
@@ -397,14 +466,17 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
     std::vector<int> order = g.members;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return qd[a].n > qd[b].n; });
     int64_t first = 0;
+    // work-item takers of the launch: CTAs, or clusters of g.cluster CTAs
+    const int takers = g.cluster > 1 ? std::max(1, g.grid / g.cluster) : ctx->sms * g.minb;
     for (int i : order) {
-      int64_t ir = (qd[i].n + grid_max - 1) / grid_max;
+      int64_t ir = (qd[i].n + takers - 1) / takers;
       // an item ends by merging its shared table into HBM (one insert per
-      // group it saw, up to S): items of at least 16 such merges' worth of
-      // rows keep that merge a small share of the item's L2 traffic
+      // group it saw, up to the table's slots): items of at least 16 such
+      // merges' worth of rows keep that merge a small share of the item's L2
+      // traffic
+      const double tslots = double(qi[i].S) * qi[i].cl;
       const int64_t merges =
-          qi[i].S > 0 ? int64_t(std::min<double>(qi[i].pred > 0 ? qi[i].pred : double(qi[i].S), double(qi[i].S)))
-                      : 0;
+          qi[i].S > 0 ? int64_t(std::min<double>(qi[i].pred > 0 ? qi[i].pred : tslots, tslots)) : 0;
       ir = std::max<int64_t>(ir, 16 * merges);
       ir = std::min(item_cap, std::max<int64_t>(T, (ir + T - 1) / T * T));
       const int64_t nit = (qd[i].n + ir - 1) / ir;
@@ -414,9 +486,17 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
     }
     g.nspans = int(int64_t(spans.size()) - g.item_begin);
     g.nitems = first;
-    g.grid = int(std::max<int64_t>(1, std::min<int64_t>(g.nitems, grid_max)));
+    if (g.cluster == 1) g.grid = int(std::max<int64_t>(1, std::min<int64_t>(g.nitems, int64_t(ctx->sms) * g.minb)));
   }
   const int ng = int(groups.size());
+  if (trace.on) {
+    for (const auto& g : groups) {
+      int64_t rows = 0;
+      for (int i : g.members) rows += qd[i].n;
+      std::fprintf(stderr, "gba_groupby_batch: launch sig=%d cluster=%d grid=%d smem=%zu queries=%zu rows=%lld items=%lld\n",
+                   g.sig / 32, g.cluster, g.grid, g.smem, g.members.size(), (long long)rows, (long long)g.nitems);
+    }
+  }
 
   // ---- device layout: descriptors | items | block prefixes | status | counters | tables ----
   size_t off = 0;
@@ -470,8 +550,12 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
       for (int c = 0; c < qd[i].ncols; ++c) vec = vec && aligned16(qd[i].cols[c]);
       // bits 8..15: buckets probed per row; a table the query's groups will
       // overfill keeps only what reaches its home bucket
-      const int nbk = (qi[i].S > 0 && qi[i].pred > 2.0 * qi[i].S) ? 1 : 0;
-      b.pad = (vec ? 1 : 0) | (nbk << 8);  // bit 0: columns allow vector loads
+      const int nbk = (qi[i].S > 0 && qi[i].pred > 2.0 * qi[i].S * qi[i].cl) ? 1 : 0;
+      // bit 1 (bulk-copy kernel): combine equal keys within a warp first, for
+      // queries whose sample shows a key taking at least 1/32 of the rows (one
+      // lane of a warp on average) or when the knob forces it
+      const bool comb = tma_kernel && k.coalesce != 0 && (k.coalesce == 1 || skew[i] >= 1.0 / 32.0);
+      b.pad = (vec ? 1 : 0) | (comb ? 2 : 0) | (nbk << 8);  // bit 0: columns allow vector loads
       hq[j] = b;
     }
     if (!spans.empty()) std::memcpy(h + o_items, spans.data(), sizeof(BatchSpan) * spans.size());
@@ -500,8 +584,13 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
       e = gba_launch_batch_init(d_qs, reinterpret_cast<const int64_t*>(d + o_ipre), nt, ipre[nt], cs);
     if (e == cudaSuccess) e = mark(1, cs);
     for (int g = 0; g < ng && e == cudaSuccess; ++g)
-      e = gba_launch_stream_agg(groups[g].proto, bps, d_qs, d_spans + groups[g].item_begin, groups[g].nspans,
-                                groups[g].nitems, d_ctr + g, groups[g].smem, sprobe, groups[g].grid, cs);
+      e = tma_kernel ? gba_launch_stream_tma(groups[g].proto, groups[g].cluster, groups[g].minb, d_qs,
+                                             d_spans + groups[g].item_begin, groups[g].nspans,
+                                             groups[g].nitems, d_ctr + g, groups[g].smem, sprobe, groups[g].grid,
+                                             nst, groups[g].stage_bytes, cs)
+                     : gba_launch_stream_agg(groups[g].proto, bps, d_qs, d_spans + groups[g].item_begin,
+                                             groups[g].nspans, groups[g].nitems, d_ctr + g, groups[g].smem, sprobe,
+                                             groups[g].grid, cs);
     if (e == cudaSuccess) e = mark(2, cs);
     if (e == cudaSuccess)
       e = gba_launch_batch_compact(d_qs, reinterpret_cast<const int64_t*>(d + o_cpre), nt, cpre[nt], cs);
@@ -512,7 +601,8 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   trace.mark("plan");
   if (nt > 0) {
     for (int g = 0; g < ng; ++g)
-      GBA_CUDA_TRY(ctx, gba_prepare_stream_agg(groups[g].proto, bps));
+      GBA_CUDA_TRY(ctx, tma_kernel ? gba_prepare_stream_tma(groups[g].proto, groups[g].cluster, groups[g].minb)
+                                   : gba_prepare_stream_agg(groups[g].proto, bps));
     if (as_graph) {
       // the graph depends only on launch shapes and buffer addresses
       std::vector<int64_t> key = {nt,
@@ -525,6 +615,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
                                   int64_t(reinterpret_cast<uintptr_t>(h)),
                                   sprobe,
                                   bps,
+                                  tma_kernel ? nst : 0,
                                   timing ? 1 : 0};
       for (const auto& g : groups) {
         key.push_back(g.sig);
@@ -533,6 +624,8 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
         key.push_back(g.nitems);
         key.push_back(g.nspans);
         key.push_back(g.grid);
+        key.push_back(int64_t(g.stage_bytes));
+        key.push_back(g.cluster * 8 + g.minb);
       }
       if (!ctx->batch_exec || key != ctx->batch_key) {
         if (ctx->batch_exec) {

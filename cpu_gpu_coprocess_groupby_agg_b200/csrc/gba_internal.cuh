@@ -319,3 +319,51 @@ inline cudaError_t gba_allow_max_smem(K* kernel) {
   return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - int(a.sharedSizeBytes));
 }
 
+
+// ---------------------------------------------------------------------------
+// Thread-block-cluster distributed shared memory (sm_90+): addresses in the
+// shared::cluster window, mapped from this CTA's shared address to the same
+// offset in CTA `rank` of the cluster.
+__device__ __forceinline__ unsigned cluster_ctarank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t dsmem_map(uint32_t local_addr, unsigned rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(local_addr), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void dsmem_ld_v4(uint32_t addr, unsigned& x0, unsigned& x1, unsigned& x2, unsigned& x3) {
+  asm volatile("ld.volatile.shared::cluster.v4.u32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(x0), "=r"(x1), "=r"(x2), "=r"(x3)
+               : "r"(addr));
+}
+__device__ __forceinline__ unsigned dsmem_atom_add_u32(uint32_t addr, unsigned v) {
+  unsigned old;
+  asm volatile("atom.shared::cluster.add.u32 %0, [%1], %2;" : "=r"(old) : "r"(addr), "r"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ void dsmem_red_add_u32(uint32_t addr, unsigned v) {
+  asm volatile("red.shared::cluster.add.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned dsmem_cas_b32(uint32_t addr, unsigned cmp, unsigned val) {
+  unsigned old;
+  asm volatile("atom.shared::cluster.cas.b32 %0, [%1], %2, %3;" : "=r"(old) : "r"(addr), "r"(cmp), "r"(val) : "memory");
+  return old;
+}
+__device__ __forceinline__ unsigned long long dsmem_cas_b64(uint32_t addr, unsigned long long cmp,
+                                                            unsigned long long val) {
+  unsigned long long old;
+  asm volatile("atom.shared::cluster.cas.b64 %0, [%1], %2, %3;" : "=l"(old) : "r"(addr), "l"(cmp), "l"(val) : "memory");
+  return old;
+}
+__device__ __forceinline__ void dsmem_st_u32(uint32_t addr, unsigned v) {
+  asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+// All threads of every CTA of the cluster: release this CTA's shared-memory
+// writes, wait for every other CTA's (a hardware barrier; it completes once
+// all threads of the cluster have arrived).
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\nbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}

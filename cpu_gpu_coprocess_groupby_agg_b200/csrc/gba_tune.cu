@@ -10,7 +10,9 @@
 //   one query (gba_groupby):   tile_rows (TMA tile length), blocks_per_sm,
 //                              partition_bits (around the automatic choice),
 //                              learned_load / load_factor (HBM table load)
-//   a batch (gba_groupby_batch): blocks_per_sm, learned_load / load_factor,
+//   a batch (gba_groupby_batch): use_tma (which streaming kernel),
+//                              blocks_per_sm, nstages, coalesce, table_slots
+//                              (GROW sizing), learned_load / load_factor,
 //                              item_rows, smem_probe_cap (buckets probed)
 // The outputs are written by every trial; the last trial leaves a complete,
 // correct result for the best knobs only if the caller reruns with them.
@@ -94,9 +96,25 @@ extern "C" gba_status gba_autotune(gba_context* ctx, int32_t nq, const gba_query
                       }});
     axes.push_back({"load", {nan, 0.25, 0.5, 0.7}, set_load});
   } else {
+    // the streaming kernel first (bulk-copy staging or register loads), then
+    // the knobs of each: CTAs per SM for the register-loading kernel, ring
+    // depth and warp combining of equal keys for the bulk-copy one
+    axes.push_back({"use_tma", {nan, 0}, [](gba_knobs& k, double v) {
+                      k.use_tma = std::isnan(v) ? -1 : int32_t(v);
+                    }});
     axes.push_back({"blocks_per_sm", {nan, 1, 2, 4}, [](gba_knobs& k, double v) {
                       k.blocks_per_sm = std::isnan(v) ? 0 : int32_t(v);
                     }});
+    axes.push_back({"nstages", {nan, 2, 4}, [](gba_knobs& k, double v) {
+                      k.nstages = std::isnan(v) ? 0 : int32_t(v);
+                    }});
+    axes.push_back({"coalesce", {nan, 0, 1}, [](gba_knobs& k, double v) {
+                      k.coalesce = std::isnan(v) ? -1 : int32_t(v);
+                    }});
+    if (best.sizing == GBA_SIZING_GROW)
+      axes.push_back({"table_slots", {nan, double(1 << 14), double(1 << 18)}, [](gba_knobs& k, double v) {
+                        k.table_slots = std::isnan(v) ? 0 : int64_t(v);
+                      }});
     axes.push_back({"load", {nan, 0.25, 0.5}, set_load});
     axes.push_back({"item_rows", {nan, double(1 << 17), double(1 << 19)}, [](gba_knobs& k, double v) {
                       k.item_rows = std::isnan(v) ? 0 : int32_t(v);

@@ -24,6 +24,7 @@
 #include "smem_table.cuh"
 
 namespace {
+#include "stream_rows.cuh"
 
 // rows per lane per chunk: fewer when a row carries many accumulators, and
 // half as many when two CTAs share an SM (MINB = 2: half the registers)
@@ -62,132 +63,6 @@ __device__ __forceinline__ void ld_vec8(const unsigned long long* p, unsigned lo
       o[2 * h + 1] = (unsigned long long)a.w << 32 | a.z;
     }
   }
-}
-
-// The shared table is probed by 16-byte buckets (4 32-bit or 2 64-bit keys):
-// one vector load compares a whole bucket.  Inside a bucket, slots fill in
-// order (a key is only ever claimed in the first empty slot of a complete
-// read of its bucket, and slots never empty during an item), so a key found
-// absent from a full read with an empty slot is absent from the bucket, and
-// it can live in one slot only.
-template <bool K64>
-struct BucketT {
-  static constexpr int SPB = K64 ? 2 : 4;  // slots per bucket
-  typedef typename SmemTable<K64>::KeyW KeyW;
-};
-
-template <bool K64>
-__device__ __forceinline__ void ld_bucket(const typename SmemTable<K64>::KeyW* keys, int b,
-                                          typename SmemTable<K64>::KeyW (&o)[BucketT<K64>::SPB]) {
-  unsigned x0, x1, x2, x3;
-  asm volatile("ld.volatile.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
-               : "=r"(x0), "=r"(x1), "=r"(x2), "=r"(x3)
-               : "r"(smem_u32(keys + b * BucketT<K64>::SPB)));
-  if constexpr (K64) {
-    o[0] = (unsigned long long)x1 << 32 | x0;
-    o[1] = (unsigned long long)x3 << 32 | x2;
-  } else {
-    o[0] = x0;
-    o[1] = x1;
-    o[2] = x2;
-    o[3] = x3;
-  }
-}
-
-template <bool K64>
-__device__ __forceinline__ int bucket_home(const SmemTable<K64>& t, uint32_t h) {
-  return int((uint64_t(h) * unsigned(t.S / BucketT<K64>::SPB)) >> 32);
-}
-
-// slot of `key` in the shared table, inserting it if absent; -1 when
-// `max_buckets` buckets from its home bucket are full without it
-// (out of line: it is the slow path, and inlining it for every row of the
-// unrolled chunk overflows the instruction cache)
-template <bool K64>
-__device__ __noinline__ int bucket_find_or_insert(const SmemTable<K64> t, uint64_t key, uint32_t h,
-                                                  int max_buckets) {
-  constexpr int SPB = BucketT<K64>::SPB;
-  typedef typename SmemTable<K64>::KeyW KeyW;
-  const KeyW kk = KeyW(key), empty = smem_empty_key<K64>();
-  const int nb = t.S / SPB;
-  int b = bucket_home<K64>(t, h);
-  for (int p = 0; p < max_buckets; ++p) {
-    for (int tries = 0; tries <= SPB; ++tries) {  // a lost claim means one more slot of the bucket is filled
-      KeyW k[SPB];
-      ld_bucket<K64>(t.keys, b, k);
-      int free_e = -1;
-#pragma unroll
-      for (int e = SPB - 1; e >= 0; --e) {
-        if (k[e] == kk) return b * SPB + e;
-        if (k[e] == empty) free_e = e;
-      }
-      if (free_e < 0) break;
-      const KeyW prev = atomicCAS(&t.keys[b * SPB + free_e], empty, kk);
-      if (prev == empty || prev == kk) return b * SPB + free_e;
-    }
-    b = b + 1 == nb ? 0 : b + 1;
-  }
-  return -1;
-}
-
-// Accumulator updates of up to R rows (bit i of `rows` set: row i goes to
-// shared slot slot[i]).  COUNT and the low word of an integer SUM are issued
-// for all rows before any returned value is used; the SUM's carry into its
-// high word follows.  Other ops take the generic per-row path.
-template <bool K64, typename Sig, int R>
-__device__ __forceinline__ void smem_apply_rows(const SmemTable<K64>& t, const QDesc& q, const int (&slot)[R],
-                                                const unsigned long long (&v)[R][Sig::NA], unsigned rows) {
-#pragma unroll
-  for (int a = 0; a < Sig::NA; ++a) {
-    const int op = Sig::op(q, a);
-    const int w = Sig::woff(q, a);
-    // split word: low halves at lo32[slot], high halves at lo32[S + slot]
-    unsigned* lo32 = reinterpret_cast<unsigned*>(t.acc + size_t(w) * t.S);
-    if (op == ACC_CNT) {
-#pragma unroll
-      for (int i = 0; i < R; ++i)
-        if (rows >> i & 1u) atomicAdd(lo32 + slot[i], unsigned(v[i][a]));
-    } else if (op == ACC_ADD_I) {
-      unsigned old[R];
-#pragma unroll
-      for (int i = 0; i < R; ++i) {
-        old[i] = 0u;
-        if (rows >> i & 1u) old[i] = atomicAdd(lo32 + slot[i], unsigned(v[i][a]));
-      }
-#pragma unroll
-      for (int i = 0; i < R; ++i) {
-        if (!(rows >> i & 1u)) continue;
-        const unsigned lo = unsigned(v[i][a]), hi = unsigned(v[i][a] >> 32);
-        const unsigned add_hi = hi + ((old[i] + lo) < old[i] ? 1u : 0u);
-        if (add_hi) atomicAdd(lo32 + t.S + slot[i], add_hi);
-      }
-    } else {
-#pragma unroll
-      for (int i = 0; i < R; ++i) {
-        if (!(rows >> i & 1u)) continue;
-        if (op == ACC_ADD_F)
-          smem_fsum(smem_ref<K64>(t, w, slot[i]), smem_ref<K64>(t, w + 1, slot[i]), smem_ref<K64>(t, w + 2, slot[i]),
-                    __longlong_as_double(v[i][a]));
-        else smem_acc(op, smem_ref<K64>(t, w, slot[i]), v[i][a]);
-      }
-    }
-  }
-}
-
-// A row's accumulator contributions, passed by value to the out-of-line slow
-// path: a reference to one row of the caller's v[R][NA] would take the array's
-// address and move all of it to local memory for the whole chunk.
-template <int NA>
-struct AccVals {
-  unsigned long long x[NA];
-};
-
-// HBM-table insert that did not find its key in the home slot (first
-// occurrence, or a displaced key): out of line, like bucket_find_or_insert.
-template <bool K64, typename Sig>
-__device__ __noinline__ void gtable_insert_slow(const GTable gt, const QDesc& q, uint64_t key, uint64_t home,
-                                                unsigned long long cur, const AccVals<Sig::NA> v, unsigned* flags) {
-  gtable_finish<K64, Sig>(gt, q, key, home, cur, v.x, flags);
 }
 
 template <bool K64, typename Sig, int R>
@@ -255,83 +130,8 @@ __device__ __forceinline__ void stream_chunk(const BatchQ& bq, const SmemTable<K
 #pragma unroll
     for (int i = 0; i < R; ++i) row_contrib<Sig>(q, raw[i], v[i]);
   }
-
-  // shared-table pass, phase by phase over the lane's R rows so that their
-  // shared-memory round trips overlap: first every row's home-slot key, then
-  // the rows that did not find their key there walk the probe sequence, then
-  // the accumulator updates of all rows are issued before any result is used
-  unsigned miss = 0;
-  uint32_t h[R];
-#pragma unroll
-  for (int i = 0; i < R; ++i) h[i] = table_hash(key[i]);
-  if (bq.S > 0) {
-    typedef typename SmemTable<K64>::KeyW KeyW;
-    constexpr int SPB = BucketT<K64>::SPB;
-    int slot[R];
-    KeyW kb[R][SPB];
-#pragma unroll
-    for (int i = 0; i < R; ++i) ld_bucket<K64>(st.keys, bucket_home<K64>(st, h[i]), kb[i]);
-    unsigned hit = 0;
-#pragma unroll
-    for (int i = 0; i < R; ++i) {
-      slot[i] = -1;
-      if (!live[i]) continue;
-      if (key[i] == emptyk) {  // the all-ones key has its own slot
-        smem_apply_side<K64, Sig>(st, q, v[i]);
-        continue;
-      }
-      bool has_empty = false;
-#pragma unroll
-      for (int e = 0; e < SPB; ++e) {
-        if (kb[i][e] == KeyW(key[i])) slot[i] = bucket_home<K64>(st, h[i]) * SPB + e;
-        has_empty = has_empty || kb[i][e] == smem_empty_key<K64>();
-      }
-      // a home bucket read full without the key settles a one-bucket probe
-      if (slot[i] < 0 && (has_empty || nbk > 1)) slot[i] = bucket_find_or_insert<K64>(st, key[i], h[i], nbk);
-      if (slot[i] >= 0) hit |= 1u << i;
-      else miss |= 1u << i;
-    }
-    smem_apply_rows<K64, Sig, R>(st, q, slot, v, hit);
-  } else {
-#pragma unroll
-    for (int i = 0; i < R; ++i) {
-      if (!live[i]) continue;
-      if (key[i] == emptyk) gtable_insert<K64, Sig>(bq.gt, q, key[i], 0u, v[i], bq.flags);
-      else miss |= 1u << i;
-    }
-  }
-  if (miss == 0) return;
-  // HBM-table pass: every missed row's home-slot load first, then the inserts
-  // (measured: also loading the slot after the home slot, to place displaced
-  // keys without a second round trip, costs more in L2 requests than it saves)
-  constexpr int stride = 1 + NA;
-  uint64_t home[R];
-  unsigned long long cur[R];
-#pragma unroll
-  for (int i = 0; i < R; ++i) {
-    home[i] = 0;
-    cur[i] = 0;
-    if (miss >> i & 1u) {
-      home[i] = gtable_home(bq.gt, h[i]);
-      cur[i] = __ldcg(bq.gt.base + home[i] * stride);
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < R; ++i) {
-    if (!(miss >> i & 1u)) continue;
-    if (cur[i] == key[i]) {  // the key sits in its home slot: reductions only
-      unsigned long long* sp = bq.gt.base + home[i] * stride;
-#pragma unroll
-      for (int a = 0; a < NA; ++a) global_acc(Sig::op(q, a), sp + 1 + a, v[i][a]);
-    } else {
-      AccVals<NA> vv;
-#pragma unroll
-      for (int a = 0; a < NA; ++a) vv.x[a] = v[i][a];
-      gtable_insert_slow<K64, Sig>(bq.gt, q, key[i], home[i], cur[i], vv, bq.flags);
-    }
-  }
+  stream_rows<K64, Sig, R>(bq, st, nbk, key, v, live);
 }
-
 // Persistent streaming aggregation over a work queue of items given as query
 // spans (see BatchSpan).
 // sprobe: buckets probed before a row goes to the HBM table (BatchQ.pad bits

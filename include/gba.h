@@ -107,7 +107,9 @@ typedef struct gba_output {
 typedef enum gba_sizing {
   GBA_SIZING_PLAIN = 0,   /* fixed load factor on the row count, overflow -> regrow */
   GBA_SIZING_LEARNED = 1, /* MLP cardinality estimate, overflow -> regrow */
-  GBA_SIZING_FIXED = 2    /* table_slots as given, overflow -> regrow */
+  GBA_SIZING_FIXED = 2,   /* table_slots as given, overflow -> regrow */
+  GBA_SIZING_GROW = 3     /* estimator-free: the plain capacity, but at most table_slots (default 2^16)
+                             to start with; a query whose table overflows reruns with 4x the slots */
 } gba_sizing;
 
 typedef enum gba_strategy {
@@ -144,6 +146,10 @@ typedef struct gba_knobs {
                              order (signed for I32/I64 keys, unsigned for U32), sorted on the device;
                              0 (default) = hash-table order.  No reference counterpart: its partitions
                              hold their groups in table order (groupby_agg_intra_partition.cu:245-276). */
+  int32_t cluster_ctas;   /* batch, learned sizing: the most CTAs of a thread-block cluster whose shared
+                             tables together hold one query's table (distributed shared memory), for
+                             queries whose predicted groups outgrow one CTA's table (0 = auto: 8; 1 = off;
+                             2, 4, 8 or 16) */
 } gba_knobs;
 
 /* What the last call on a context did. */

@@ -75,7 +75,11 @@ def test_batch_graph_replay_and_direct_launch_agree(ctx):
 
 
 @pytest.mark.parametrize("knobs", [dict(tile_rows=2048), dict(blocks_per_sm=2), dict(item_rows=4096),
-                                   dict(smem_slots=128), dict(preagg=0), dict(smem_probe_cap=1)])
+                                   dict(smem_slots=128), dict(preagg=0), dict(smem_probe_cap=1),
+                                   dict(use_tma=0), dict(use_tma=0, blocks_per_sm=4), dict(nstages=1),
+                                   dict(nstages=2), dict(nstages=4), dict(coalesce=1), dict(coalesce=0),
+                                   dict(coalesce=1, smem_slots=64), dict(sizing="grow"),
+                                   dict(sizing="grow", table_slots=256)])
 def test_batch_knobs_do_not_change_results(ctx, knobs):
     qs = _queries(12, seed=7)
     _check(qs, ctx.groupby_batch(_device(qs), knobs=knobs), str(knobs))
@@ -110,3 +114,48 @@ def test_batch_empty_and_capacity_error(ctx):
     with pytest.raises(A.GbaError) as e:
         ctx.groupby_batch(dq, outs=outs)
     assert e.value.status == A.ERR_OUTPUT_CAPACITY
+
+
+def test_batch_bulk_copy_kernel_ragged_and_unaligned(ctx):
+    """The bulk-copy kernel's edges: queries whose row count is not a multiple
+    of 4 (tail rows read from global memory), fewer rows than one stage, one
+    row, and columns that start off a 16-byte boundary (no bulk copies)."""
+    import torch
+    qs = []
+    for i, n in enumerate([1, 3, 5, 2047, 2049, 4099, 70_001, 131_075]):
+        keys, cols = _data(n, [np.int32, np.int64][i % 2], max(1, n // 7), seed=300 + i, zipf=1.2)
+        qs.append((keys, cols, [("sum", 0), ("count", None), ("min", 0)]))
+    dq = _device(qs)
+    # a query whose key and value columns start off a 16-byte boundary: 4 and
+    # 8 bytes into their buffers
+    keys, cols = _data(50_001, np.int32, 3000, seed=333)
+    cols = cols[:1]
+    kb = torch.zeros(50_002, dtype=torch.int32, device="cuda")
+    kb[1:] = torch.from_numpy(keys).cuda()
+    vb = torch.zeros(50_002, dtype=torch.int64, device="cuda")
+    vb[1:] = torch.from_numpy(cols[0]).cuda()
+    qs.append((keys, cols, [("sum", 0), ("count", None), ("min", 0)]))
+    dq.append((kb[1:], [vb[1:]], qs[-1][2], False, [False]))
+    for knobs in (dict(), dict(coalesce=1), dict(nstages=1)):
+        _check(qs, ctx.groupby_batch(dq, knobs=knobs), f"ragged {knobs}")
+
+
+@pytest.mark.parametrize("cluster", [2, 4, 8, 16])
+def test_batch_cluster_tables_match_oracle(ctx, cluster):
+    """Queries whose predicted groups outgrow one CTA's shared table but fit a
+    cluster's (learned sizing, integer SUM/COUNT): their shared table is spread
+    over the CTAs of a thread-block cluster (distributed shared memory)."""
+    assert E.load_default(ctx), "committed estimator weights are missing"
+    specs = [(400_000, np.int64, 12_000, 0.0), (600_000, np.int32, 30_000, 0.3), (300_000, np.uint32, 60_000, 0.0),
+             (900_000, np.int64, 100_000, 0.8), (250_000, np.int32, 8_000, 1.1), (50_000, np.int64, 200, 0.5)]
+    aggsets = [[("sum", 0), ("count", None)], [("count", None)], [("sum", 0), ("sum", 2), ("count", None)],
+               [("sum", 3), ("count", None)], [("sum", 0), ("count", None)], [("sum", 0), ("count", None)]]
+    qs = []
+    for i, ((n, kdt, ndv, z), aggs) in enumerate(zip(specs, aggsets)):
+        keys, cols = _data(n, kdt, ndv, seed=700 + i, zipf=z)
+        qs.append((keys, cols, aggs))
+    res = ctx.groupby_batch(_device(qs), knobs=dict(sizing="learned", cluster_ctas=cluster))
+    _check(qs, res, f"cluster {cluster}")
+    # the same with the graph replayed and with warp combining forced
+    res = ctx.groupby_batch(_device(qs), knobs=dict(sizing="learned", cluster_ctas=cluster, coalesce=1))
+    _check(qs, res, f"cluster {cluster} combined")
