@@ -113,10 +113,20 @@ def dist_setup():
     return ws, rank, local
 
 
-def get_workload(name: str):
+def get_workload(name: str, rows: int = 0):
+    """A single-query workload; rows > 0 takes that many rows of the same
+    shape (distinct ids of the high-cardinality workload scale alike), for
+    profiling captures that must stay small."""
+    import dataclasses
     from cpu_gpu_coprocess_groupby_agg_b200 import workloads as W
-    return {"skewed": W.skewed, "small": W.small, "highcard": W.high_card,
-            "large": lambda: W.large_serving_query(seed=900)}[name]()
+    w = {"skewed": W.skewed, "small": W.small, "highcard": W.high_card,
+         "large": lambda: W.large_serving_query(seed=900)}[name]()
+    if rows > 0 and rows != w.n:
+        if name == "highcard":
+            w = W.high_card(n=rows, ndv=max(1, rows // 4))
+        else:
+            w = dataclasses.replace(w, n=rows, name=f"{w.name}[rows {rows}]")
+    return w
 
 
 BATCH_NAME = "batch_256q_rows2^12-2^24_logu_ndv16-rows/2_zipf0-1.5_sum+count"
@@ -183,7 +193,7 @@ def run_reference(args, ws, rank):
         single = (len(sample), m1)
         same = True
     else:
-        w = get_workload(args.workload)
+        w = get_workload(args.workload, args.rows)
         m = cpu_sample_rows(w)
         keys, cols = O.gen(w.spec, m, nthreads=cores)
         name, total_rows, aggs = w.name, w.n, w.aggs
@@ -241,6 +251,7 @@ def main():
     ap.add_argument("--knob", action="append", default=[], help="name=value knob override")
     ap.add_argument("--no-autotune", action="store_true", help="batch: default knobs instead of gba_autotune's")
     ap.add_argument("--ndv-range", default="", help="batch: only queries with LO <= distinct ids < HI ('LO:HI')")
+    ap.add_argument("--rows", type=int, default=0, help="single query: rows of a smaller case of the same shape")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     ws, rank, local = dist_setup()
@@ -265,7 +276,7 @@ def main():
         return run_batch(args, ws, rank, local, pg)
     if args.workload == "serve":
         return run_serve(args, ws, rank, local, pg)
-    w = get_workload(args.workload)
+    w = get_workload(args.workload, args.rows)
     ctx = Context(local)
     if args.sizing == "learned" and not E.load_default(ctx):
         raise SystemExit(f"learned sizing needs trained weights at {E.WEIGHTS}")

@@ -64,6 +64,7 @@ struct QInfo {
   int strategy = GBA_STRATEGY_TABLE;
   int S = 0;         // shared-table slots in the batch kernel (per CTA)
   int cl = 1;        // CTAs of the cluster whose tables form the query's shared table
+  bool tma = false;  // streamed by the bulk-copy kernel (else the register-loading one)
   int slot = -1;     // index among the table-strategy queries
 };
 
@@ -75,6 +76,7 @@ struct Group {
   size_t stage_bytes = 0;    // bulk-copy kernel: bytes of one ring slot
   int cluster = 1;           // bulk-copy kernel: CTAs per cluster
   int minb = 1;              // CTAs per SM of the launch
+  bool tma = false;          // bulk-copy kernel (k_stream_tma) or register-loading one (k_stream_agg)
   int64_t item_begin = 0, nitems = 0;  // item_begin: index of the group's first span
   int nspans = 0;
   int grid = 0;
@@ -337,14 +339,21 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   // the 256-query batch, the kernel takes 16.4 ms at 1, 11.1-12.3 ms at 2 and
   // 10.3 ms at 4 (where registers spill); 3 (40 registers, few spills) is 1-2%
   // faster than 4 and is what the autotuner picks there.
-  // The streaming kernel: by default the bulk-copy one (k_stream_tma: 1 or 2
+  // Two streaming kernels: the register-loading one (k_stream_agg, bps CTAs
+  // per SM, automatic 3) and the bulk-copy one (k_stream_tma: tbps = 1 or 2
   // CTAs per SM, automatic 2, each warp staging its rows through a ring of
-  // `nst` slots); knobs.use_tma = 0 selects the register-loading one
-  // (k_stream_agg, 1 to 4 CTAs per SM).
-  const bool tma_kernel = k.use_tma != 0;
+  // `nst` slots).  knobs.use_tma = 0 / 1 sends every query to one of them;
+  // automatic (-1): a query whose predicted groups outgrow half the
+  // register-loading kernel's shared table goes to the bulk-copy kernel, the
+  // rest (and every query under plain sizing) to the register-loading one.
+  // Measured per cardinality class of the 256-query batch (kernel ms,
+  // register-loading vs bulk-copy): ids < 256: 0.69 vs 0.89; 256-4096: 1.47 vs
+  // 1.53; 4096-16384: 1.60 vs 1.40; 16384-65536: 2.60 vs 2.36; 65536-262144:
+  // 1.32 vs 1.04; 262144-2^20: 2.35 vs 2.25; above 2^20: 2.94 vs 2.65.
   const int nst = k.nstages >= 1 && k.nstages <= 4 ? k.nstages : 3;
-  const int bps = tma_kernel ? (k.blocks_per_sm == 1 ? 1 : 2)
-                             : (k.blocks_per_sm >= 1 && k.blocks_per_sm <= 4 ? k.blocks_per_sm : 3);
+  const int bps = k.blocks_per_sm >= 1 && k.blocks_per_sm <= 4 ? k.blocks_per_sm : 3;
+  const int tbps = k.blocks_per_sm == 1 ? 1 : 2;
+  bool any_tma = false;
   // buckets probed in a shared table before a row goes to the HBM table
   const int sprobe = k.smem_probe_cap > 0 ? k.smem_probe_cap : 2;
   // Strategy: a query alone leaves the HBM-table strategy once its table
@@ -373,17 +382,29 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
                                                      : gba_choose_strategy(ctx, qd[i], k, pred[i], qi[i].p);
   }
 
+  // ---- streaming kernel of each query ----
+  for (int i = 0; i < nq; ++i) {
+    if (qi[i].strategy != GBA_STRATEGY_TABLE) continue;
+    if (k.use_tma == 0) qi[i].tma = false;
+    else if (k.use_tma == 1) qi[i].tma = true;
+    else qi[i].tma = qi[i].pred > 0 && qi[i].p.preagg && qi[i].pred > 0.5 * batch_smem_slots(ctx, qd[i], bps);
+    any_tma = any_tma || qi[i].tma;
+  }
+
   // ---- cluster tables ----
-  // A query whose predicted groups outgrow one CTA's shared table (more than
-  // half its slots) but fit the tables of a cluster of 2-16 CTAs at load 0.7
-  // gets such a cluster (the smallest that fits): its rows then meet a
-  // shared-memory table spread over the cluster instead of the HBM table.
-  // Learned sizing only (the group count is needed); integer SUM/COUNT
-  // signatures only.
-  const int maxcl = k.cluster_ctas == 1 ? 1 : (k.cluster_ctas >= 2 && k.cluster_ctas <= 16 ? k.cluster_ctas : 8);
-  for (int i = 0; i < nq && tma_kernel && maxcl > 1; ++i) {
-    if (qi[i].strategy != GBA_STRATEGY_TABLE || !qi[i].p.preagg || qi[i].pred <= 0 || k.smem_slots > 0 ||
-        !gba_stream_tma_cluster_ok(qd[i]))
+  // With knobs.cluster_ctas = c (2, 4, 8 or 16), a bulk-copy query whose
+  // predicted groups outgrow one CTA's shared table (more than half its slots)
+  // but fit the tables of a cluster of up to c CTAs at load 0.7 gets such a
+  // cluster (the smallest that fits): its rows then meet a shared-memory
+  // table spread over the cluster instead of the HBM table.  Learned sizing
+  // only (the group count is needed); integer SUM/COUNT signatures only.  Off
+  // by default: measured on the batch, the remote shared-memory atomics cost
+  // more than the L2 traffic they save (4096-16384 ids: 1.58 ms without
+  // clusters, 2.07 with 2 CTAs, 3.18 with 16).
+  const int maxcl = k.cluster_ctas >= 2 && k.cluster_ctas <= 16 ? k.cluster_ctas : 1;
+  for (int i = 0; i < nq && maxcl > 1; ++i) {
+    if (qi[i].strategy != GBA_STRATEGY_TABLE || !qi[i].tma || !qi[i].p.preagg || qi[i].pred <= 0 ||
+        k.smem_slots > 0 || !gba_stream_tma_cluster_ok(qd[i]))
       continue;
     const double S1 = tma_smem_slots(ctx, qd[i], 1, nst, gba_stream_tma_slot_bytes(qd[i], 1));
     if (S1 <= 0 || qi[i].pred <= 0.5 * S1) continue;
@@ -399,20 +420,21 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   std::vector<int> tq;  // table-strategy queries, group by group
   for (int i = 0; i < nq; ++i) {
     if (qi[i].strategy != GBA_STRATEGY_TABLE) continue;
-    // one launch per signature, key width and cluster size
-    const int sig = (2 * gba_batch_sig_id(qd[i]) + (qd[i].key64 ? 1 : 0)) * 32 + qi[i].cl;
+    // one launch per signature, key width, kernel and cluster size
+    const int sig = ((2 * gba_batch_sig_id(qd[i]) + (qd[i].key64 ? 1 : 0)) * 2 + (qi[i].tma ? 1 : 0)) * 32 + qi[i].cl;
     auto it = std::find_if(groups.begin(), groups.end(), [&](const Group& g) { return g.sig == sig; });
     if (it == groups.end()) {
       groups.push_back(Group{sig, qd[i], {}});
       groups.back().cluster = qi[i].cl;
+      groups.back().tma = qi[i].tma;
       it = groups.end() - 1;
     }
     it->members.push_back(i);
   }
   for (auto& g : groups) {
     g.smem = gba_stream_smem_bytes(g.proto, 0);
-    g.minb = g.cluster > 1 ? 1 : bps;
-    if (tma_kernel) {
+    g.minb = !g.tma ? bps : (g.cluster > 1 ? 1 : tbps);
+    if (g.tma) {
       // one ring slot holds a chunk of any member (run-time signatures may
       // differ in columns per member)
       for (int i : g.members) g.stage_bytes = std::max(g.stage_bytes, gba_stream_tma_slot_bytes(qd[i], g.minb));
@@ -421,7 +443,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
     for (int i : g.members) {
       // run-time signatures may differ in accumulator words per member
       int S = !qi[i].p.preagg ? 0
-              : tma_kernel    ? tma_smem_slots(ctx, qd[i], g.minb, nst, g.stage_bytes)
+              : g.tma         ? tma_smem_slots(ctx, qd[i], g.minb, nst, g.stage_bytes)
                               : batch_smem_slots(ctx, qd[i], bps);
       if (k.smem_slots > 0) S = std::min(S, k.smem_slots);
       // a known-small group count needs only a small shared table (cheaper
@@ -430,7 +452,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
       if (S > 0 && qi[i].pred > 0) S = std::min<int64_t>(S, std::max<int64_t>(256, int64_t(qi[i].pred * 4.0 + 31) / 32 * 32));
       S = S / 4 * 4;  // whole 16-byte buckets
       qi[i].S = S;
-      g.smem = std::max(g.smem, tma_kernel ? gba_stream_tma_smem_bytes(qd[i], S, nst, g.stage_bytes)
+      g.smem = std::max(g.smem, g.tma ? gba_stream_tma_smem_bytes(qd[i], S, nst, g.stage_bytes)
                                            : gba_stream_smem_bytes(qd[i], S));
       qi[i].slot = int(tq.size());
       tq.push_back(i);
@@ -554,7 +576,9 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
       // bit 1 (bulk-copy kernel): combine equal keys within a warp first, for
       // queries whose sample shows a key taking at least 1/32 of the rows (one
       // lane of a warp on average) or when the knob forces it
-      const bool comb = tma_kernel && k.coalesce != 0 && (k.coalesce == 1 || skew[i] >= 1.0 / 32.0);
+      // (measured on the batch's queries of fewer than 256 ids: combining made
+      // the kernel slower, 1.37 against 0.89 ms, so it is opt-in)
+      const bool comb = qi[i].tma && k.coalesce == 1;
       b.pad = (vec ? 1 : 0) | (comb ? 2 : 0) | (nbk << 8);  // bit 0: columns allow vector loads
       hq[j] = b;
     }
@@ -584,7 +608,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
       e = gba_launch_batch_init(d_qs, reinterpret_cast<const int64_t*>(d + o_ipre), nt, ipre[nt], cs);
     if (e == cudaSuccess) e = mark(1, cs);
     for (int g = 0; g < ng && e == cudaSuccess; ++g)
-      e = tma_kernel ? gba_launch_stream_tma(groups[g].proto, groups[g].cluster, groups[g].minb, d_qs,
+      e = groups[g].tma ? gba_launch_stream_tma(groups[g].proto, groups[g].cluster, groups[g].minb, d_qs,
                                              d_spans + groups[g].item_begin, groups[g].nspans,
                                              groups[g].nitems, d_ctr + g, groups[g].smem, sprobe, groups[g].grid,
                                              nst, groups[g].stage_bytes, cs)
@@ -601,7 +625,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   trace.mark("plan");
   if (nt > 0) {
     for (int g = 0; g < ng; ++g)
-      GBA_CUDA_TRY(ctx, tma_kernel ? gba_prepare_stream_tma(groups[g].proto, groups[g].cluster, groups[g].minb)
+      GBA_CUDA_TRY(ctx, groups[g].tma ? gba_prepare_stream_tma(groups[g].proto, groups[g].cluster, groups[g].minb)
                                    : gba_prepare_stream_agg(groups[g].proto, bps));
     if (as_graph) {
       // the graph depends only on launch shapes and buffer addresses
@@ -615,7 +639,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
                                   int64_t(reinterpret_cast<uintptr_t>(h)),
                                   sprobe,
                                   bps,
-                                  tma_kernel ? nst : 0,
+                                  any_tma ? nst : 0,
                                   timing ? 1 : 0};
       for (const auto& g : groups) {
         key.push_back(g.sig);
@@ -625,7 +649,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
         key.push_back(g.nspans);
         key.push_back(g.grid);
         key.push_back(int64_t(g.stage_bytes));
-        key.push_back(g.cluster * 8 + g.minb);
+        key.push_back(g.cluster * 16 + g.minb * 2 + (g.tma ? 1 : 0));
       }
       if (!ctx->batch_exec || key != ctx->batch_key) {
         if (ctx->batch_exec) {

@@ -99,7 +99,7 @@ extern "C" gba_status gba_autotune(gba_context* ctx, int32_t nq, const gba_query
     // the streaming kernel first (bulk-copy staging or register loads), then
     // the knobs of each: CTAs per SM for the register-loading kernel, ring
     // depth and warp combining of equal keys for the bulk-copy one
-    axes.push_back({"use_tma", {nan, 0}, [](gba_knobs& k, double v) {
+    axes.push_back({"use_tma", {nan, 0, 1}, [](gba_knobs& k, double v) {
                       k.use_tma = std::isnan(v) ? -1 : int32_t(v);
                     }});
     axes.push_back({"blocks_per_sm", {nan, 1, 2, 4}, [](gba_knobs& k, double v) {
@@ -108,7 +108,7 @@ extern "C" gba_status gba_autotune(gba_context* ctx, int32_t nq, const gba_query
     axes.push_back({"nstages", {nan, 2, 4}, [](gba_knobs& k, double v) {
                       k.nstages = std::isnan(v) ? 0 : int32_t(v);
                     }});
-    axes.push_back({"coalesce", {nan, 0, 1}, [](gba_knobs& k, double v) {
+    axes.push_back({"coalesce", {nan, 1}, [](gba_knobs& k, double v) {
                       k.coalesce = std::isnan(v) ? -1 : int32_t(v);
                     }});
     if (best.sizing == GBA_SIZING_GROW)

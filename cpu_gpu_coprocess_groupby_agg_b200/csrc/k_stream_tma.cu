@@ -46,10 +46,13 @@ constexpr int kTmaMaxStages = 4;
 constexpr int kTmaWarps = kTmaThreads / 32;
 
 // rows per lane per chunk: fewer with more accumulators, and fewer when
-// several CTAs share an SM (their registers are split)
+// several CTAs share an SM (their registers and shared memory are split).
+// With 16-byte rows a slot holds 2 KB (one CTA per SM) or 1 KB (two), so
+// three slots per warp keep about 64 KB of copies in flight per SM and leave
+// the rest of the shared memory to the tables.
 template <typename Sig, int MINB>
 __host__ __device__ constexpr int tma_rows_per_lane() {
-  return MINB == 1 ? (Sig::NA <= 2 ? 8 : (Sig::NA <= 4 ? 4 : 2)) : (Sig::NA <= 2 ? 4 : (Sig::NA <= 4 ? 2 : 1));
+  return MINB == 1 ? (Sig::NA <= 2 ? 4 : (Sig::NA <= 4 ? 2 : 1)) : (Sig::NA <= 2 ? 2 : 1);
 }
 
 __host__ __device__ inline int col_bytes_of(int t) { return (t == GBA_I64 || t == GBA_F64) ? 8 : 4; }

@@ -127,12 +127,16 @@ typedef struct gba_knobs {
   int32_t preagg;         /* -1 auto, 0 off, 1 on */
   int32_t smem_slots;     /* shared-memory table slots per CTA */
   int32_t partition_bits; /* radix fan-out 2^bits */
-  int32_t blocks_per_sm;  /* single query: CTAs per SM of the pre-aggregation grid; batch: 1, 2, 3 or 4 (0 = 3) */
+  int32_t blocks_per_sm;  /* single query: CTAs per SM of the pre-aggregation grid; batch: 1, 2, 3 or 4 (0 = 3)
+                             for the register-loading kernel, 1 or 2 (0 = 2) for the bulk-copy one */
   int32_t block_threads;
   int32_t tile_rows;
   int32_t nstages;        /* TMA pipeline depth */
-  int32_t use_tma;        /* -1 auto, 0 off, 1 on */
-  int32_t coalesce;       /* -1 auto, 0 off, 1 on: __match_any_sync pre-combining */
+  int32_t use_tma;        /* -1 auto, 0 off, 1 on.  Single query: the TMA tile loader of the table
+                             strategy.  Batch: which streaming kernel (1: the bulk-copy one, whose warps
+                             stage rows with cp.async.bulk; 0: the register-loading one; auto: bulk copy
+                             for queries whose predicted groups outgrow the other's shared table) */
+  int32_t coalesce;       /* -1 auto, 0 off, 1 on: __match_any_sync pre-combining (batch: opt-in) */
   int32_t probe_cap;      /* HBM table probe cap (0 = auto) */
   int32_t smem_probe_cap; /* shared table probe cap (0 = auto) */
   int32_t max_regrow;     /* regrow attempts before GBA_ERR_TABLE_OVERFLOW */
@@ -146,10 +150,10 @@ typedef struct gba_knobs {
                              order (signed for I32/I64 keys, unsigned for U32), sorted on the device;
                              0 (default) = hash-table order.  No reference counterpart: its partitions
                              hold their groups in table order (groupby_agg_intra_partition.cu:245-276). */
-  int32_t cluster_ctas;   /* batch, learned sizing: the most CTAs of a thread-block cluster whose shared
-                             tables together hold one query's table (distributed shared memory), for
-                             queries whose predicted groups outgrow one CTA's table (0 = auto: 8; 1 = off;
-                             2, 4, 8 or 16) */
+  int32_t cluster_ctas;   /* batch, learned sizing, bulk-copy kernel: the most CTAs of a thread-block
+                             cluster whose shared tables together hold one query's table (distributed
+                             shared memory), for queries whose predicted groups outgrow one CTA's table
+                             (0 or 1 = off, the default; 2, 4, 8 or 16) */
 } gba_knobs;
 
 /* What the last call on a context did. */
