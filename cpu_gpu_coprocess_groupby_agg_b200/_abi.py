@@ -82,6 +82,7 @@ class Knobs(C.Structure):
         ("learned_min_rows", C.c_int64),
         ("sort_output", C.c_int32),
         ("cluster_ctas", C.c_int32),
+        ("exchange", C.c_int32),
     ]
 
 

@@ -60,3 +60,16 @@ cudaError_t gba_prepare_stream_tma(const QDesc& proto, int cluster, int minb);
 cudaError_t gba_launch_stream_tma(const QDesc& proto, int cluster, int minb, const BatchQ* d_qs,
                                   const BatchSpan* d_spans, int nspans, int64_t nitems, unsigned* item_ctr,
                                   size_t smem, int sprobe, int grid, int nstages, size_t slot_bytes, cudaStream_t s);
+// Owner-exchange aggregation (k_exchange.cu): one cooperative launch of `grid`
+// CTAs (one per SM) over the nxq queries d_xq (indices into d_qs), each with
+// a shared table of BatchQ.S slots per CTA.  Rows move in windows of `win`
+// rows through two exchange buffers xbuf of 2 x grid x region records of
+// (1 + ncols) 8-byte words (region >= win); cursors (2 x grid), bar (2) and
+// *bar_flags must be zero at launch.
+size_t gba_exchange_smem_bytes(const QDesc& q, int S);
+size_t gba_exchange_static_smem();
+cudaError_t gba_prepare_exchange(const QDesc& proto);
+int gba_exchange_grid(const QDesc& proto, size_t smem, int sms);
+cudaError_t gba_launch_exchange(const QDesc& proto, const BatchQ* d_qs, const int* d_xq, int nxq, int64_t win,
+                                unsigned long long* xbuf, int64_t region, unsigned* cursors, unsigned* bar,
+                                unsigned* bar_flags, size_t smem, int sprobe, int grid, cudaStream_t s);

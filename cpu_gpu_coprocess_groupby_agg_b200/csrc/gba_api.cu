@@ -34,6 +34,7 @@ extern "C" void gba_default_knobs(gba_knobs* k) {
   k->coalesce = -1;
   k->max_regrow = 4;
   k->use_graph = -1;
+  k->exchange = 0;  // owner exchange: opt-in until measured
 }
 
 extern "C" const char* gba_status_string(gba_status s) {

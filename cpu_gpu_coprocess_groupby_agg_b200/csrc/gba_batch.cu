@@ -65,6 +65,7 @@ struct QInfo {
   int S = 0;         // shared-table slots in the batch kernel (per CTA)
   int cl = 1;        // CTAs of the cluster whose tables form the query's shared table
   bool tma = false;  // streamed by the bulk-copy kernel (else the register-loading one)
+  bool xch = false;  // aggregated by the owner-exchange kernel
   int slot = -1;     // index among the table-strategy queries
 };
 
@@ -141,6 +142,24 @@ int tma_smem_slots(const gba_context* ctx, const QDesc& q, int minb, int nst, si
   const int S = int(std::min<size_t>(16384, (budget - fixed) / slot));
   return S < 32 ? 0 : S;
 }
+
+// Shared-table slots per CTA of the owner-exchange kernel (one CTA per SM;
+// the table is the CTA's whole dynamic shared memory).
+int exchange_smem_slots(const gba_context* ctx, const QDesc& q) {
+  const size_t budget = size_t(ctx->max_smem_optin);
+  const size_t fixed = gba_exchange_smem_bytes(q, 0) + gba_exchange_static_smem() + 1024;
+  if (budget <= fixed) return 0;
+  const size_t slot = (q.key64 ? 8 : 4) + 8 * size_t(q.nwords);
+  return int(std::min<size_t>(65536, (budget - fixed) / slot)) / 4 * 4;
+}
+
+// Owner-exchange launch of one aggregate signature and key width.
+struct XGroup {
+  QDesc proto;
+  std::vector<int> members;
+  size_t smem = 0;
+  int64_t xq_off = 0;  // first entry of the group in the device list of query slots
+};
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
@@ -382,9 +401,35 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
                                                      : gba_choose_strategy(ctx, qd[i], k, pred[i], qi[i].p);
   }
 
+  // ---- owner exchange ----
+  // A query whose predicted groups outgrow one streaming CTA's shared table
+  // but fit 0.6 of the exchange kernel's tables over all SMs goes to the
+  // owner-exchange kernel (learned sizing, at least 2^19 rows, no key taking
+  // 1/32 of the sample: a hot key would load its owner alone).  Its HBM table
+  // only takes keys whose shared probe window is full, so it is sized small
+  // (an overflow reruns the query alone with a larger table).
+  int xgrid = ctx->sms;
+  for (int i = 0; i < nq; ++i) {
+    if (qi[i].strategy != GBA_STRATEGY_TABLE || k.exchange == 0 || qd[i].n <= 0) continue;
+    const int Sx = exchange_smem_slots(ctx, qd[i]);
+    if (Sx < 256) continue;
+    if (k.exchange == 1) qi[i].xch = true;
+    else
+      qi[i].xch = k.sizing == GBA_SIZING_LEARNED && qi[i].pred > 0 && qi[i].p.preagg && qd[i].n >= (int64_t(1) << 19) &&
+                  skew[i] < 1.0 / 32.0 && qi[i].pred > 0.5 * batch_smem_slots(ctx, qd[i], bps) &&
+                  qi[i].pred <= 0.6 * double(xgrid) * Sx;
+    if (qi[i].xch) {
+      qi[i].S = Sx;
+      if (qi[i].pred > 0) {
+        const uint64_t small = std::max<uint64_t>(uint64_t(1) << 16, uint64_t(qi[i].pred * 0.5) + 1);
+        qi[i].p.table_slots = std::min<uint64_t>(qi[i].p.table_slots, small);
+      }
+    }
+  }
+
   // ---- streaming kernel of each query ----
   for (int i = 0; i < nq; ++i) {
-    if (qi[i].strategy != GBA_STRATEGY_TABLE) continue;
+    if (qi[i].strategy != GBA_STRATEGY_TABLE || qi[i].xch) continue;
     if (k.use_tma == 0) qi[i].tma = false;
     else if (k.use_tma == 1) qi[i].tma = true;
     else qi[i].tma = qi[i].pred > 0 && qi[i].p.preagg && qi[i].pred > 0.5 * batch_smem_slots(ctx, qd[i], bps);
@@ -419,7 +464,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   std::vector<Group> groups;
   std::vector<int> tq;  // table-strategy queries, group by group
   for (int i = 0; i < nq; ++i) {
-    if (qi[i].strategy != GBA_STRATEGY_TABLE) continue;
+    if (qi[i].strategy != GBA_STRATEGY_TABLE || qi[i].xch) continue;
     // one launch per signature, key width, kernel and cluster size
     const int sig = ((2 * gba_batch_sig_id(qd[i]) + (qd[i].key64 ? 1 : 0)) * 2 + (qi[i].tma ? 1 : 0)) * 32 + qi[i].cl;
     auto it = std::find_if(groups.begin(), groups.end(), [&](const Group& g) { return g.sig == sig; });
@@ -471,6 +516,38 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
       }
     }
   }
+  // exchange launches: one per signature and key width, queries largest first
+  std::vector<XGroup> xgroups;
+  int64_t xwin = 0, xstride = 1;
+  for (int i = 0; i < nq; ++i) {
+    if (!qi[i].xch) continue;
+    const int sig = 2 * gba_batch_sig_id(qd[i]) + (qd[i].key64 ? 1 : 0);
+    auto it = std::find_if(xgroups.begin(), xgroups.end(), [&](const XGroup& g) {
+      return 2 * gba_batch_sig_id(g.proto) + (g.proto.key64 ? 1 : 0) == sig;
+    });
+    if (it == xgroups.end()) {
+      xgroups.push_back(XGroup{qd[i], {}});
+      it = xgroups.end() - 1;
+    }
+    it->members.push_back(i);
+    it->smem = std::max(it->smem, gba_exchange_smem_bytes(qd[i], qi[i].S));
+    qi[i].slot = int(tq.size());
+    tq.push_back(i);
+    xwin = std::max<int64_t>(xwin, qd[i].n);
+    xstride = std::max<int64_t>(xstride, 1 + qd[i].ncols);
+  }
+  for (auto& g : xgroups) {
+    std::stable_sort(g.members.begin(), g.members.end(), [&](int a, int b) { return qd[a].n > qd[b].n; });
+    GBA_CUDA_TRY(ctx, gba_prepare_exchange(g.proto));
+    const int gg = gba_exchange_grid(g.proto, g.smem, ctx->sms);
+    if (gg < 1) {
+      ctx->err = "owner-exchange kernel: no CTA fits an SM";
+      return GBA_ERR_CUDA;
+    }
+    xgrid = std::min(xgrid, gg);
+  }
+  // rows per window: 2^20 (two buffers of 2^20 records of 16 bytes stay in L2)
+  xwin = std::min<int64_t>(xwin, int64_t(1) << 20);
   const int nt = int(tq.size());
 
   // ---- work items ----
@@ -531,9 +608,20 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   const size_t o_items = take(sizeof(BatchSpan) * spans.size());
   const size_t o_ipre = take(8 * size_t(nt + 1));
   const size_t o_cpre = take(8 * size_t(nt + 1));
+  int64_t nxq = 0;
+  for (auto& g : xgroups) {
+    g.xq_off = nxq;
+    nxq += int64_t(g.members.size());
+  }
+  const size_t o_xq = take(4 * size_t(std::max<int64_t>(nxq, 1)));
   const size_t desc_bytes = off;
-  const size_t o_stat = take(16 * size_t(nt) + 4 * size_t(ng));
-  const size_t stat_bytes = 16 * size_t(nt) + 4 * size_t(ng);
+  // status: per query flags + group count, per launch item counters, then the
+  // exchange kernel's barrier words, flags and per-owner cursors of two buffers
+  const size_t xstat = nxq ? 16 + 8 * size_t(xgrid) : 0;
+  const size_t o_stat = take(16 * size_t(nt) + 4 * size_t(ng) + xstat);
+  const size_t stat_bytes = 16 * size_t(nt) + 4 * size_t(ng) + xstat;
+  const size_t o_xstat = o_stat + 16 * size_t(nt) + 4 * size_t(ng);
+  const size_t o_xbuf = nxq ? take(2 * size_t(xgrid) * size_t(xwin) * size_t(xstride) * 8) : 0;
   std::vector<size_t> o_tab(nt);
   std::vector<int64_t> ipre(nt + 1, 0), cpre(nt + 1, 0);
   for (int j = 0; j < nt; ++j) {
@@ -572,7 +660,8 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
       for (int c = 0; c < qd[i].ncols; ++c) vec = vec && aligned16(qd[i].cols[c]);
       // bits 8..15: buckets probed per row; a table the query's groups will
       // overfill keeps only what reaches its home bucket
-      const int nbk = (qi[i].S > 0 && qi[i].pred > 2.0 * qi[i].S * qi[i].cl) ? 1 : 0;
+      const double tslots = double(qi[i].S) * (qi[i].xch ? xgrid : qi[i].cl);
+      const int nbk = (qi[i].S > 0 && qi[i].pred > 2.0 * tslots) ? 1 : 0;
       // bit 1 (bulk-copy kernel): combine equal keys within a warp first, for
       // queries whose sample shows a key taking at least 1/32 of the rows (one
       // lane of a warp on average) or when the knob forces it
@@ -585,6 +674,9 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
     if (!spans.empty()) std::memcpy(h + o_items, spans.data(), sizeof(BatchSpan) * spans.size());
     std::memcpy(h + o_ipre, ipre.data(), 8 * size_t(nt + 1));
     std::memcpy(h + o_cpre, cpre.data(), 8 * size_t(nt + 1));
+    for (const auto& g : xgroups)
+      for (size_t m = 0; m < g.members.size(); ++m)
+        reinterpret_cast<int*>(h + o_xq)[g.xq_off + int64_t(m)] = qi[g.members[m]].slot;
   }
 
   // ---- the launch sequence (direct or as a replayed graph) ----
@@ -615,6 +707,13 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
                      : gba_launch_stream_agg(groups[g].proto, bps, d_qs, d_spans + groups[g].item_begin,
                                              groups[g].nspans, groups[g].nitems, d_ctr + g, groups[g].smem, sprobe,
                                              groups[g].grid, cs);
+    for (size_t g = 0; g < xgroups.size() && e == cudaSuccess; ++g)
+      e = gba_launch_exchange(xgroups[g].proto, d_qs, reinterpret_cast<const int*>(d + o_xq) + xgroups[g].xq_off,
+                              int(xgroups[g].members.size()), xwin,
+                              reinterpret_cast<unsigned long long*>(d + o_xbuf), xwin,
+                              reinterpret_cast<unsigned*>(d + o_xstat + 16),
+                              reinterpret_cast<unsigned*>(d + o_xstat),
+                              reinterpret_cast<unsigned*>(d + o_xstat + 8), xgroups[g].smem, sprobe, xgrid, cs);
     if (e == cudaSuccess) e = mark(2, cs);
     if (e == cudaSuccess)
       e = gba_launch_batch_compact(d_qs, reinterpret_cast<const int64_t*>(d + o_cpre), nt, cpre[nt], cs);
@@ -651,6 +750,14 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
         key.push_back(int64_t(g.stage_bytes));
         key.push_back(g.cluster * 16 + g.minb * 2 + (g.tma ? 1 : 0));
       }
+      key.push_back(nxq);
+      key.push_back(xwin);
+      key.push_back(xgrid);
+      for (const auto& g : xgroups) {
+        key.push_back(2 * gba_batch_sig_id(g.proto) + (g.proto.key64 ? 1 : 0));
+        key.push_back(int64_t(g.smem));
+        key.push_back(int64_t(g.members.size()));
+      }
       if (!ctx->batch_exec || key != ctx->batch_key) {
         if (ctx->batch_exec) {
           cudaGraphExecDestroy(ctx->batch_exec);
@@ -679,7 +786,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
       float ms = 0.f;
       if (cudaEventElapsedTime(&ms, ctx->tev[r], ctx->tev[r + 1]) == cudaSuccess) ctx->stats.kernel_ms[r] += ms;
     }
-    ctx->stats.kernel_launches += 2 + ng;
+    ctx->stats.kernel_launches += 2 + ng + int(xgroups.size());
     for (int i : tq) {
       ctx->stats.main_rows += qd[i].n;
       ctx->stats.main_bytes += qd[i].n * int64_t(gba_row_bytes(qd[i]));
@@ -689,6 +796,10 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   // ---- results; reruns of overflowed queries; partition-strategy queries ----
   gba_status result = GBA_OK;
   gba_stats acc = ctx->stats;
+  if (nxq > 0 && (*reinterpret_cast<const unsigned*>(h + h_stat + (o_xstat - o_stat) + 8) & GBA_FLAG_WAIT_TIMEOUT)) {
+    ctx->err = "owner-exchange kernel: a bounded grid-barrier wait timed out";
+    return GBA_ERR_TIMEOUT;
+  }
   std::vector<int> rerun;
   for (int j = 0; j < nt; ++j) {
     const int i = tq[j];

@@ -1,0 +1,287 @@
+// Owner-exchange aggregation (sm_100a): the batch kernel for queries whose
+// groups outgrow one CTA's shared table but fit the shared tables of all SMs
+// together.
+//
+// Replaces, for those queries, the reference's spill of a tile's leftover rows
+// to an unbounded global linear-probe table (tiled_groupby_agg_partition/src/
+// kernel.cu:116-158) and the per-partition global table of phase 2
+// (kernel.cu:294-351): here no row's aggregate goes through an HBM table.
+//
+// One cooperative launch, one CTA of 512 threads per SM.  CTA c owns the keys
+// whose owner hash falls in the c-th of grid equal ranges, and holds their
+// groups in its shared-memory table for the whole query.  A query's rows are
+// taken in windows of `win` rows:
+//   A  (route)  every CTA reads its slice of the window (coalesced streaming
+//               loads), counts its rows per owner in shared memory, reserves
+//               each owner's run with one global atomic per owner and tile,
+//               and writes every row, as a record (key, then each value
+//               column, 8 bytes each), into its owner's region of the
+//               window's exchange buffer;
+//   (a grid barrier: every record of the window written)
+//   B  (reduce) every CTA reads the records of its own region and applies
+//               them to its shared table (stream_rows.cuh: the same probe and
+//               32-bit atomics as the streaming kernels; a key whose probe
+//               window is full goes to the query's HBM table).
+// Two exchange buffers alternate between windows, so the records of one
+// window are read while the next window's are written; a buffer of
+// win x record bytes stays in L2 between its writes and its reads, so the
+// rows cross HBM once.  After a query's last window every CTA writes the
+// groups of its table straight to the query's output (one atomic per CTA
+// reserves its rows); keys that went to the HBM table are written by the
+// batch's compaction kernel after the launch, so a group is written once.
+//
+// The grid barrier is a counter and a generation word in global memory with
+// a bounded wait (GBA_FLAG_WAIT_TIMEOUT; a CTA that gives up returns, and the
+// others give up at their next barrier).  The launch is cooperative, so all
+// CTAs are resident together.
+#include "batch_kernels.h"
+#include "gba_internal.cuh"
+#include "smem_table.cuh"
+
+namespace {
+#include "stream_rows.cuh"
+
+constexpr int kXThreads = 512;
+constexpr int kXRows = 4;                       // rows per thread per tile
+constexpr int kXTile = kXThreads * kXRows;      // rows per tile
+constexpr int kXMaxGrid = 1024;
+
+// Grid-wide barrier of a cooperative launch, bounded: false when the wait
+// gave up (the timeout flag is raised).
+__device__ bool grid_barrier(unsigned* count, unsigned* gen, unsigned nblocks, unsigned* flags, int* s_fail) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned g = *(volatile unsigned*)gen;
+    __threadfence();  // this CTA's writes before its arrival
+    if (atomicAdd(count, 1u) == nblocks - 1) {
+      *(volatile unsigned*)count = 0u;
+      __threadfence();
+      atomicAdd(gen, 1u);
+    } else {
+      bool ok = false;
+      for (unsigned it = 0; it < (1u << 24) && !ok; ++it) {
+        ok = *(volatile unsigned*)gen != g;
+        if (!ok) __nanosleep(64);
+      }
+      if (!ok) {
+        atomicOr(flags, GBA_FLAG_WAIT_TIMEOUT);
+        *s_fail = 1;
+      }
+    }
+    __threadfence();  // the other CTAs' writes before this CTA's next reads
+  }
+  __syncthreads();
+  return *s_fail == 0;
+}
+
+template <bool K64, typename Sig>
+__global__ void __launch_bounds__(kXThreads, 1)
+    k_exchange_agg(const BatchQ* qs, const int* xq, int nxq, int64_t win, unsigned long long* xbuf, int64_t region,
+                   unsigned* cursors, unsigned* bar, unsigned* bar_flags, int sprobe) {
+  constexpr int NA = Sig::NA;
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ unsigned s_cnt[kXMaxGrid];
+  __shared__ unsigned s_base[kXMaxGrid];
+  __shared__ unsigned s_warp[kXThreads / 32];
+  __shared__ unsigned long long s_out;
+  __shared__ int s_fail;
+  __shared__ __align__(16) BatchQ s_q;
+  const int tid = threadIdx.x;
+  const unsigned lane = lane_id(), warp = unsigned(tid) >> 5;
+  const unsigned G = gridDim.x, me = blockIdx.x;
+  for (unsigned o = tid; o < G; o += blockDim.x) s_cnt[o] = 0u;
+  if (tid == 0) s_fail = 0;
+  __syncthreads();
+  int64_t wglob = 0;  // windows done by the launch (selects the exchange buffer)
+  for (int x = 0; x < nxq; ++x) {
+    {
+      const unsigned* src = reinterpret_cast<const unsigned*>(qs + xq[x]);
+      unsigned* dst = reinterpret_cast<unsigned*>(&s_q);
+      for (int w = tid; w < int(sizeof(BatchQ) / 4); w += blockDim.x) dst[w] = src[w];
+    }
+    __syncthreads();
+    const QDesc& q = s_q.q;
+    const int ncols = Sig::ncols(q);
+    const int stride = 1 + ncols;  // record words
+    const SmemTable<K64> st = smem_table_carve<K64>(smem, s_q.S, Sig::nwords(q));
+    smem_table_init<K64, Sig>(st, q);
+    const int nbk = (s_q.pad >> 8) & 255 ? (s_q.pad >> 8) & 255 : sprobe;
+    __syncthreads();
+    const int64_t n = q.n;
+    for (int64_t w0 = 0; w0 < n; w0 += win, ++wglob) {
+      const int b = int(wglob & 1);
+      unsigned long long* buf = xbuf + size_t(b) * G * size_t(region) * stride;
+      unsigned* cur = cursors + size_t(b) * G;
+      // ---- A: route this CTA's slice of the window to the owners ----
+      const int64_t we = w0 + win < n ? w0 + win : n;
+      const int64_t slice = ((we - w0 + G - 1) / G + kXTile - 1) / kXTile * kXTile;
+      const int64_t sb = w0 + slice * me < we ? w0 + slice * me : we;
+      const int64_t se = sb + slice < we ? sb + slice : we;
+      for (int64_t t0 = sb; t0 < se; t0 += kXTile) {
+        uint64_t key[kXRows];
+        unsigned long long raw[kXRows][GBA_MAX_COLS];
+        unsigned own[kXRows], rank[kXRows];
+#pragma unroll
+        for (int i = 0; i < kXRows; ++i) {
+          const int64_t r = t0 + tid + int64_t(kXThreads) * i;
+          own[i] = ~0u;
+          if (r < se) {
+            key[i] = K64 ? __ldcs(static_cast<const unsigned long long*>(q.keys) + r)
+                         : __ldcs(static_cast<const unsigned*>(q.keys) + r);
+#pragma unroll
+            for (int c = 0; c < GBA_MAX_COLS; ++c)
+              if (c < ncols)
+                raw[i][c] = gba_type_bytes(Sig::coltype(q, c)) == 8
+                                ? __ldcs(static_cast<const unsigned long long*>(q.cols[c]) + r)
+                                : __ldcs(static_cast<const unsigned*>(q.cols[c]) + r);
+            own[i] = unsigned((uint64_t(part_hash(key[i])) * G) >> 32);
+            rank[i] = atomicAdd(&s_cnt[own[i]], 1u);
+          }
+        }
+        __syncthreads();
+        for (unsigned o = tid; o < G; o += blockDim.x) {
+          const unsigned c = s_cnt[o];
+          s_base[o] = c ? atomicAdd(&cur[o], c) : 0u;
+          s_cnt[o] = 0u;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < kXRows; ++i) {
+          if (own[i] == ~0u) continue;
+          const uint64_t pos = uint64_t(s_base[own[i]]) + rank[i];  // < region: a window has win <= region rows
+          unsigned long long* rec = buf + (uint64_t(own[i]) * uint64_t(region) + pos) * stride;
+          rec[0] = key[i];
+#pragma unroll
+          for (int c = 0; c < GBA_MAX_COLS; ++c)
+            if (c < ncols) rec[1 + c] = raw[i][c];
+        }
+      }
+      if (!grid_barrier(bar, bar + 1, G, bar_flags, &s_fail)) return;
+      // ---- B: this CTA's records into its shared table ----
+      const unsigned cnt = __ldcg(&cur[me]);
+      const unsigned long long* mine = buf + uint64_t(me) * uint64_t(region) * stride;
+      for (unsigned r0 = 0; r0 < cnt; r0 += kXTile) {
+        uint64_t k2[kXRows];
+        unsigned long long v[kXRows][NA];
+        bool live[kXRows];
+#pragma unroll
+        for (int i = 0; i < kXRows; ++i) {
+          const unsigned r = r0 + tid + kXThreads * i;
+          live[i] = r < cnt;
+          k2[i] = K64 ? EMPTY64 : uint64_t(EMPTY32);
+          unsigned long long raw[GBA_MAX_COLS] = {0ull, 0ull, 0ull, 0ull};
+          if (live[i]) {
+            const unsigned long long* rec = mine + uint64_t(r) * stride;
+            k2[i] = __ldcg(rec);
+#pragma unroll
+            for (int c = 0; c < GBA_MAX_COLS; ++c)
+              if (c < ncols) raw[c] = __ldcg(rec + 1 + c);
+          }
+          row_contrib<Sig>(q, raw, v[i]);
+        }
+        stream_rows<K64, Sig, kXRows>(s_q, st, nbk, k2, v, live);
+      }
+      __syncthreads();
+      if (tid == 0) cur[me] = 0u;  // the buffer's next writers start after the next barrier
+    }
+    // ---- the query's groups of this CTA's table, straight to its output ----
+    __syncthreads();
+    {
+      const OutDesc& o = s_q.out;
+      const int per = (st.S + kXThreads - 1) / kXThreads;
+      unsigned cnt = 0;
+      for (int j = 0; j < per; ++j) {
+        const int i = tid * per + j;
+        if (i < st.S && uint64_t(st.keys[i]) != uint64_t(smem_empty_key<K64>())) ++cnt;
+      }
+      unsigned xs = cnt;  // inclusive warp scan
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const unsigned y = __shfl_up_sync(GBA_FULL_MASK, xs, d);
+        if (int(lane) >= d) xs += y;
+      }
+      if (lane == 31) s_warp[warp] = xs;
+      __syncthreads();
+      if (tid == 0) {
+        unsigned run = 0;
+        for (int w = 0; w < kXThreads / 32; ++w) {
+          const unsigned c = s_warp[w];
+          s_warp[w] = run;
+          run += c;
+        }
+        const unsigned side = *st.side_present ? 1u : 0u;
+        s_out = run + side ? atomicAdd(o.count, (unsigned long long)(run + side)) : 0ull;
+        if (side) {  // the all-ones key's group, after this CTA's others
+          const unsigned long long pos = s_out + run;
+          if (pos < (unsigned long long)o.capacity) {
+            if (K64) static_cast<unsigned long long*>(o.keys)[pos] = EMPTY64;
+            else static_cast<unsigned*>(o.keys)[pos] = EMPTY32;
+#pragma unroll
+            for (int a = 0; a < NA; ++a) o.accs[a][pos] = smem_acc_read<K64, Sig>(st, q, a, -1);
+          }
+        }
+      }
+      __syncthreads();
+      unsigned long long pos = s_out + s_warp[warp] + (xs - cnt);
+      for (int j = 0; j < per; ++j) {
+        const int i = tid * per + j;
+        if (i >= st.S || uint64_t(st.keys[i]) == uint64_t(smem_empty_key<K64>())) continue;
+        if (pos < (unsigned long long)o.capacity) {
+          if (K64) static_cast<unsigned long long*>(o.keys)[pos] = st.keys[i];
+          else static_cast<unsigned*>(o.keys)[pos] = unsigned(st.keys[i]);
+#pragma unroll
+          for (int a = 0; a < NA; ++a) o.accs[a][pos] = smem_acc_read<K64, Sig>(st, q, a, i);
+        }
+        ++pos;
+      }
+    }
+    __syncthreads();  // s_q and the table are rewritten by the next query
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+size_t gba_exchange_smem_bytes(const QDesc& q, int S) { return smem_table_bytes(S, q.key64, q.nwords) + 64; }
+
+size_t gba_exchange_static_smem() { return 2 * kXMaxGrid * 4 + sizeof(BatchQ) + 256; }
+
+cudaError_t gba_prepare_exchange(const QDesc& proto) {
+  return gba_dispatch_sig(proto, [&](auto K, auto sig) -> cudaError_t {
+    return gba_allow_max_smem(k_exchange_agg<decltype(K)::value, decltype(sig)>);
+  });
+}
+
+int gba_exchange_grid(const QDesc& proto, size_t smem, int sms) {
+  int per_sm = 0;
+  gba_dispatch_sig(proto, [&](auto K, auto sig) -> cudaError_t {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_exchange_agg<decltype(K)::value, decltype(sig)>,
+                                                      kXThreads, smem) != cudaSuccess) {
+      cudaGetLastError();
+      per_sm = 0;
+    }
+    return cudaSuccess;
+  });
+  return per_sm >= 1 ? std::min(sms, kXMaxGrid) : 0;
+}
+
+cudaError_t gba_launch_exchange(const QDesc& proto, const BatchQ* d_qs, const int* d_xq, int nxq, int64_t win,
+                                unsigned long long* xbuf, int64_t region, unsigned* cursors, unsigned* bar,
+                                unsigned* bar_flags, size_t smem, int sprobe, int grid, cudaStream_t s) {
+  if (nxq <= 0) return cudaSuccess;
+  if (grid < 1 || grid > kXMaxGrid || win > region) return cudaErrorInvalidValue;
+  return gba_dispatch_sig(proto, [&](auto K, auto sig) -> cudaError_t {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(unsigned(grid));
+    cfg.blockDim = dim3(kXThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_exchange_agg<decltype(K)::value, decltype(sig)>, d_qs, d_xq, nxq, win, xbuf,
+                              region, cursors, bar, bar_flags, sprobe);
+  });
+}

@@ -154,6 +154,12 @@ typedef struct gba_knobs {
                              cluster whose shared tables together hold one query's table (distributed
                              shared memory), for queries whose predicted groups outgrow one CTA's table
                              (0 or 1 = off, the default; 2, 4, 8 or 16) */
+  int32_t exchange;       /* batch: owner-exchange aggregation (-1 auto, 0 off, 1 every table query):
+                             every SM owns a range of keys and holds their groups in its shared table;
+                             rows reach their owner through exchange buffers that stay in L2.  Auto:
+                             learned sizing, queries of at least 2^19 rows whose predicted groups
+                             outgrow one CTA's table but fit the SMs' tables together, without a key
+                             taking 1/32 of the sample */
 } gba_knobs;
 
 /* What the last call on a context did. */

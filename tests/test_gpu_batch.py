@@ -159,3 +159,33 @@ def test_batch_cluster_tables_match_oracle(ctx, cluster):
     # the same with the graph replayed and with warp combining forced
     res = ctx.groupby_batch(_device(qs), knobs=dict(sizing="learned", cluster_ctas=cluster, coalesce=1))
     _check(qs, res, f"cluster {cluster} combined")
+
+
+@pytest.mark.parametrize("knobs", [dict(exchange=1), dict(exchange=1, sizing="learned"),
+                                   dict(exchange=1, smem_probe_cap=1)])
+def test_batch_owner_exchange_matches_oracle(ctx, knobs):
+    """Every table query through the owner-exchange kernel (each SM owns a
+    range of keys; rows reach their owner through buffers that alternate
+    between windows): all key types and aggregate signatures of the mixed
+    queries, empty and tiny queries among them."""
+    if knobs.get("sizing") == "learned":
+        assert E.load_default(ctx), "committed estimator weights are missing"
+    qs = _queries(20, seed=21)
+    _check(qs, ctx.groupby_batch(_device(qs), knobs=knobs), str(knobs))
+
+
+def test_batch_owner_exchange_windows_and_overflow(ctx):
+    """Queries longer than one exchange window (2^20 rows), groups beyond the
+    SMs' shared tables (keys go to the HBM table, each key in one place), and
+    the automatic choice under learned sizing."""
+    assert E.load_default(ctx), "committed estimator weights are missing"
+    specs = [(2_500_003, np.int64, 300_000, 0.0), (1_200_000, np.int32, 40_000, 0.2),
+             (1_500_000, np.uint32, 2_000_000, 0.0), (700_000, np.int64, 20_000, 0.4)]
+    aggsets = [[("sum", 0), ("count", None)], [("sum", 0), ("sum", 2), ("count", None)],
+               [("sum", 3), ("count", None)], AGGS_ALL]
+    qs = []
+    for i, ((n, kdt, ndv, z), aggs) in enumerate(zip(specs, aggsets)):
+        keys, cols = _data(n, kdt, ndv, seed=800 + i, zipf=z)
+        qs.append((keys, cols, aggs))
+    for knobs in (dict(exchange=1), dict(sizing="learned"), dict(sizing="learned", exchange=0)):
+        _check(qs, ctx.groupby_batch(_device(qs), knobs=knobs), f"exchange {knobs}")
