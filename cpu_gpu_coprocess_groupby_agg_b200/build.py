@@ -81,10 +81,14 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
                 print(f"== {futs[f].name}\n{log}", file=sys.stderr)
     lib = LIBDIR / "libgba.so"
     if _stale(lib, objs) or todo:
-        cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", str(lib), *map(str, objs), "-lpthread"]
+        # linked beside the library and renamed over it, so a reader never sees a partial file
+        tmp = LIBDIR / f".libgba.so.{os.getpid()}"
+        cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", str(tmp), *map(str, objs), "-lpthread"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
+            tmp.unlink(missing_ok=True)
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+        os.replace(tmp, lib)
     build_driver(lib)
     return lib
 

@@ -66,6 +66,7 @@ struct QInfo {
   int cl = 1;        // CTAs of the cluster whose tables form the query's shared table
   bool tma = false;  // streamed by the bulk-copy kernel (else the register-loading one)
   bool xch = false;  // aggregated by the owner-exchange kernel
+  int hot = 0;       // exchange: hot-table slots per CTA
   int slot = -1;     // index among the table-strategy queries
 };
 
@@ -145,9 +146,9 @@ int tma_smem_slots(const gba_context* ctx, const QDesc& q, int minb, int nst, si
 
 // Shared-table slots per CTA of the owner-exchange kernel (one CTA per SM;
 // the table is the CTA's whole dynamic shared memory).
-int exchange_smem_slots(const gba_context* ctx, const QDesc& q) {
+int exchange_smem_slots(const gba_context* ctx, const QDesc& q, int hot) {
   const size_t budget = size_t(ctx->max_smem_optin);
-  const size_t fixed = gba_exchange_smem_bytes(q, 0) + gba_exchange_static_smem() + 1024;
+  const size_t fixed = gba_exchange_smem_bytes(q, 0, hot) + gba_exchange_static_smem() + 1024;
   if (budget <= fixed) return 0;
   const size_t slot = (q.key64 ? 8 : 4) + 8 * size_t(q.nwords);
   return int(std::min<size_t>(65536, (budget - fixed) / slot)) / 4 * 4;
@@ -404,22 +405,25 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   // ---- owner exchange ----
   // A query whose predicted groups outgrow one streaming CTA's shared table
   // but fit 0.6 of the exchange kernel's tables over all SMs goes to the
-  // owner-exchange kernel (learned sizing, at least 2^19 rows, no key taking
-  // 1/32 of the sample: a hot key would load its owner alone).  Its HBM table
-  // only takes keys whose shared probe window is full, so it is sized small
-  // (an overflow reruns the query alone with a larger table).
+  // owner-exchange kernel (learned sizing, at least 2^19 rows).  A query whose
+  // sample shows a key taking 1/256 of the rows (or any query without an
+  // estimate) also gets hot tables of 1024 slots, so its hottest keys are
+  // aggregated where they are read instead of loading their owners.  Its HBM
+  // table only takes keys whose shared probe window is full, so it is sized
+  // small (an overflow reruns the query alone with a larger table).
   int xgrid = ctx->sms;
   for (int i = 0; i < nq; ++i) {
     if (qi[i].strategy != GBA_STRATEGY_TABLE || k.exchange == 0 || qd[i].n <= 0) continue;
-    const int Sx = exchange_smem_slots(ctx, qd[i]);
+    const int hot = (qi[i].pred <= 0 || skew[i] >= 1.0 / 256.0) ? 1024 : 0;
+    const int Sx = exchange_smem_slots(ctx, qd[i], hot);
     if (Sx < 256) continue;
     if (k.exchange == 1) qi[i].xch = true;
     else
       qi[i].xch = k.sizing == GBA_SIZING_LEARNED && qi[i].pred > 0 && qi[i].p.preagg && qd[i].n >= (int64_t(1) << 19) &&
-                  skew[i] < 1.0 / 32.0 && qi[i].pred > 0.5 * batch_smem_slots(ctx, qd[i], bps) &&
-                  qi[i].pred <= 0.6 * double(xgrid) * Sx;
+                  qi[i].pred > 0.5 * batch_smem_slots(ctx, qd[i], bps) && qi[i].pred <= 0.6 * double(xgrid) * Sx;
     if (qi[i].xch) {
       qi[i].S = Sx;
+      qi[i].hot = hot;
       if (qi[i].pred > 0) {
         const uint64_t small = std::max<uint64_t>(uint64_t(1) << 16, uint64_t(qi[i].pred * 0.5) + 1);
         qi[i].p.table_slots = std::min<uint64_t>(qi[i].p.table_slots, small);
@@ -519,6 +523,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   // exchange launches: one per signature and key width, queries largest first
   std::vector<XGroup> xgroups;
   int64_t xwin = 0, xstride = 1;
+  int xhot = 0;
   for (int i = 0; i < nq; ++i) {
     if (!qi[i].xch) continue;
     const int sig = 2 * gba_batch_sig_id(qd[i]) + (qd[i].key64 ? 1 : 0);
@@ -530,11 +535,15 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
       it = xgroups.end() - 1;
     }
     it->members.push_back(i);
-    it->smem = std::max(it->smem, gba_exchange_smem_bytes(qd[i], qi[i].S));
+    it->smem = std::max(it->smem, gba_exchange_smem_bytes(qd[i], qi[i].S, qi[i].hot));
     qi[i].slot = int(tq.size());
     tq.push_back(i);
     xwin = std::max<int64_t>(xwin, qd[i].n);
     xstride = std::max<int64_t>(xstride, 1 + qd[i].ncols);
+    if (qi[i].hot) {  // hot tables leave as partial records of 1 + naccs words
+      xstride = std::max<int64_t>(xstride, 1 + qd[i].naccs);
+      xhot = std::max(xhot, qi[i].hot);
+    }
   }
   for (auto& g : xgroups) {
     std::stable_sort(g.members.begin(), g.members.end(), [&](int a, int b) { return qd[a].n > qd[b].n; });
@@ -546,8 +555,11 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
     }
     xgrid = std::min(xgrid, gg);
   }
-  // rows per window: 2^20 (two buffers of 2^20 records of 16 bytes stay in L2)
+  // rows per window: 2^20 (two buffers of 2^20 records of 16 bytes stay in
+  // L2); an owner's region also holds the partial records of every CTA's hot
+  // table
   xwin = std::min<int64_t>(xwin, int64_t(1) << 20);
+  const int64_t xregion = std::max<int64_t>(xwin, int64_t(xgrid) * (xhot + 1));
   const int nt = int(tq.size());
 
   // ---- work items ----
@@ -621,7 +633,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   const size_t o_stat = take(16 * size_t(nt) + 4 * size_t(ng) + xstat);
   const size_t stat_bytes = 16 * size_t(nt) + 4 * size_t(ng) + xstat;
   const size_t o_xstat = o_stat + 16 * size_t(nt) + 4 * size_t(ng);
-  const size_t o_xbuf = nxq ? take(2 * size_t(xgrid) * size_t(xwin) * size_t(xstride) * 8) : 0;
+  const size_t o_xbuf = nxq ? take(2 * size_t(xgrid) * size_t(xregion) * size_t(xstride) * 8) : 0;
   std::vector<size_t> o_tab(nt);
   std::vector<int64_t> ipre(nt + 1, 0), cpre(nt + 1, 0);
   for (int j = 0; j < nt; ++j) {
@@ -668,7 +680,8 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
       // (measured on the batch's queries of fewer than 256 ids: combining made
       // the kernel slower, 1.37 against 0.89 ms, so it is opt-in)
       const bool comb = qi[i].tma && k.coalesce == 1;
-      b.pad = (vec ? 1 : 0) | (comb ? 2 : 0) | (nbk << 8);  // bit 0: columns allow vector loads
+      // bits 16..27 (exchange): hot-table slots / 4
+      b.pad = (vec ? 1 : 0) | (comb ? 2 : 0) | (nbk << 8) | ((qi[i].hot / 4) << 16);  // bit 0: vector loads
       hq[j] = b;
     }
     if (!spans.empty()) std::memcpy(h + o_items, spans.data(), sizeof(BatchSpan) * spans.size());
@@ -710,7 +723,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
     for (size_t g = 0; g < xgroups.size() && e == cudaSuccess; ++g)
       e = gba_launch_exchange(xgroups[g].proto, d_qs, reinterpret_cast<const int*>(d + o_xq) + xgroups[g].xq_off,
                               int(xgroups[g].members.size()), xwin,
-                              reinterpret_cast<unsigned long long*>(d + o_xbuf), xwin,
+                              reinterpret_cast<unsigned long long*>(d + o_xbuf), xregion,
                               reinterpret_cast<unsigned*>(d + o_xstat + 16),
                               reinterpret_cast<unsigned*>(d + o_xstat),
                               reinterpret_cast<unsigned*>(d + o_xstat + 8), xgroups[g].smem, sprobe, xgrid, cs);
@@ -752,6 +765,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
       }
       key.push_back(nxq);
       key.push_back(xwin);
+      key.push_back(xregion);
       key.push_back(xgrid);
       for (const auto& g : xgroups) {
         key.push_back(2 * gba_batch_sig_id(g.proto) + (g.proto.key64 ? 1 : 0));

@@ -30,6 +30,14 @@
 // reserves its rows); keys that went to the HBM table are written by the
 // batch's compaction kernel after the launch, so a group is written once.
 //
+// Skewed keys: a query with bits 16..27 of BatchQ.pad set gives every CTA a
+// small "hot" table of 4 x that many slots beside its owner table.  In A a
+// row whose key is in the CTA's hot table, or can enter its home bucket there,
+// is aggregated on the spot instead of routed, so a key that takes a large
+// share of the rows does not load its owner alone.  After the query's last
+// window every CTA routes its hot table's groups as partial records (key and
+// accumulator values) to their owners, which merge them like rows.
+//
 // The grid barrier is a counter and a generation word in global memory with
 // a bounded wait (GBA_FLAG_WAIT_TIMEOUT; a CTA that gives up returns, and the
 // others give up at their next barrier).  The launch is cooperative, so all
@@ -105,6 +113,10 @@ __global__ void __launch_bounds__(kXThreads, 1)
     const int stride = 1 + ncols;  // record words
     const SmemTable<K64> st = smem_table_carve<K64>(smem, s_q.S, Sig::nwords(q));
     smem_table_init<K64, Sig>(st, q);
+    const int hot = ((s_q.pad >> 16) & 4095) * 4;  // hot-table slots (0: none)
+    const SmemTable<K64> ht = smem_table_carve<K64>(
+        smem + ((smem_table_bytes(s_q.S, K64, Sig::nwords(q)) + 127) & ~size_t(127)), hot, Sig::nwords(q));
+    if (hot > 0) smem_table_init<K64, Sig>(ht, q);
     const int nbk = (s_q.pad >> 8) & 255 ? (s_q.pad >> 8) & 255 : sprobe;
     __syncthreads();
     const int64_t n = q.n;
@@ -121,11 +133,15 @@ __global__ void __launch_bounds__(kXThreads, 1)
         uint64_t key[kXRows];
         unsigned long long raw[kXRows][GBA_MAX_COLS];
         unsigned own[kXRows], rank[kXRows];
+        bool live[kXRows];
 #pragma unroll
         for (int i = 0; i < kXRows; ++i) {
           const int64_t r = t0 + tid + int64_t(kXThreads) * i;
-          own[i] = ~0u;
-          if (r < se) {
+          live[i] = r < se;
+          key[i] = K64 ? EMPTY64 : uint64_t(EMPTY32);
+#pragma unroll
+          for (int c = 0; c < GBA_MAX_COLS; ++c) raw[i][c] = 0ull;
+          if (live[i]) {
             key[i] = K64 ? __ldcs(static_cast<const unsigned long long*>(q.keys) + r)
                          : __ldcs(static_cast<const unsigned*>(q.keys) + r);
 #pragma unroll
@@ -134,6 +150,21 @@ __global__ void __launch_bounds__(kXThreads, 1)
                 raw[i][c] = gba_type_bytes(Sig::coltype(q, c)) == 8
                                 ? __ldcs(static_cast<const unsigned long long*>(q.cols[c]) + r)
                                 : __ldcs(static_cast<const unsigned*>(q.cols[c]) + r);
+          }
+        }
+        if (hot > 0) {  // keys of the hot table are aggregated here, the rest routed
+          unsigned long long v[kXRows][NA];
+#pragma unroll
+          for (int i = 0; i < kXRows; ++i) row_contrib<Sig>(q, raw[i], v[i]);
+          uint32_t hh[kXRows];
+          const unsigned miss = smem_rows<K64, Sig, kXRows>(ht, q, 1, key, v, live, hh);
+#pragma unroll
+          for (int i = 0; i < kXRows; ++i) live[i] = (miss >> i) & 1u;
+        }
+#pragma unroll
+        for (int i = 0; i < kXRows; ++i) {
+          own[i] = ~0u;
+          if (live[i]) {
             own[i] = unsigned((uint64_t(part_hash(key[i])) * G) >> 32);
             rank[i] = atomicAdd(&s_cnt[own[i]], 1u);
           }
@@ -150,10 +181,14 @@ __global__ void __launch_bounds__(kXThreads, 1)
           if (own[i] == ~0u) continue;
           const uint64_t pos = uint64_t(s_base[own[i]]) + rank[i];  // < region: a window has win <= region rows
           unsigned long long* rec = buf + (uint64_t(own[i]) * uint64_t(region) + pos) * stride;
-          rec[0] = key[i];
+          if (stride == 2) {  // one 16-byte store (records of an even word count are 16-byte aligned)
+            *reinterpret_cast<ulonglong2*>(rec) = make_ulonglong2(key[i], raw[i][0]);
+          } else {
+            rec[0] = key[i];
 #pragma unroll
-          for (int c = 0; c < GBA_MAX_COLS; ++c)
-            if (c < ncols) rec[1 + c] = raw[i][c];
+            for (int c = 0; c < GBA_MAX_COLS; ++c)
+              if (c < ncols) rec[1 + c] = raw[i][c];
+          }
         }
       }
       if (!grid_barrier(bar, bar + 1, G, bar_flags, &s_fail)) return;
@@ -172,10 +207,16 @@ __global__ void __launch_bounds__(kXThreads, 1)
           unsigned long long raw[GBA_MAX_COLS] = {0ull, 0ull, 0ull, 0ull};
           if (live[i]) {
             const unsigned long long* rec = mine + uint64_t(r) * stride;
-            k2[i] = __ldcg(rec);
+            if (stride == 2) {
+              const ulonglong2 x = __ldcg(reinterpret_cast<const ulonglong2*>(rec));
+              k2[i] = x.x;
+              raw[0] = x.y;
+            } else {
+              k2[i] = __ldcg(rec);
 #pragma unroll
-            for (int c = 0; c < GBA_MAX_COLS; ++c)
-              if (c < ncols) raw[c] = __ldcg(rec + 1 + c);
+              for (int c = 0; c < GBA_MAX_COLS; ++c)
+                if (c < ncols) raw[c] = __ldcg(rec + 1 + c);
+            }
           }
           row_contrib<Sig>(q, raw, v[i]);
         }
@@ -183,6 +224,55 @@ __global__ void __launch_bounds__(kXThreads, 1)
       }
       __syncthreads();
       if (tid == 0) cur[me] = 0u;  // the buffer's next writers start after the next barrier
+    }
+    if (hot > 0) {
+      // ---- the hot tables' groups to their owners, as partial records ----
+      const int b = int(wglob & 1);
+      const int pstride = 1 + NA;
+      unsigned long long* buf = xbuf + size_t(b) * G * size_t(region) * pstride;
+      unsigned* cur = cursors + size_t(b) * G;
+      for (int i = tid; i <= hot; i += kXThreads) {
+        uint64_t k;
+        if (i < hot) {
+          k = uint64_t(ht.keys[i]);
+          if (k == uint64_t(smem_empty_key<K64>())) continue;
+        } else {
+          if (!*ht.side_present) continue;
+          k = K64 ? EMPTY64 : uint64_t(EMPTY32);
+        }
+        const unsigned o = unsigned((uint64_t(part_hash(k)) * G) >> 32);
+        const unsigned pos = atomicAdd(&cur[o], 1u);  // < hot + 1 per CTA: within the region
+        unsigned long long* rec = buf + (uint64_t(o) * uint64_t(region) + pos) * pstride;
+        rec[0] = k;
+#pragma unroll
+        for (int a = 0; a < NA; ++a) rec[1 + a] = smem_acc_read<K64, Sig>(ht, q, a, i < hot ? i : -1);
+      }
+      if (!grid_barrier(bar, bar + 1, G, bar_flags, &s_fail)) return;
+      const unsigned cnt = __ldcg(&cur[me]);
+      const unsigned long long* mine = buf + uint64_t(me) * uint64_t(region) * pstride;
+      for (unsigned r0 = 0; r0 < cnt; r0 += kXTile) {
+        uint64_t k2[kXRows];
+        unsigned long long v[kXRows][NA];
+        bool live[kXRows];
+#pragma unroll
+        for (int i = 0; i < kXRows; ++i) {
+          const unsigned r = r0 + tid + kXThreads * i;
+          live[i] = r < cnt;
+          k2[i] = K64 ? EMPTY64 : uint64_t(EMPTY32);
+#pragma unroll
+          for (int a = 0; a < NA; ++a) v[i][a] = acc_identity(Sig::op(q, a));
+          if (live[i]) {
+            const unsigned long long* rec = mine + uint64_t(r) * pstride;
+            k2[i] = __ldcg(rec);
+#pragma unroll
+            for (int a = 0; a < NA; ++a) v[i][a] = __ldcg(rec + 1 + a);  // partial values merge as contributions
+          }
+        }
+        stream_rows<K64, Sig, kXRows>(s_q, st, nbk, k2, v, live);
+      }
+      __syncthreads();
+      if (tid == 0) cur[me] = 0u;
+      ++wglob;
     }
     // ---- the query's groups of this CTA's table, straight to its output ----
     __syncthreads();
@@ -242,7 +332,10 @@ __global__ void __launch_bounds__(kXThreads, 1)
 }  // namespace
 
 // ---------------------------------------------------------------------------
-size_t gba_exchange_smem_bytes(const QDesc& q, int S) { return smem_table_bytes(S, q.key64, q.nwords) + 64; }
+size_t gba_exchange_smem_bytes(const QDesc& q, int S, int hot) {
+  return ((smem_table_bytes(S, q.key64, q.nwords) + 127) & ~size_t(127)) +
+         (hot > 0 ? smem_table_bytes(hot, q.key64, q.nwords) : 0) + 64;
+}
 
 size_t gba_exchange_static_smem() { return 2 * kXMaxGrid * 4 + sizeof(BatchQ) + 256; }
 

@@ -171,54 +171,66 @@ __device__ __forceinline__ void hbm_rows(const BatchQ& bq, const uint64_t (&key)
   }
 }
 
-// A thread's R rows (key[i], accumulator contributions v[i]; rows whose bit in
-// `live` is clear are skipped) into the item's shared table, or, for rows
-// whose key is not in it and cannot enter it, into the query's HBM table.
+// The shared-table pass over a thread's R rows (key[i], accumulator
+// contributions v[i]; rows whose bit in `live` is clear are skipped), phase by
+// phase so that their shared-memory round trips overlap: first every row's
+// home bucket, then the rows that did not find their key there walk the probe
+// sequence (nbk buckets), then the accumulator updates of all rows are issued
+// before any result is used.  h receives the rows' table hashes; returns the
+// rows whose key is not in the table and cannot enter it.
+template <bool K64, typename Sig, int R>
+__device__ __forceinline__ unsigned smem_rows(const SmemTable<K64>& st, const QDesc& q, int nbk,
+                                              const uint64_t (&key)[R], const unsigned long long (&v)[R][Sig::NA],
+                                              const bool (&live)[R], uint32_t (&h)[R]) {
+  typedef typename SmemTable<K64>::KeyW KeyW;
+  constexpr int SPB = BucketT<K64>::SPB;
+  const uint64_t emptyk = K64 ? EMPTY64 : uint64_t(EMPTY32);
+  unsigned miss = 0;
+#pragma unroll
+  for (int i = 0; i < R; ++i) h[i] = table_hash(key[i]);
+  int slot[R];
+  KeyW kb[R][SPB];
+#pragma unroll
+  for (int i = 0; i < R; ++i) ld_bucket<K64>(st.keys, bucket_home<K64>(st, h[i]), kb[i]);
+  unsigned hit = 0;
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    slot[i] = -1;
+    if (!live[i]) continue;
+    if (key[i] == emptyk) {  // the all-ones key has its own slot
+      smem_apply_side<K64, Sig>(st, q, v[i]);
+      continue;
+    }
+    bool has_empty = false;
+#pragma unroll
+    for (int e = 0; e < SPB; ++e) {
+      if (kb[i][e] == KeyW(key[i])) slot[i] = bucket_home<K64>(st, h[i]) * SPB + e;
+      has_empty = has_empty || kb[i][e] == smem_empty_key<K64>();
+    }
+    // a home bucket read full without the key settles a one-bucket probe
+    if (slot[i] < 0 && (has_empty || nbk > 1)) slot[i] = bucket_find_or_insert<K64>(st, key[i], h[i], nbk);
+    if (slot[i] >= 0) hit |= 1u << i;
+    else miss |= 1u << i;
+  }
+  smem_apply_rows<K64, Sig, R>(st, q, slot, v, hit);
+  return miss;
+}
+
+// A thread's R rows into the item's shared table, or, for rows whose key is
+// not in it and cannot enter it, into the query's HBM table.
 template <bool K64, typename Sig, int R>
 __device__ __forceinline__ void stream_rows(const BatchQ& bq, const SmemTable<K64>& st, int nbk, const uint64_t (&key)[R],
                                             const unsigned long long (&v)[R][Sig::NA], const bool (&live)[R]) {
-  constexpr int NA = Sig::NA;
   const QDesc& q = bq.q;
   const uint64_t emptyk = K64 ? EMPTY64 : uint64_t(EMPTY32);
-  // shared-table pass, phase by phase over the lane's R rows so that their
-  // shared-memory round trips overlap: first every row's home-slot key, then
-  // the rows that did not find their key there walk the probe sequence, then
-  // the accumulator updates of all rows are issued before any result is used
   unsigned miss = 0;
   uint32_t h[R];
-#pragma unroll
-  for (int i = 0; i < R; ++i) h[i] = table_hash(key[i]);
   if (bq.S > 0) {
-    typedef typename SmemTable<K64>::KeyW KeyW;
-    constexpr int SPB = BucketT<K64>::SPB;
-    int slot[R];
-    KeyW kb[R][SPB];
-#pragma unroll
-    for (int i = 0; i < R; ++i) ld_bucket<K64>(st.keys, bucket_home<K64>(st, h[i]), kb[i]);
-    unsigned hit = 0;
-#pragma unroll
-    for (int i = 0; i < R; ++i) {
-      slot[i] = -1;
-      if (!live[i]) continue;
-      if (key[i] == emptyk) {  // the all-ones key has its own slot
-        smem_apply_side<K64, Sig>(st, q, v[i]);
-        continue;
-      }
-      bool has_empty = false;
-#pragma unroll
-      for (int e = 0; e < SPB; ++e) {
-        if (kb[i][e] == KeyW(key[i])) slot[i] = bucket_home<K64>(st, h[i]) * SPB + e;
-        has_empty = has_empty || kb[i][e] == smem_empty_key<K64>();
-      }
-      // a home bucket read full without the key settles a one-bucket probe
-      if (slot[i] < 0 && (has_empty || nbk > 1)) slot[i] = bucket_find_or_insert<K64>(st, key[i], h[i], nbk);
-      if (slot[i] >= 0) hit |= 1u << i;
-      else miss |= 1u << i;
-    }
-    smem_apply_rows<K64, Sig, R>(st, q, slot, v, hit);
+    miss = smem_rows<K64, Sig, R>(st, q, nbk, key, v, live, h);
   } else {
 #pragma unroll
     for (int i = 0; i < R; ++i) {
+      h[i] = table_hash(key[i]);
       if (!live[i]) continue;
       if (key[i] == emptyk) gtable_insert<K64, Sig>(bq.gt, q, key[i], 0u, v[i], bq.flags);
       else miss |= 1u << i;
