@@ -94,6 +94,9 @@ extern "C" gba_status gba_destroy(gba_context* ctx) {
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
   if (ctx->batch_exec) cudaGraphExecDestroy(ctx->batch_exec);
   if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
+  if (ctx->aux_stream) cudaStreamDestroy(ctx->aux_stream);
+  for (auto& e : ctx->fork_ev)
+    if (e) cudaEventDestroy(e);
   if (ctx->h_batch) cudaFreeHost(ctx->h_batch);
   if (ctx->rp_buf) cudaFree(ctx->rp_buf);
   if (ctx->avg_buf) cudaFree(ctx->avg_buf);

@@ -712,14 +712,21 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
     if (e == cudaSuccess)
       e = gba_launch_batch_init(d_qs, reinterpret_cast<const int64_t*>(d + o_ipre), nt, ipre[nt], cs);
     if (e == cudaSuccess) e = mark(1, cs);
+    // the streaming launches alternate between two streams, so one launch's
+    // tail (its last, small items) overlaps the next launch
+    const bool fork = ng >= 2;
+    if (fork && e == cudaSuccess) e = cudaEventRecord(ctx->fork_ev[0], cs);
+    if (fork && e == cudaSuccess) e = cudaStreamWaitEvent(ctx->aux_stream, ctx->fork_ev[0], 0);
     for (int g = 0; g < ng && e == cudaSuccess; ++g)
       e = groups[g].tma ? gba_launch_stream_tma(groups[g].proto, groups[g].cluster, groups[g].minb, d_qs,
                                              d_spans + groups[g].item_begin, groups[g].nspans,
                                              groups[g].nitems, d_ctr + g, groups[g].smem, sprobe, groups[g].grid,
-                                             nst, groups[g].stage_bytes, cs)
+                                             nst, groups[g].stage_bytes, fork && (g & 1) ? ctx->aux_stream : cs)
                      : gba_launch_stream_agg(groups[g].proto, bps, d_qs, d_spans + groups[g].item_begin,
                                              groups[g].nspans, groups[g].nitems, d_ctr + g, groups[g].smem, sprobe,
-                                             groups[g].grid, cs);
+                                             groups[g].grid, fork && (g & 1) ? ctx->aux_stream : cs);
+    if (fork && e == cudaSuccess) e = cudaEventRecord(ctx->fork_ev[1], ctx->aux_stream);
+    if (fork && e == cudaSuccess) e = cudaStreamWaitEvent(cs, ctx->fork_ev[1], 0);
     for (size_t g = 0; g < xgroups.size() && e == cudaSuccess; ++g)
       e = gba_launch_exchange(xgroups[g].proto, d_qs, reinterpret_cast<const int*>(d + o_xq) + xgroups[g].xq_off,
                               int(xgroups[g].members.size()), xwin,
@@ -735,6 +742,10 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
     return e;
   };
   trace.mark("plan");
+  if (nt > 0 && ng >= 2 && !ctx->aux_stream) {
+    GBA_CUDA_TRY(ctx, cudaStreamCreateWithFlags(&ctx->aux_stream, cudaStreamNonBlocking));
+    for (auto& ev : ctx->fork_ev) GBA_CUDA_TRY(ctx, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  }
   if (nt > 0) {
     for (int g = 0; g < ng; ++g)
       GBA_CUDA_TRY(ctx, groups[g].tma ? gba_prepare_stream_tma(groups[g].proto, groups[g].cluster, groups[g].minb)

@@ -40,6 +40,9 @@ struct gba_context {
   unsigned char* h_batch = nullptr;
   size_t h_batch_bytes = 0;
   cudaStream_t cap_stream = nullptr;
+  // a second stream (and fork/join events) for batch launches that run side by side
+  cudaStream_t aux_stream = nullptr;
+  cudaEvent_t fork_ev[2] = {};
   cudaGraphExec_t batch_exec = nullptr;
   std::vector<int64_t> batch_key;
   // drop-in API: a tile's groups before the reference-layout partitioning
