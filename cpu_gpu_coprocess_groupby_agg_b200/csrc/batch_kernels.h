@@ -63,15 +63,16 @@ cudaError_t gba_launch_stream_tma(const QDesc& proto, int cluster, int minb, con
 // Owner-exchange aggregation (k_exchange.cu): one cooperative launch of `grid`
 // CTAs (one per SM) over the nxq queries d_xq (indices into d_qs), each with
 // a shared table of BatchQ.S slots per CTA (and a hot table of 4 x
-// (BatchQ.pad >> 16 & 4095) slots).  Rows move in windows of `win`
-// rows through two exchange buffers xbuf of 2 x grid x region records of
-// (1 + ncols) 8-byte words (region >= win); cursors (2 x grid), bar (2) and
-// *bar_flags must be zero at launch.
+// (BatchQ.pad >> 16 & 4095) slots).  Rows move in windows of `win` rows
+// through two exchange buffers of buf_words 8-byte words each, which hold
+// grid regions of `region` records of the widest record (1 + ncols words for
+// rows, 1 + naccs for hot-table partials; region >= win); cursors (2 x grid),
+// bar (2) and *bar_flags must be zero at launch.
 // S owner-table slots and `hot` hot-table slots per CTA
 size_t gba_exchange_smem_bytes(const QDesc& q, int S, int hot);
 size_t gba_exchange_static_smem();
 cudaError_t gba_prepare_exchange(const QDesc& proto);
 int gba_exchange_grid(const QDesc& proto, size_t smem, int sms);
 cudaError_t gba_launch_exchange(const QDesc& proto, const BatchQ* d_qs, const int* d_xq, int nxq, int64_t win,
-                                unsigned long long* xbuf, int64_t region, unsigned* cursors, unsigned* bar,
-                                unsigned* bar_flags, size_t smem, int sprobe, int grid, cudaStream_t s);
+                                unsigned long long* xbuf, int64_t region, int64_t buf_words, unsigned* cursors,
+                                unsigned* bar, unsigned* bar_flags, size_t smem, int sprobe, int grid, cudaStream_t s);

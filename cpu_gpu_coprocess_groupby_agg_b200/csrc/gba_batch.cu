@@ -731,6 +731,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
       e = gba_launch_exchange(xgroups[g].proto, d_qs, reinterpret_cast<const int*>(d + o_xq) + xgroups[g].xq_off,
                               int(xgroups[g].members.size()), xwin,
                               reinterpret_cast<unsigned long long*>(d + o_xbuf), xregion,
+                              int64_t(xgrid) * xregion * xstride,
                               reinterpret_cast<unsigned*>(d + o_xstat + 16),
                               reinterpret_cast<unsigned*>(d + o_xstat),
                               reinterpret_cast<unsigned*>(d + o_xstat + 8), xgroups[g].smem, sprobe, xgrid, cs);

@@ -22,7 +22,10 @@
 //               them to its shared table (stream_rows.cuh: the same probe and
 //               32-bit atomics as the streaming kernels; a key whose probe
 //               window is full goes to the query's HBM table).
-// Two exchange buffers alternate between windows, so the records of one
+// Two exchange buffers of buf_words words each alternate between windows
+// (buf_words holds grid regions of `region` records of the widest record any
+// phase writes: a buffer's rows of one window and the other buffer's partial
+// records never overlap), so the records of one
 // window are read while the next window's are written; a buffer of
 // win x record bytes stays in L2 between its writes and its reads, so the
 // rows cross HBM once.  After a query's last window every CTA writes the
@@ -85,7 +88,7 @@ __device__ bool grid_barrier(unsigned* count, unsigned* gen, unsigned nblocks, u
 template <bool K64, typename Sig>
 __global__ void __launch_bounds__(kXThreads, 1)
     k_exchange_agg(const BatchQ* qs, const int* xq, int nxq, int64_t win, unsigned long long* xbuf, int64_t region,
-                   unsigned* cursors, unsigned* bar, unsigned* bar_flags, int sprobe) {
+                   int64_t buf_words, unsigned* cursors, unsigned* bar, unsigned* bar_flags, int sprobe) {
   constexpr int NA = Sig::NA;
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ unsigned s_cnt[kXMaxGrid];
@@ -122,7 +125,7 @@ __global__ void __launch_bounds__(kXThreads, 1)
     const int64_t n = q.n;
     for (int64_t w0 = 0; w0 < n; w0 += win, ++wglob) {
       const int b = int(wglob & 1);
-      unsigned long long* buf = xbuf + size_t(b) * G * size_t(region) * stride;
+      unsigned long long* buf = xbuf + size_t(b) * size_t(buf_words);
       unsigned* cur = cursors + size_t(b) * G;
       // ---- A: route this CTA's slice of the window to the owners ----
       const int64_t we = w0 + win < n ? w0 + win : n;
@@ -229,7 +232,7 @@ __global__ void __launch_bounds__(kXThreads, 1)
       // ---- the hot tables' groups to their owners, as partial records ----
       const int b = int(wglob & 1);
       const int pstride = 1 + NA;
-      unsigned long long* buf = xbuf + size_t(b) * G * size_t(region) * pstride;
+      unsigned long long* buf = xbuf + size_t(b) * size_t(buf_words);
       unsigned* cur = cursors + size_t(b) * G;
       for (int i = tid; i <= hot; i += kXThreads) {
         uint64_t k;
@@ -359,8 +362,8 @@ int gba_exchange_grid(const QDesc& proto, size_t smem, int sms) {
 }
 
 cudaError_t gba_launch_exchange(const QDesc& proto, const BatchQ* d_qs, const int* d_xq, int nxq, int64_t win,
-                                unsigned long long* xbuf, int64_t region, unsigned* cursors, unsigned* bar,
-                                unsigned* bar_flags, size_t smem, int sprobe, int grid, cudaStream_t s) {
+                                unsigned long long* xbuf, int64_t region, int64_t buf_words, unsigned* cursors,
+                                unsigned* bar, unsigned* bar_flags, size_t smem, int sprobe, int grid, cudaStream_t s) {
   if (nxq <= 0) return cudaSuccess;
   if (grid < 1 || grid > kXMaxGrid || win > region) return cudaErrorInvalidValue;
   return gba_dispatch_sig(proto, [&](auto K, auto sig) -> cudaError_t {
@@ -375,6 +378,6 @@ cudaError_t gba_launch_exchange(const QDesc& proto, const BatchQ* d_qs, const in
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     return cudaLaunchKernelEx(&cfg, k_exchange_agg<decltype(K)::value, decltype(sig)>, d_qs, d_xq, nxq, win, xbuf,
-                              region, cursors, bar, bar_flags, sprobe);
+                              region, buf_words, cursors, bar, bar_flags, sprobe);
   });
 }
