@@ -106,6 +106,26 @@ extern "C" gba_status gba_groupby_partition_u32(gba_context* ctx, const uint32_t
 // C++ drop-ins
 namespace {
 
+// One merged partition's piece of the phase-1 output: `len` pairs at `src`
+// of the uploaded runs, to `dst` of the partition's own rows.
+struct SegCopy {
+  uint64_t src, dst;
+  uint64_t len;
+};
+
+// Gathers every segment of a merged partition into contiguous rows: one CTA
+// per segment at a time, 128-bit copies where both ends allow them.
+__global__ void k_gather_segments(const SegCopy* segs, int nseg, const uint32_t* src_k, const uint32_t* src_v,
+                                  uint32_t* dst_k, uint32_t* dst_v) {
+  for (int i = blockIdx.x; i < nseg; i += gridDim.x) {
+    const SegCopy c = segs[i];
+    for (uint64_t j = threadIdx.x; j < c.len; j += blockDim.x) {
+      dst_k[c.dst + j] = src_k[c.src + j];
+      dst_v[c.dst + j] = src_v[c.src + j];
+    }
+  }
+}
+
 // One host worker: a library context, a stream and device column buffers.
 struct TileWorker {
   gba_context* ctx = nullptr;
@@ -113,6 +133,11 @@ struct TileWorker {
   uint32_t* d_keys = nullptr;
   uint32_t* d_vals = nullptr;
   size_t cap = 0;
+  // phase 2: the uploaded phase-1 output (keys then values) and the segment list
+  uint32_t* d_runs = nullptr;
+  size_t runs_cap = 0;
+  SegCopy* d_segs = nullptr;
+  size_t segs_cap = 0;
   int device = 0;
 
   explicit TileWorker(int dev) : device(dev) {
@@ -128,6 +153,8 @@ struct TileWorker {
     if (s) cudaStreamSynchronize(s);
     if (d_keys) cudaFree(d_keys);
     if (d_vals) cudaFree(d_vals);
+    if (d_runs) cudaFree(d_runs);
+    if (d_segs) cudaFree(d_segs);
     if (s) cudaStreamDestroy(s);
     if (ctx) gba_destroy(ctx);
   }
@@ -143,6 +170,24 @@ struct TileWorker {
     cuda(cudaMalloc(&d_keys, std::max<size_t>(rows, 1) * 4), "cudaMalloc");
     cuda(cudaMalloc(&d_vals, std::max<size_t>(rows, 1) * 4), "cudaMalloc");
     cap = rows;
+  }
+  void reserve_runs(size_t pairs, size_t nseg) {
+    if (pairs > runs_cap) {
+      cuda(cudaStreamSynchronize(s), "sync");
+      if (d_runs) cudaFree(d_runs);
+      d_runs = nullptr;
+      runs_cap = 0;
+      cuda(cudaMalloc(&d_runs, std::max<size_t>(pairs, 1) * 8), "cudaMalloc");
+      runs_cap = pairs;
+    }
+    if (nseg > segs_cap) {
+      cuda(cudaStreamSynchronize(s), "sync");
+      if (d_segs) cudaFree(d_segs);
+      d_segs = nullptr;
+      segs_cap = 0;
+      cuda(cudaMalloc(&d_segs, std::max<size_t>(nseg, 1) * sizeof(SegCopy)), "cudaMalloc");
+      segs_cap = nseg;
+    }
   }
   static void cuda(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
@@ -329,25 +374,102 @@ void groupby_agg_intra_partition(std::vector<par_result>& par_result_vec, key_ty
                    "cudaMallocHost");
   TileWorker::cuda(cudaMallocHost(&host_agg_vals_result, std::max<size_t>(total, 1) * sizeof(val_type)),
                    "cudaMallocHost");
-  run_workers(nstreams, np, [&](TileWorker& w, size_t i) {
+  if (total == 0) return;
+
+  // Every segment (a tile's run of one partition) of every merged partition.
+  // Phase 1 left each tile's groups contiguous at the front of the tile's own
+  // range, so the segments sorted by address join into a few contiguous runs
+  // (about one per tile); each run is copied to the device once, and each
+  // merged partition is gathered there by one kernel.  (One host-to-device
+  // copy per segment, thousands of them, had made phase 2 slower than the
+  // reference, which gathers them on the host.)
+  struct Seg {
+    const key_type* k;
+    const val_type* v;
+    uint64_t len;
+    size_t part;
+    uint64_t dst;  // offset in the partition's gathered rows
+    uint64_t src;  // offset in the uploaded runs
+  };
+  std::vector<Seg> segs;
+  for (size_t i = 0; i < np; ++i) {
     const par_result& pr = par_result_vec[i];
-    w.reserve(pr.size);
-    size_t at = 0;
-    for (size_t sgm = 0; sgm < pr.key.size(); ++sgm) {
-      const size_t len = pr.end_indicator[sgm];
+    uint64_t at = 0;
+    for (size_t sg = 0; sg < pr.key.size(); ++sg) {
+      const uint64_t len = pr.end_indicator[sg];
       if (!len) continue;
-      TileWorker::cuda(cudaMemcpyAsync(w.d_keys + at, pr.key[sgm], len * 4, cudaMemcpyHostToDevice, w.s), "H2D");
-      TileWorker::cuda(cudaMemcpyAsync(w.d_vals + at, pr.val[sgm], len * 4, cudaMemcpyHostToDevice, w.s), "H2D");
+      segs.push_back(Seg{pr.key[sg], pr.val[sg], len, i, at, 0});
       at += len;
     }
-    uint64_t o[2];
-    w.group_partition(at, 1, o);
-    const size_t g = o[1];
-    TileWorker::cuda(cudaMemcpyAsync(host_groupby_keys_result + par_kv_begin[i], w.d_keys, g * 4,
-                                     cudaMemcpyDeviceToHost, w.s), "D2H");
-    TileWorker::cuda(cudaMemcpyAsync(host_agg_vals_result + par_kv_begin[i], w.d_vals, g * 4,
-                                     cudaMemcpyDeviceToHost, w.s), "D2H");
+  }
+  std::vector<size_t> order(segs.size());
+  for (size_t i = 0; i < order.size(); ++i) order[i] = i;
+  std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return segs[a].k < segs[b].k; });
+  struct Run {
+    const key_type* k;
+    const val_type* v;
+    uint64_t len, off;
+  };
+  std::vector<Run> runs;
+  uint64_t up = 0;
+  for (size_t oi : order) {
+    Seg& g = segs[oi];
+    if (!runs.empty()) {
+      Run& r = runs.back();
+      if (g.k == r.k + r.len && g.v == r.v + r.len) {  // continues the run
+        g.src = r.off + r.len;
+        r.len += g.len;
+        up += g.len;
+        continue;
+      }
+      if (g.k >= r.k && g.k + g.len <= r.k + r.len && g.v == r.v + (g.k - r.k)) {  // inside the run
+        g.src = r.off + uint64_t(g.k - r.k);
+        continue;
+      }
+    }
+    g.src = up;
+    runs.push_back(Run{g.k, g.v, g.len, up});
+    up += g.len;
+  }
+  // per merged partition, its segment copies (in segment order)
+  std::vector<SegCopy> copies(segs.size());
+  std::vector<size_t> first(np + 1, 0);
+  for (const Seg& g : segs) ++first[g.part + 1];
+  for (size_t i = 0; i < np; ++i) first[i + 1] += first[i];
+  {
+    std::vector<size_t> fill(first.begin(), first.end() - 1);
+    for (const Seg& g : segs) copies[fill[g.part]++] = SegCopy{g.src, g.dst, g.len};
+  }
+  size_t maxpart = 0;
+  for (size_t i = 0; i < np; ++i) maxpart = std::max<size_t>(maxpart, par_result_vec[i].size);
+
+  run_workers(1, 1, [&](TileWorker& w, size_t) {
+    w.reserve_runs(up, copies.size());
+    w.reserve(maxpart);
+    uint32_t* rk = w.d_runs;
+    uint32_t* rv = w.d_runs + up;
+    for (const Run& r : runs) {
+      TileWorker::cuda(cudaMemcpyAsync(rk + r.off, r.k, r.len * 4, cudaMemcpyHostToDevice, w.s), "H2D");
+      TileWorker::cuda(cudaMemcpyAsync(rv + r.off, r.v, r.len * 4, cudaMemcpyHostToDevice, w.s), "H2D");
+    }
+    TileWorker::cuda(cudaMemcpyAsync(w.d_segs, copies.data(), copies.size() * sizeof(SegCopy),
+                                     cudaMemcpyHostToDevice, w.s), "H2D");
+    for (size_t i = 0; i < np; ++i) {
+      const int nseg = int(first[i + 1] - first[i]);
+      if (nseg > 0) {
+        k_gather_segments<<<std::min(nseg, 4 * w.ctx->sms), 256, 0, w.s>>>(w.d_segs + first[i], nseg, rk, rv,
+                                                                          w.d_keys, w.d_vals);
+        TileWorker::cuda(cudaGetLastError(), "gather");
+      }
+      uint64_t o[2];
+      w.group_partition(par_result_vec[i].size, 1, o);
+      const size_t g = o[1];
+      TileWorker::cuda(cudaMemcpyAsync(host_groupby_keys_result + par_kv_begin[i], w.d_keys, g * 4,
+                                       cudaMemcpyDeviceToHost, w.s), "D2H");
+      TileWorker::cuda(cudaMemcpyAsync(host_agg_vals_result + par_kv_begin[i], w.d_vals, g * 4,
+                                       cudaMemcpyDeviceToHost, w.s), "D2H");
+      par_result_kv_num[i] = g;
+    }
     TileWorker::cuda(cudaStreamSynchronize(w.s), "sync");
-    par_result_kv_num[i] = g;
   });
 }

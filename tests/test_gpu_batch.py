@@ -189,3 +189,21 @@ def test_batch_owner_exchange_windows_and_overflow(ctx):
         qs.append((keys, cols, aggs))
     for knobs in (dict(exchange=1), dict(sizing="learned"), dict(sizing="learned", exchange=0)):
         _check(qs, ctx.groupby_batch(_device(qs), knobs=knobs), f"exchange {knobs}")
+
+
+def test_batch_owner_exchange_on_the_batch_class_256_4096(ctx):
+    """The 86 queries of the benchmark batch with 256 to 4095 distinct ids
+    (Zipf s in [0, 1.5]), every one forced through the owner-exchange kernel
+    with hot tables where the sample is skewed: the case that once exposed
+    hot-table partial records written over the other exchange buffer."""
+    import torch
+    from cpu_gpu_coprocess_groupby_agg_b200 import gen_device, workloads as W
+    assert E.load_default(ctx), "committed estimator weights are missing"
+    allq = [q for q in W.batch_queries() if 256 <= q.meta["ndv"] < 4096]
+    dq = [(*gen_device(q.spec, q.n), q.aggs) for q in allq]
+    res = ctx.groupby_batch(dq, knobs=dict(sizing="learned", exchange=1))
+    for q, (k, c, _), r in zip(allq, dq, res):
+        order = torch.argsort(r.keys)
+        gk = r.keys[order].cpu().numpy()
+        ga = [a[order].cpu().numpy() for a in r.aggs]
+        compare(gk, ga, k.cpu().numpy(), [x.cpu().numpy() for x in c], q.aggs, label=q.name, presorted=True)
