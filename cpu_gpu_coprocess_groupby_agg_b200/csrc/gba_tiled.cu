@@ -19,6 +19,9 @@
 // with another tile's aggregation.
 #include <algorithm>
 #include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <exception>
 #include <map>
 #include <mutex>
@@ -237,6 +240,12 @@ class WorkerPool {
   std::map<int, std::vector<TileWorker*>> free_;
 };
 
+int dev_of_call() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  return dev;
+}
+
 // Runs fn(worker, item) for items [0, count) over `nw` workers; rethrows the
 // first error after every worker stopped.
 template <typename Fn>
@@ -443,22 +452,35 @@ void groupby_agg_intra_partition(std::vector<par_result>& par_result_vec, key_ty
   size_t maxpart = 0;
   for (size_t i = 0; i < np; ++i) maxpart = std::max<size_t>(maxpart, par_result_vec[i].size);
 
-  run_workers(1, 1, [&](TileWorker& w, size_t) {
-    w.reserve_runs(up, copies.size());
-    w.reserve(maxpart);
-    uint32_t* rk = w.d_runs;
-    uint32_t* rv = w.d_runs + up;
+  // The runs and the segment list go up once, on the first worker's stream;
+  // then the workers take merged partitions in turn, each gathering its
+  // partition from the shared runs into its own buffers, aggregating it and
+  // copying its groups back.
+  const bool trace = std::getenv("GBA_TRACE") != nullptr;
+  const auto t0 = std::chrono::steady_clock::now();
+  TileWorker* up_w = WorkerPool::get().acquire(dev_of_call());
+  cudaEvent_t uploaded = nullptr;
+  try {
+    up_w->reserve_runs(up, copies.size());
     for (const Run& r : runs) {
-      TileWorker::cuda(cudaMemcpyAsync(rk + r.off, r.k, r.len * 4, cudaMemcpyHostToDevice, w.s), "H2D");
-      TileWorker::cuda(cudaMemcpyAsync(rv + r.off, r.v, r.len * 4, cudaMemcpyHostToDevice, w.s), "H2D");
+      TileWorker::cuda(cudaMemcpyAsync(up_w->d_runs + r.off, r.k, r.len * 4, cudaMemcpyHostToDevice, up_w->s), "H2D");
+      TileWorker::cuda(cudaMemcpyAsync(up_w->d_runs + up + r.off, r.v, r.len * 4, cudaMemcpyHostToDevice, up_w->s),
+                       "H2D");
     }
-    TileWorker::cuda(cudaMemcpyAsync(w.d_segs, copies.data(), copies.size() * sizeof(SegCopy),
-                                     cudaMemcpyHostToDevice, w.s), "H2D");
-    for (size_t i = 0; i < np; ++i) {
+    TileWorker::cuda(cudaMemcpyAsync(up_w->d_segs, copies.data(), copies.size() * sizeof(SegCopy),
+                                     cudaMemcpyHostToDevice, up_w->s), "H2D");
+    TileWorker::cuda(cudaEventCreateWithFlags(&uploaded, cudaEventDisableTiming), "event");
+    TileWorker::cuda(cudaEventRecord(uploaded, up_w->s), "event");
+    const uint32_t* rk = up_w->d_runs;
+    const uint32_t* rv = up_w->d_runs + up;
+    const SegCopy* dsegs = up_w->d_segs;
+    run_workers(nstreams, np, [&](TileWorker& w, size_t i) {
+      TileWorker::cuda(cudaStreamWaitEvent(w.s, uploaded, 0), "wait");
+      w.reserve(par_result_vec[i].size);
       const int nseg = int(first[i + 1] - first[i]);
       if (nseg > 0) {
-        k_gather_segments<<<std::min(nseg, 4 * w.ctx->sms), 256, 0, w.s>>>(w.d_segs + first[i], nseg, rk, rv,
-                                                                          w.d_keys, w.d_vals);
+        k_gather_segments<<<std::min(nseg, 4 * w.ctx->sms), 256, 0, w.s>>>(dsegs + first[i], nseg, rk, rv, w.d_keys,
+                                                                          w.d_vals);
         TileWorker::cuda(cudaGetLastError(), "gather");
       }
       uint64_t o[2];
@@ -468,8 +490,20 @@ void groupby_agg_intra_partition(std::vector<par_result>& par_result_vec, key_ty
                                        cudaMemcpyDeviceToHost, w.s), "D2H");
       TileWorker::cuda(cudaMemcpyAsync(host_agg_vals_result + par_kv_begin[i], w.d_vals, g * 4,
                                        cudaMemcpyDeviceToHost, w.s), "D2H");
+      TileWorker::cuda(cudaStreamSynchronize(w.s), "sync");
       par_result_kv_num[i] = g;
-    }
-    TileWorker::cuda(cudaStreamSynchronize(w.s), "sync");
-  });
+    });
+  } catch (...) {
+    if (uploaded) cudaEventDestroy(uploaded);
+    cudaStreamSynchronize(up_w->s);
+    WorkerPool::get().release(up_w);
+    throw;
+  }
+  cudaEventDestroy(uploaded);
+  cudaStreamSynchronize(up_w->s);
+  WorkerPool::get().release(up_w);
+  if (trace)
+    std::fprintf(stderr, "groupby_agg_intra_partition: %zu merged partitions, %zu runs, %zu segments, %.3f ms\n", np,
+                 runs.size(), segs.size(),
+                 std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
 }
