@@ -492,7 +492,9 @@ def run_batch(args, ws, rank, local, pg):
                    "knobs_from": "gba_autotune on this batch before timing" if tuned[args.sizing][1] is not None
                    else "defaults / --knob"},
         "whole_step_hbm_gbs": round(in_bytes / (ms_step / 1e3) / 1e9, 1),
-        "roofline": {"bound": "hbm", "kernel": "k_stream_agg (+ k_part_agg of partition-strategy queries)",
+        "roofline": {"bound": "hbm",
+                     "kernel": "k_stream_agg + k_stream_tma (the batch's streaming launches; + k_part_agg of "
+                               "partition-strategy queries)",
                      "achieved": round(achieved, 1) if achieved else None, "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4) if achieved else None, "peak_kind": peak_kind,
                      "traffic": traffic, "alg_bytes_per_step": int(main_bytes), "launch_ms": round(main_ms, 4)},

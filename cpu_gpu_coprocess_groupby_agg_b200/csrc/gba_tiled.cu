@@ -90,8 +90,13 @@ extern "C" gba_status gba_groupby_partition_u32(gba_context* ctx, const uint32_t
   o.aggs[0] = g_sums;
   o.capacity = int64_t(cap);
   int64_t g = 0;
+  const auto t0 = std::chrono::steady_clock::now();
   st = gba_groupby(ctx, &q, &o, nullptr, stream, &g);
   if (st != GBA_OK) return st;
+  if (std::getenv("GBA_TRACE"))
+    std::fprintf(stderr, "gba_groupby_partition_u32: %lld rows, %lld groups, strategy %d, %lld slots, %.3f ms\n",
+                 (long long)n_rows, (long long)g, ctx->stats.strategy, (long long)ctx->stats.table_slots,
+                 std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
   unsigned long long* offs = reinterpret_cast<unsigned long long*>(b + o_offs);
   GBA_CUDA_TRY(ctx, gba_launch_refpart(g_keys, g_sums, g, P, out_keys, out_vals, reinterpret_cast<unsigned*>(b + o_hist),
                                        offs, reinterpret_cast<unsigned long long*>(b + o_cur), ctx->sms, s));
