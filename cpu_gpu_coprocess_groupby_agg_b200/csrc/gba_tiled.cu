@@ -372,6 +372,8 @@ void groupby_agg_intra_partition(std::vector<par_result>& par_result_vec, key_ty
   (void)Capacity;
   (void)max_load_num;
   if (par_result_vec.empty()) throw std::invalid_argument("groupby_agg_intra_partition: no partitions");
+  const bool trace = std::getenv("GBA_TRACE") != nullptr;
+  const auto t_in = std::chrono::steady_clock::now();
   par_result_vec = merge_partitions(par_result_vec, min_load_num);
   const size_t np = par_result_vec.size();
   par_kv_begin.clear();
@@ -388,6 +390,9 @@ void groupby_agg_intra_partition(std::vector<par_result>& par_result_vec, key_ty
                    "cudaMallocHost");
   TileWorker::cuda(cudaMallocHost(&host_agg_vals_result, std::max<size_t>(total, 1) * sizeof(val_type)),
                    "cudaMallocHost");
+  if (trace)
+    std::fprintf(stderr, "groupby_agg_intra_partition: merge and pinned result arrays (%zu pairs): %.3f ms\n", total,
+                 std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_in).count());
   if (total == 0) return;
 
   // Every segment (a tile's run of one partition) of every merged partition.
@@ -461,7 +466,6 @@ void groupby_agg_intra_partition(std::vector<par_result>& par_result_vec, key_ty
   // then the workers take merged partitions in turn, each gathering its
   // partition from the shared runs into its own buffers, aggregating it and
   // copying its groups back.
-  const bool trace = std::getenv("GBA_TRACE") != nullptr;
   const auto t0 = std::chrono::steady_clock::now();
   TileWorker* up_w = WorkerPool::get().acquire(dev_of_call());
   cudaEvent_t uploaded = nullptr;

@@ -4,8 +4,9 @@
 // No counterpart in the reference: it sizes every table from the tile length
 // (Capacity = tile_len, test/test.cu:104) and never estimates group counts.
 //
-// Features of one query (32 floats), from a strided sample of up to 1024 rows
-// in each of up to 256 evenly spaced tiles of `tile_rows` rows:
+// Features of one query (32 floats), from a sample of up to 1024 rows (128
+// evenly spaced runs of 8 rows) in each of up to 256 evenly spaced tiles of
+// `tile_rows` rows:
 //   0 log2(n+1)/32          1 log2(s+1)/32 (s = sampled rows)
 //   2 d/s (d = distinct sampled keys)   3..6 f1/s, f2/s, f3/s, f4+/s
 //   7 log2(d+1)/32          8 log2(GEE+1)/32, GEE = sqrt(n/s) f1 + (d - f1)
@@ -37,7 +38,12 @@ constexpr int OW1 = 0, OB1 = OW1 + H * F, OW2 = OB1 + H, OB2 = OW2 + H * H, OW3 
               OW4 = OB3 + H, OB4 = OW4 + H, NPARAM = OB4 + 1;
 
 __device__ __forceinline__ uint64_t sample_row(const EstQuery& e, int64_t item) {
-  // item = sampled tile * 1024 + j; rows j*stride inside the tile
+  // item = sampled tile * 1024 + j: the tile's 1024 sampled rows are 128 runs
+  // of 8 consecutive rows at evenly spaced positions (run j / 8 starts at
+  // (j / 8) * len / 128).  A run of 8 keys fills whole 32-byte sectors (one
+  // row per position had spent a sector on every 4- or 8-byte key), and 128
+  // positions still spread the sample over the tile: a column that repeats
+  // with a period shows its every value (runs of 32 at 32 positions did not)
   const int64_t st = item >> 10, j = item & 1023;
   const int64_t tile = st * e.tile_step;
   const int64_t tb = tile * e.tile_rows;
@@ -45,7 +51,7 @@ __device__ __forceinline__ uint64_t sample_row(const EstQuery& e, int64_t item) 
   const int64_t len = te - tb;
   if (len <= 0) return ~0ull;
   if (len <= 1024) return j < len ? uint64_t(tb + j) : ~0ull;
-  return uint64_t(tb + j * (len / 1024));
+  return uint64_t(tb + (j >> 3) * (len / 128) + (j & 7));
 }
 
 // every query's count table to {empty key, 0} (blockIdx.y = query)
