@@ -696,10 +696,20 @@ def run_serve(args, ws, rank, local, pg):
             raise SystemExit(f"serving: {len(bad)} requests failed, first status {bad[0].status}: {err}")
         lat = np.array([x.latency_ms + lag for x, _, lag in infos])
         rows = sum(n for _, n, _ in infos)
+        big = np.array([n >= (1 << 27) for _, n, _ in infos])
+        svc = np.array([x.service_ms for x, _, _ in infos])
+
+        def pct(a, q):
+            return round(float(np.percentile(a, q)), 3) if len(a) else None
         return {"value": round(rows / (t_end - t0) / 1e9, 4), "unit": "G rows/s", "requests": len(infos),
+                "last_error": err,
                 "seconds": round(t_end - t0, 3), "offered_seconds": round(float(np.sum(gaps)), 3),
                 "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
-                "mean_batch": round(float(np.mean([x.batch_size for x, _, _ in infos])), 2)}
+                "mean_batch": round(float(np.mean([x.batch_size for x, _, _ in infos])), 2),
+                "large_requests": {"count": int(big.sum()), "p50_ms": pct(lat[big], 50), "p99_ms": pct(lat[big], 99),
+                                   "service_p50_ms": pct(svc[big], 50)},
+                "small_requests": {"count": int((~big).sum()), "p50_ms": pct(lat[~big], 50),
+                                   "p99_ms": pct(lat[~big], 99), "service_p50_ms": pct(svc[~big], 50)}}
 
     learned = one_run("learned", 5)
     plain = one_run("plain", 5)

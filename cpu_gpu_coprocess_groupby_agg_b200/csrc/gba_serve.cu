@@ -66,7 +66,8 @@ struct gba_server {
   int64_t submitted = 0, finished = 0;
   bool stop = false;
   gba_context* admin = nullptr;  // validates queries at submit (under mu)
-  std::string last_failure;      // message of the latest failed request
+  std::string last_failure;      // message of the latest failed request (or failed batch)
+  int64_t batch_failures = 0;    // batch calls that failed and were rerun request by request
 };
 
 static int64_t ctx_resident_bytes(const gba_context* c) {
@@ -146,6 +147,12 @@ static void lane_main(gba_server* sv, int lane) {
           take[i]->info.n_groups = ng[i];
         }
       } else {
+        {
+          std::lock_guard<std::mutex> lk(sv->mu);
+          ++sv->batch_failures;
+          sv->last_failure = "lane " + std::to_string(lane) + ": a batch of " + std::to_string(nb) + " failed (" +
+                             gba_status_string(st) + ": " + ctx->err + "); its requests ran one by one";
+        }
         for (int i = 0; i < nb; ++i) {  // attribute the failure
           int64_t g = 0;
           take[i]->info.status = gba_groupby(ctx, &take[i]->q, &take[i]->out, &sv->cfg.knobs, s, &g);
