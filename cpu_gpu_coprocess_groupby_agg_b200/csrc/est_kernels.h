@@ -15,6 +15,8 @@ struct EstQuery {
   int64_t tile_step;    // sample every tile_step-th tile
   int sampled_tiles;
   int key64;
+  int64_t chunk_base;         // first sampling block of this query (k_est_sample's grid is flat)
+  int nchunks;                // sampling blocks of this query: kEstChunkTiles sampled tiles each
   unsigned long long* table;  // cap x {key, count}
   uint64_t cap;
   unsigned* hll;              // 64 registers
@@ -26,6 +28,8 @@ struct EstQuery {
 void gba_est_plan(EstQuery* e, int64_t n, int64_t tile_rows);
 int64_t gba_est_nparam();
 cudaError_t gba_launch_est_init(const EstQuery* d_qs, int nq, cudaStream_t s);
-cudaError_t gba_launch_est_sample(const EstQuery* d_qs, int nq, int64_t max_items, cudaStream_t s);
+// sampled tiles per block of k_est_sample
+#define GBA_EST_CHUNK_TILES 4
+cudaError_t gba_launch_est_sample(const EstQuery* d_qs, int nq, int64_t total_chunks, cudaStream_t s);
 cudaError_t gba_launch_est_reduce(const EstQuery* d_qs, int nq, cudaStream_t s);
 cudaError_t gba_launch_mlp_forward(const float* W, const float* X, int n, float* out, cudaStream_t s);

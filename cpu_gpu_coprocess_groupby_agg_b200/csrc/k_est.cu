@@ -70,82 +70,151 @@ __global__ void k_est_init(const EstQuery* qs, int nq) {
 // class min(c, 4) and enters class min(c + m, 4) (classes 1, 2, 3, 4+), and
 // c == 0 makes it a new distinct key.  Whatever order the increments run in,
 // the totals end exact, so the sample's frequency profile needs no scan of
-// the count table afterwards.  f[0] distinct, f[1..4] f1..f4+, f[5] max count,
-// f[6] sampled rows (block-local shared counters, flushed once per query).
-__device__ __forceinline__ void freq_step(unsigned long long* f, unsigned long long old, unsigned long long m) {
+// the count table afterwards.  A thread keeps its own signed deltas
+// (d[0] distinct, d[1..4] f1..f4+) and maximum; they are summed per warp and
+// per block before they reach the query's counters.
+struct FreqAcc {
+  int d[5];
+  unsigned mx;
+  unsigned rows;
+};
+
+__device__ __forceinline__ void freq_step(FreqAcc& f, unsigned long long old, unsigned m) {
   const unsigned long long nw = old + m;
-  const unsigned long long co = old < 4 ? old : 4, cn = nw < 4 ? nw : 4;
-  if (old == 0) atomicAdd(&f[0], 1ull);
-  if (co != cn) {
-    if (co) atomicAdd(&f[co], ~0ull);  // -1
-    atomicAdd(&f[cn], 1ull);
-  }
-  atomicMax(&f[5], nw);
-  atomicAdd(&f[6], m);
+  const int co = old < 4 ? int(old) : 4, cn = nw < 4 ? int(nw) : 4;
+  if (old == 0) f.d[0] += 1;
+#pragma unroll
+  for (int c = 1; c <= 4; ++c) f.d[c] += (c == cn) - (c == co);
+  const unsigned nw32 = nw < 0xffffffffull ? unsigned(nw) : 0xffffffffu;
+  f.mx = f.mx > nw32 ? f.mx : nw32;
+  f.rows += m;
 }
 
-// one thread per sampled row; per-query count table (keys + counts, linear
-// probing, capacity 1.5x the sample), 64 HLL registers and the frequency
-// classes.  Lanes of a warp holding the same key add their rows with one
-// atomic from the lowest of them (a skewed column's hot key would otherwise
-// serialise thousands of atomics on one counter).
-__global__ void k_est_sample(const EstQuery* qs, int nq) {
+// First insert of a sampled key into its query's count table (linear
+// probing from slot s); returns the key's count before this one's m rows.
+__device__ __noinline__ unsigned long long est_count_insert(unsigned long long* table, uint64_t cap, uint64_t k,
+                                                            uint64_t s, unsigned m) {
+  for (uint64_t p = 0; p < cap; ++p) {
+    unsigned long long* slot = table + 2 * s;
+    const unsigned long long cur = __ldcg(slot);
+    if (cur == k) return atomicAdd(slot + 1, (unsigned long long)m);
+    if (cur == EMPTY64) {
+      const unsigned long long prev = atomicCAS(slot, EMPTY64, k);
+      if (prev == EMPTY64 || prev == k) return atomicAdd(slot + 1, (unsigned long long)m);
+    }
+    s = s + 1 == cap ? 0 : s + 1;
+  }
+  return 0ull;  // unreachable: the table holds 1.5x the sample
+}
+
+// One block per chunk of GBA_EST_CHUNK_TILES sampled tiles of one query (a
+// flat grid over every query's chunks).  Per sampled row: the 64 HLL
+// registers (block-local, merged once), and the query's count table (keys +
+// counts, linear probing, capacity 1.5x the sample).  Lanes of a warp
+// holding the same key add their rows with one atomic from the lowest of
+// them (a skewed column's hot key would otherwise serialise thousands of
+// atomics on one counter).  A thread works on kEstU rows at a time, each
+// step's loads and atomics issued before any result is used.
+constexpr int kEstThreads = 256;
+constexpr int kEstU = 4;
+__global__ void __launch_bounds__(kEstThreads) k_est_sample(const EstQuery* qs, int nq) {
   __shared__ unsigned long long sf[7];
-  for (int qi = blockIdx.y; qi < nq; qi += gridDim.y) {
-    const EstQuery e = qs[qi];
-    if (threadIdx.x < 7) sf[threadIdx.x] = 0ull;
-    __syncthreads();
-    const int64_t items = int64_t(e.sampled_tiles) << 10;
-    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    // whole warps iterate together (for __match_any_sync)
-    for (int64_t base = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) & ~int64_t(31); base < items;
-         base += stride) {
-      const int64_t it = base + lane_id();
-      const uint64_t r = it < items ? sample_row(e, it) : ~0ull;
-      const bool live = r != ~0ull;
-      uint64_t k = 0;
-      if (live) {
-        k = e.key64 ? static_cast<const unsigned long long*>(e.keys)[r] : static_cast<const unsigned*>(e.keys)[r];
-        const uint32_t h = e.key64 ? murmur3_64(k, 0x5bd1e995u) : murmur3_32(uint32_t(k), 0x5bd1e995u);
+  __shared__ unsigned s_hll[64];
+  int lo = 0, hi = nq - 1;
+  while (lo < hi) {  // last query whose first block is at or before this one
+    const int mid = (lo + hi + 1) >> 1;
+    if (qs[mid].chunk_base <= int64_t(blockIdx.x)) lo = mid;
+    else hi = mid - 1;
+  }
+  const EstQuery e = qs[lo];
+  const int64_t chunk = int64_t(blockIdx.x) - e.chunk_base;
+  if (chunk >= e.nchunks) return;  // past the last query's blocks (block-uniform)
+  if (threadIdx.x < 7) sf[threadIdx.x] = 0ull;
+  if (threadIdx.x < 64) s_hll[threadIdx.x] = 0u;
+  __syncthreads();
+  const int64_t items = int64_t(e.sampled_tiles) << 10;
+  const int64_t c0 = chunk * (int64_t(GBA_EST_CHUNK_TILES) << 10);
+  const int64_t c1 = c0 + (int64_t(GBA_EST_CHUNK_TILES) << 10) < items ? c0 + (int64_t(GBA_EST_CHUNK_TILES) << 10) : items;
+  FreqAcc f;
+#pragma unroll
+  for (int c = 0; c < 5; ++c) f.d[c] = 0;
+  f.mx = 0u;
+  f.rows = 0u;
+  unsigned long long ones = 0ull;  // rows of the all-ones key (64-bit keys only)
+  // every thread runs the same number of steps (whole warps, for __match_any_sync)
+  for (int64_t base = c0; base < c1; base += int64_t(kEstThreads) * kEstU) {
+    uint64_t k[kEstU];
+    bool live[kEstU];
+#pragma unroll
+    for (int u = 0; u < kEstU; ++u) {
+      const int64_t it = base + int64_t(u) * kEstThreads + threadIdx.x;
+      const uint64_t r = it < c1 ? sample_row(e, it) : ~0ull;
+      live[u] = r != ~0ull;
+      k[u] = 0;
+      if (live[u])
+        k[u] = e.key64 ? __ldcs(static_cast<const unsigned long long*>(e.keys) + r)
+                       : __ldcs(static_cast<const unsigned*>(e.keys) + r);
+    }
+    unsigned m[kEstU];
+    uint64_t s[kEstU];
+    unsigned long long cur[kEstU];
+#pragma unroll
+    for (int u = 0; u < kEstU; ++u) {
+      if (live[u]) {
+        const uint32_t h = e.key64 ? murmur3_64(k[u], 0x5bd1e995u) : murmur3_32(uint32_t(k[u]), 0x5bd1e995u);
         // HLL: the top 6 bits select the register, the rank of the first set
         // bit among the remaining 26 is its candidate value
-        const unsigned reg = h >> 26;
-        const unsigned rank = __clz((h << 6) | (1u << 5)) + 1;
-        if (rank > __ldcg(&e.hll[reg])) atomicMax(&e.hll[reg], rank);
+        atomicMax(&s_hll[h >> 26], unsigned(__clz((h << 6) | (1u << 5)) + 1));
       }
-      const unsigned live_mask = __ballot_sync(GBA_FULL_MASK, live);
-      const unsigned peers = __match_any_sync(GBA_FULL_MASK, live ? k : ~0ull) & live_mask;
-      if (!live || (peers & ((1u << lane_id()) - 1u))) continue;  // not the group's lowest lane
-      const unsigned long long m = __popc(peers);
-      if (k == EMPTY64) {  // the table's empty marker (only a 64-bit key can equal it)
-        freq_step(sf, atomicAdd(&e.stats[3], m), m);
+      const unsigned live_mask = __ballot_sync(GBA_FULL_MASK, live[u]);
+      const unsigned peers = __match_any_sync(GBA_FULL_MASK, live[u] ? k[u] : ~0ull) & live_mask;
+      // the group's lowest lane carries its m rows; the others drop out
+      m[u] = (live[u] && !(peers & ((1u << lane_id()) - 1u))) ? unsigned(__popc(peers)) : 0u;
+      s[u] = 0;
+      cur[u] = EMPTY64;
+      if (m[u] && k[u] != EMPTY64) {
+        s[u] = (uint64_t(table_hash(k[u])) * e.cap) >> 32;
+        cur[u] = __ldcg(e.table + 2 * s[u]);
+      }
+    }
+    unsigned long long old[kEstU];
+#pragma unroll
+    for (int u = 0; u < kEstU; ++u) {
+      old[u] = 0ull;
+      if (m[u] && k[u] != EMPTY64 && cur[u] == k[u]) old[u] = atomicAdd(e.table + 2 * s[u] + 1, (unsigned long long)m[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < kEstU; ++u) {
+      if (!m[u]) continue;
+      if (k[u] == EMPTY64) {  // the table's empty marker (only a 64-bit key can equal it)
+        ones += m[u];
         continue;
       }
-      uint64_t s = (uint64_t(table_hash(k)) * e.cap) >> 32;
-      for (uint64_t p = 0; p < e.cap; ++p) {
-        unsigned long long* slot = e.table + 2 * s;
-        const unsigned long long cur = __ldcg(slot);
-        if (cur == k) {
-          freq_step(sf, atomicAdd(slot + 1, m), m);
-          break;
-        }
-        if (cur == EMPTY64) {
-          const unsigned long long prev = atomicCAS(slot, EMPTY64, k);
-          if (prev == EMPTY64 || prev == k) {
-            freq_step(sf, atomicAdd(slot + 1, m), m);
-            break;
-          }
-        }
-        s = s + 1 == e.cap ? 0 : s + 1;
-      }
+      if (cur[u] != k[u]) old[u] = est_count_insert(e.table, e.cap, k[u], s[u], m[u]);
+      freq_step(f, old[u], m[u]);
     }
-    __syncthreads();
-    if (threadIdx.x < 7 && sf[threadIdx.x] != 0ull) {
-      if (threadIdx.x == 5) atomicMax(&e.freq[5], sf[5]);
-      else atomicAdd(&e.freq[threadIdx.x], sf[threadIdx.x]);
-    }
-    __syncthreads();
   }
+  // the all-ones key's count: its old value decides its frequency class, so it
+  // takes one atomic per thread that saw it
+  if (ones) freq_step(f, atomicAdd(&e.stats[3], ones), unsigned(ones));
+  // warp sums, then one shared update per warp
+#pragma unroll
+  for (int c = 0; c < 5; ++c) f.d[c] = __reduce_add_sync(GBA_FULL_MASK, f.d[c]);
+  f.mx = __reduce_max_sync(GBA_FULL_MASK, f.mx);
+  f.rows = __reduce_add_sync(GBA_FULL_MASK, f.rows);
+  if (lane_id() == 0) {
+#pragma unroll
+    for (int c = 0; c < 5; ++c)
+      if (f.d[c]) atomicAdd(&sf[c], (unsigned long long)(long long)f.d[c]);
+    if (f.mx) atomicMax(&sf[5], (unsigned long long)f.mx);
+    if (f.rows) atomicAdd(&sf[6], (unsigned long long)f.rows);
+  }
+  __syncthreads();
+  if (threadIdx.x < 7 && sf[threadIdx.x] != 0ull) {
+    if (threadIdx.x == 5) atomicMax(&e.freq[5], sf[5]);
+    else atomicAdd(&e.freq[threadIdx.x], sf[threadIdx.x]);
+  }
+  if (threadIdx.x < 64 && s_hll[threadIdx.x] > __ldcg(&e.hll[threadIdx.x])) atomicMax(&e.hll[threadIdx.x], s_hll[threadIdx.x]);
 }
 
 // per query (one thread each): frequency profile and HLL registers -> the 32
@@ -374,13 +443,13 @@ size_t train_smem() { return sizeof(float) * (size_t(kTrainB) * (F + 5 * H) + kT
 
 // ---------------------------------------------------------------------------
 // launchers
-cudaError_t gba_launch_est_sample(const EstQuery* d_qs, int nq, int64_t max_items, cudaStream_t s) {
-  // up to 16 sampled rows per thread: with one row per thread, the largest
-  // query set the grid's width and the many small queries of a batch left
-  // most of their blocks empty (hundreds of thousands of idle blocks)
-  const int gx = int(std::min<int64_t>((max_items + 256 * 16 - 1) / (256 * 16), 64));
-  dim3 grid(std::max(gx, 1), std::min(nq, 65535));
-  k_est_sample<<<grid, 256, 0, s>>>(d_qs, nq);
+cudaError_t gba_launch_est_sample(const EstQuery* d_qs, int nq, int64_t total_chunks, cudaStream_t s) {
+  // a flat grid: one block per chunk of GBA_EST_CHUNK_TILES sampled tiles of
+  // a query, so every query gets as many blocks as its sample needs (a grid
+  // of queries x the largest query's blocks left most blocks empty)
+  if (nq <= 0 || total_chunks <= 0) return cudaSuccess;
+  if (total_chunks > int64_t(0x7fffffff)) return cudaErrorInvalidValue;
+  k_est_sample<<<unsigned(total_chunks), kEstThreads, 0, s>>>(d_qs, nq);
   return cudaGetLastError();
 }
 cudaError_t gba_launch_est_init(const EstQuery* d_qs, int nq, cudaStream_t s) {
@@ -580,11 +649,13 @@ gba_status gba_est_features_device(gba_context* ctx, const QDesc* qs, int nq, in
   const size_t o_h = take(4 * 64 * size_t(nq));
   const size_t o_fr = take(8 * 8 * size_t(nq));
   std::vector<size_t> o_t(nq);
-  int64_t max_items = 0;
+  int64_t chunks = 0;
   for (int i = 0; i < nq; ++i) {
     gba_est_plan(&eq[i], qs[i].n, tile_rows);
     o_t[i] = take(16 * eq[i].cap);
-    max_items = std::max<int64_t>(max_items, int64_t(eq[i].sampled_tiles) << 10);
+    eq[i].chunk_base = chunks;
+    eq[i].nchunks = (eq[i].sampled_tiles + GBA_EST_CHUNK_TILES - 1) / GBA_EST_CHUNK_TILES;
+    chunks += eq[i].nchunks;
   }
   gba_status st = gba_est_reserve(ctx, off, s);
   if (st != GBA_OK) return st;
@@ -604,7 +675,7 @@ gba_status gba_est_features_device(gba_context* ctx, const QDesc* qs, int nq, in
   GBA_CUDA_TRY(ctx, cudaMemcpyAsync(base + o_q, eq.data(), sizeof(EstQuery) * nq, cudaMemcpyHostToDevice, s));
   const EstQuery* dq = reinterpret_cast<const EstQuery*>(base + o_q);
   GBA_CUDA_TRY(ctx, gba_launch_est_init(dq, nq, s));
-  GBA_CUDA_TRY(ctx, gba_launch_est_sample(dq, nq, max_items, s));
+  GBA_CUDA_TRY(ctx, gba_launch_est_sample(dq, nq, chunks, s));
   GBA_CUDA_TRY(ctx, gba_launch_est_reduce(dq, nq, s));
   *feats_out = reinterpret_cast<float*>(base + o_f);
   *stats_out = reinterpret_cast<unsigned long long*>(base + o_s);

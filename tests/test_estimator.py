@@ -66,6 +66,57 @@ def test_features_on_known_columns(ctx):
     assert abs(f[14:30].sum() - 1.0) < 1e-5          # register histogram sums to 1
 
 
+def test_feature_oracle_hash_matches_murmur3():
+    """The numpy feature oracle's MurmurHash3 against the C oracle's (which the
+    known-answer vectors pin), on 32- and 64-bit keys (CPU)."""
+    import cpu_oracle as O
+    rng = np.random.default_rng(3)
+    for key64 in (False, True):
+        ks = rng.integers(0, 2**63 if key64 else 2**32, size=300, dtype=np.uint64)
+        ks = ks if key64 else ks.astype(np.uint32)
+        h = M.murmur3_keys(ks, key64)
+        assert all(int(h[i]) == O.murmur3_32(ks[i].tobytes(), M.EST_SEED) for i in range(len(ks)))
+
+
+def test_feature_oracle_sample_layout():
+    """Sampled rows: 1024 per sampled tile (128 runs of 8), every row of a
+    tile of at most 1024 rows, every step-th tile past 256 tiles (CPU)."""
+    r = M.sampled_rows(65536 * 3 + 700)
+    assert len(r) == 3 * 1024 + 700 and r.max() == 65536 * 3 + 699
+    assert np.array_equal(r[:8], np.arange(8)) and r[8] == 512
+    r = M.sampled_rows(65536 * 300)
+    assert len(r) == 150 * 1024 and r[1024] == 2 * 65536
+
+
+def _feature_columns():
+    """(name, device key tensor): uniform, skewed, 32- and 64-bit, ragged last
+    tile, a single short tile, strided tiles, negative keys, the all-ones key."""
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(11)
+    out = [("1000 ids", torch.arange(100_000, dtype=torch.int64, device="cuda") % 1000),
+           ("500 rows", torch.randint(0, 50, (500,), dtype=torch.int32, device="cuda", generator=g)),
+           ("ragged i32", torch.randint(-5000, 5000, (65536 * 3 + 700,), dtype=torch.int32, device="cuda",
+                                        generator=g))]
+    u = torch.rand(3_000_000, device="cuda", generator=g, dtype=torch.float64)
+    out.append(("skewed i32", (1.0 / (u + 1e-4)).to(torch.int32)))          # a heavy head and a long tail
+    out.append(("strided i64", torch.randint(-2**62, 2**62, (20_000_003,), dtype=torch.int64, device="cuda",
+                                             generator=g)))
+    ones = torch.randint(0, 300, (1_000_000,), dtype=torch.int64, device="cuda", generator=g)
+    ones[::3] = -1                                                             # all-ones key, a third of the rows
+    out.append(("all-ones i64", ones))
+    return out
+
+
+@pytest.mark.gpu
+def test_features_match_oracle(ctx):
+    """All 32 features of the sampling and reduction kernels against the numpy
+    restatement of both (same sampled rows, hashes, counts and formulas)."""
+    for name, keys in _feature_columns():
+        f = ctx.est_features(keys)
+        ref = M.est_features(keys.cpu().numpy(), keys.dtype == __import__("torch").int64)
+        np.testing.assert_allclose(f, ref, rtol=1e-6, atol=1e-7, err_msg=name)
+
+
 @pytest.mark.gpu
 def test_training_learns_and_beats_plain(ctx):
     """A small training run: loss falls, and the learned estimate's q-error is
