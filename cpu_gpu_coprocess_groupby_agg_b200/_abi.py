@@ -156,6 +156,8 @@ SIGNATURES = {
                                    C.POINTER(C.c_int64)]),
     "gba_groupby_batch": (C.c_int, [_P, C.c_int32, C.POINTER(Query), C.POINTER(Output), C.POINTER(Knobs), _P,
                                     C.POINTER(C.c_int64)]),
+    "gba_groupby_batch_host": (C.c_int, [_P, C.c_int32, C.POINTER(Query), C.POINTER(Output), C.POINTER(Knobs), _P,
+                                         C.POINTER(C.c_int64)]),
     "gba_groupby_noalloc": (C.c_int, [_P, C.POINTER(Query), C.POINTER(Output), _P, C.POINTER(C.c_int64)]),
     "gba_groupby_partition_u32": (C.c_int, [_P, _P, _P, C.c_int64, C.c_int32, _P, _P, _P, _P]),
     "gba_avg_divide": (C.c_int, [_P, C.c_int32, _P, C.POINTER(C.c_int32), _P, C.c_int64, _P]),

@@ -316,6 +316,43 @@ class Context:
                               None if ov is None else [t[:g] for t in ov]))
         return res
 
+    def groupby_batch_host(self, queries: Sequence, outs: Sequence, knobs=None, stream=None) -> list:
+        """gba_groupby_batch_host: many queries over HOST columns into HOST
+        output buffers (pinned memory gives full link speed).
+
+        queries: sequence of (keys, cols, aggs) with numpy arrays or CPU
+        tensors; outs: per query (keys, [aggregate columns]) host buffers of
+        equal capacity.  Returns one Result per query (views into outs)."""
+        import torch
+        nq = len(queries)
+        qarr = (A.Query * max(nq, 1))()
+        oarr = (A.Output * max(nq, 1))()
+
+        def ptr_type(x):
+            if isinstance(x, torch.Tensor):
+                assert not x.is_cuda and x.is_contiguous(), "contiguous host tensors expected"
+                return x.data_ptr(), _torch_type(x, False), x.numel()
+            assert isinstance(x, np.ndarray) and x.flags.c_contiguous, "contiguous numpy arrays expected"
+            return x.ctypes.data, _np_type(x), x.shape[0]
+
+        for i, (keys, cols, aggs) in enumerate(queries):
+            kp, kt, n = ptr_type(keys)
+            col_specs = [ptr_type(c)[:2] for c in cols]
+            qarr[i] = build_query(n, kp, kt, col_specs, parse_aggs(aggs))
+            okeys, oaggs = outs[i][0], outs[i][1]
+            okp, _, cap = ptr_type(okeys)
+            oarr[i].keys = okp
+            for a, t in enumerate(oaggs):
+                oarr[i].aggs[a] = ptr_type(t)[0]
+            oarr[i].capacity = cap
+        kn = knobs if isinstance(knobs, A.Knobs) else make_knobs(**(knobs or {}))
+        ng = (C.c_int64 * max(nq, 1))()
+        s = stream if stream is not None else torch.cuda.current_stream()
+        A.check(self._lib.gba_groupby_batch_host(self._h, nq, qarr, oarr, C.byref(kn), C.c_void_p(s.cuda_stream), ng),
+                self._h)
+        st = self.stats()
+        return [Result(outs[i][0][:ng[i]], [t[:ng[i]] for t in outs[i][1]], ng[i], st) for i in range(nq)]
+
     # ---- learned cardinality estimator ---------------------------------------
     def est_param_count(self) -> int:
         return int(self._lib.gba_estimator_param_count())

@@ -43,7 +43,8 @@ cudaError_t gba_launch_batch_init(const BatchQ* d_qs, const int64_t* blk_prefix,
 cudaError_t gba_launch_batch_compact(const BatchQ* d_qs, const int64_t* blk_prefix, int nq, int64_t nblocks,
                                      cudaStream_t s);
 // Streaming aggregation with bulk-copy staging (k_stream_tma.cu): CTAs of
-// 512 threads, minb (1 or 2) per SM; every warp stages chunks of rows through
+// 512 threads, minb (1 or 2) per SM, or (minb 0) one CTA of 1024 threads per
+// SM; every warp stages chunks of rows through
 // its own ring of nstages (1..4) slots of slot_bytes each (the largest
 // gba_stream_tma_slot_bytes of the launch's queries), placed before the
 // shared table.  BatchQ.pad bit 1: combine equal keys within a warp before
@@ -53,7 +54,7 @@ cudaError_t gba_launch_batch_compact(const BatchQ* d_qs, const int64_t* blk_pref
 // launch is gba_stream_tma_cluster_grid CTAs (0: such clusters cannot be
 // resident).
 size_t gba_stream_tma_slot_bytes(const QDesc& q, int minb);
-size_t gba_stream_tma_smem_bytes(const QDesc& q, int S, int nstages, size_t slot_bytes);
+size_t gba_stream_tma_smem_bytes(const QDesc& q, int S, int nstages, size_t slot_bytes, int minb);
 bool gba_stream_tma_cluster_ok(const QDesc& q);
 int gba_stream_tma_cluster_grid(const QDesc& proto, int cluster, size_t smem, int sms);
 cudaError_t gba_prepare_stream_tma(const QDesc& proto, int cluster, int minb);

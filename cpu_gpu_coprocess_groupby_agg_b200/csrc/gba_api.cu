@@ -92,6 +92,8 @@ extern "C" gba_status gba_destroy(gba_context* ctx) {
   for (auto& e : ctx->tev)
     if (e) cudaEventDestroy(e);
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+  if (ctx->out_stream) cudaStreamDestroy(ctx->out_stream);
+  for (auto& e : ctx->part_ev) cudaEventDestroy(e);
   if (ctx->batch_exec) cudaGraphExecDestroy(ctx->batch_exec);
   if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
   if (ctx->aux_stream) cudaStreamDestroy(ctx->aux_stream);
@@ -390,13 +392,13 @@ void gba_make_plan(const gba_context* ctx, const QDesc& q, const gba_knobs& k, d
       // thousand the table holds: worth it when the groups fit a handful of
       // tables, or when the sample shows hot keys (the top key alone holds
       // >= 0.1% of the rows); otherwise every row pays a lookup and a miss.
-      const double slots = double(ctx->max_smem_optin) / double((q.key64 ? 8 : 4) + 8 * q.nwords);
+      const double slots = double(ctx->max_smem_optin) / double((q.key64 ? 8 : 4) + 4 * q.nwords);
       if (predicted_groups > 4.0 * slots && ctx->est_skew < 1e-3) preagg = 0;
       if (predicted_groups > 0.5 * double(q.n)) preagg = 0;  // nearly all keys distinct
     }
   }
   p->preagg = preagg;
-  const size_t slot_bytes = (q.key64 ? 8 : 4) + 8 * size_t(q.nwords);
+  const size_t slot_bytes = (q.key64 ? 8 : 4) + 4 * size_t(q.nwords);
   auto slots_with = [&](int use_tma) {
     const size_t fixed = gba_preagg_smem_bytes(q, 0, p->tile_rows, p->nstages, use_tma);
     const size_t room = size_t(ctx->max_smem_optin) > fixed + 1024 ? size_t(ctx->max_smem_optin) - fixed - 1024 : 0;
@@ -427,7 +429,7 @@ void gba_make_plan(const gba_context* ctx, const QDesc& q, const gba_knobs& k, d
 static gba_status run_table_once(gba_context* ctx, const QDesc& q, const gba_output* out, const GbaPlan& p,
                                  cudaStream_t s, bool timing, unsigned* flags_out, unsigned long long* count_out) {
   GbaTimer tm{ctx, s, timing};
-  const size_t stride = 1 + size_t(q.naccs);
+  const size_t stride = size_t(gba_gt_stride(q.naccs));
   const size_t table_bytes = (p.table_slots + 1) * stride * 8;
   gba_status st = gba_ws_reserve(ctx, table_bytes, s);
   if (st != GBA_OK) return st;

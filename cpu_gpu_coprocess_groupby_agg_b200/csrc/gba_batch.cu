@@ -78,6 +78,7 @@ struct Group {
   size_t stage_bytes = 0;    // bulk-copy kernel: bytes of one ring slot
   int cluster = 1;           // bulk-copy kernel: CTAs per cluster
   int minb = 1;              // CTAs per SM of the launch
+  int shape = 1;             // bulk-copy kernel: its CTA shape (1 or 2 CTAs of 512 threads per SM, 0: one of 1024)
   bool tma = false;          // bulk-copy kernel (k_stream_tma) or register-loading one (k_stream_agg)
   int64_t item_begin = 0, nitems = 0;  // item_begin: index of the group's first span
   int nspans = 0;
@@ -126,20 +127,22 @@ int batch_smem_slots(const gba_context* ctx, const QDesc& q, int bps) {
   const size_t budget = (size_t(ctx->max_smem_optin) + 1024) / size_t(bps) - 1024;
   const size_t fixed = gba_stream_smem_bytes(q, 0) + gba_batch_static_smem() + 1024;
   if (budget <= fixed) return 0;
-  const size_t slot = (q.key64 ? 8 : 4) + 8 * size_t(q.nwords);
+  const size_t slot = (q.key64 ? 8 : 4) + 4 * size_t(q.nwords);
   const int S = int(std::min<size_t>(16384, (budget - fixed) / slot));
   return S < 32 ? 0 : S;
 }
 
-// Shared-table slots of a query in the bulk-copy streaming kernel with `minb`
-// CTAs per SM: what a CTA's share of the SM's shared memory holds beside its
-// warps' copy rings (`nst` slots of `slot_bytes` each) and its static part
-// (barriers, chunk starts: 2 KB at most).
-int tma_smem_slots(const gba_context* ctx, const QDesc& q, int minb, int nst, size_t slot_bytes) {
-  const size_t budget = (size_t(ctx->max_smem_optin) + 1024) / size_t(minb) - 1024;
-  const size_t fixed = gba_stream_tma_smem_bytes(q, 0, nst, slot_bytes) + gba_batch_static_smem() + 2048;
+// Shared-table slots of a query in the bulk-copy streaming kernel of CTA
+// shape `shape` (1 or 2 CTAs of 512 threads per SM, 0: one of 1024 threads):
+// what a CTA's share of the SM's shared memory holds beside its warps' copy
+// rings (`nst` slots of `slot_bytes` each) and its static part (barriers,
+// chunk starts: 2 KB at most for 16 warps, 4 KB for 32).
+int tma_smem_slots(const gba_context* ctx, const QDesc& q, int shape, int nst, size_t slot_bytes) {
+  const size_t budget = (size_t(ctx->max_smem_optin) + 1024) / size_t(shape == 2 ? 2 : 1) - 1024;
+  const size_t fixed =
+      gba_stream_tma_smem_bytes(q, 0, nst, slot_bytes, shape) + gba_batch_static_smem() + (shape == 0 ? 4096 : 2048);
   if (budget <= fixed) return 0;
-  const size_t slot = (q.key64 ? 8 : 4) + 8 * size_t(q.nwords);
+  const size_t slot = (q.key64 ? 8 : 4) + 4 * size_t(q.nwords);
   const int S = int(std::min<size_t>(16384, (budget - fixed) / slot));
   return S < 32 ? 0 : S;
 }
@@ -150,7 +153,7 @@ int exchange_smem_slots(const gba_context* ctx, const QDesc& q, int hot) {
   const size_t budget = size_t(ctx->max_smem_optin);
   const size_t fixed = gba_exchange_smem_bytes(q, 0, hot) + gba_exchange_static_smem() + 1024;
   if (budget <= fixed) return 0;
-  const size_t slot = (q.key64 ? 8 : 4) + 8 * size_t(q.nwords);
+  const size_t slot = (q.key64 ? 8 : 4) + 4 * size_t(q.nwords);
   return int(std::min<size_t>(65536, (budget - fixed) / slot)) / 4 * 4;
 }
 
@@ -360,9 +363,9 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   // 10.3 ms at 4 (where registers spill); 3 (40 registers, few spills) is 1-2%
   // faster than 4 and is what the autotuner picks there.
   // Two streaming kernels: the register-loading one (k_stream_agg, bps CTAs
-  // per SM, automatic 3) and the bulk-copy one (k_stream_tma: tbps = 1 or 2
-  // CTAs per SM, automatic 2, each warp staging its rows through a ring of
-  // `nst` slots).  knobs.use_tma = 0 / 1 sends every query to one of them;
+  // per SM, automatic 3) and the bulk-copy one (k_stream_tma: 1 or 2 CTAs of
+  // 512 threads per SM, automatic 2, or one of 1024 threads, each warp staging
+  // its rows through a ring of `nst` slots).  knobs.use_tma = 0 / 1 sends every query to one of them;
   // automatic (-1): a query whose predicted groups outgrow half the
   // register-loading kernel's shared table goes to the bulk-copy kernel, the
   // rest (and every query under plain sizing) to the register-loading one.
@@ -372,7 +375,16 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   // 1.32 vs 1.04; 262144-2^20: 2.35 vs 2.25; above 2^20: 2.94 vs 2.65.
   const int nst = k.nstages >= 1 && k.nstages <= 4 ? k.nstages : 3;
   const int bps = k.blocks_per_sm >= 1 && k.blocks_per_sm <= 4 ? k.blocks_per_sm : 3;
-  const int tbps = k.blocks_per_sm == 1 ? 1 : 2;
+  // bulk-copy kernel CTA shape: one CTA of 1024 threads per SM (automatic;
+  // one shared table of twice the slots for as many warps as two 512-thread
+  // CTAs), or CTAs of 512 threads (knobs.block_threads = 512, or
+  // blocks_per_sm 1 or 2: that many per SM, 2 by default).  Measured per
+  // class of the 256-query batch (kernel ms, 512 x 2 against 1024 x 1): 0.92
+  // against 0.85 on 65536-262143 ids, 1.93 against 1.81 on 262144-2^20, the
+  // others within 1%.
+  const int tshape = k.block_threads == 1024                                                   ? 0
+                     : k.block_threads == 512 || k.blocks_per_sm == 1 || k.blocks_per_sm == 2 ? (k.blocks_per_sm == 1 ? 1 : 2)
+                                                                                              : 0;
   bool any_tma = false;
   // buckets probed in a shared table before a row goes to the HBM table
   const int sprobe = k.smem_probe_cap > 0 ? k.smem_probe_cap : 2;
@@ -387,15 +399,15 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
     ctx->est_skew = skew[i];
     gba_make_plan(ctx, qd[i], k, pred[i], &qi[i].p);
     qi[i].pred = pred[i];
-    double table_bytes = double(qi[i].p.table_slots + 1) * 8.0 * double(1 + qd[i].naccs);
+    double table_bytes = double(qi[i].p.table_slots + 1) * 8.0 * double(gba_gt_stride(qd[i].naccs));
     // A learned-sized table that cannot stay in L2 at the batch's load anyway
     // (above twice its 126 MB) is sized at load 0.5: half the DRAM footprint for
     // its inserts, at the cost of longer probes (an under-estimate still regrows).
-    if (k.sizing == GBA_SIZING_LEARNED && pred[i] > 0 && table_bytes > 256.0 * double(1 << 20)) {
+    if (k.sizing == GBA_SIZING_LEARNED && pred[i] > 0 && table_bytes > 32.0 * double(1 << 20)) {
       const double g = std::min(double(std::max<int64_t>(qd[i].n, 1)), pred[i] * 1.25 + 64.0);
       const uint64_t at_half = uint64_t(g / 0.5) + 1;
       if (at_half < qi[i].p.table_slots) qi[i].p.table_slots = at_half;
-      table_bytes = double(qi[i].p.table_slots + 1) * 8.0 * double(1 + qd[i].naccs);
+      table_bytes = double(qi[i].p.table_slots + 1) * 8.0 * double(gba_gt_stride(qd[i].naccs));
     }
     qi[i].strategy = k.strategy != GBA_STRATEGY_AUTO ? k.strategy
                      : table_bytes <= kBatchTableMax ? GBA_STRATEGY_TABLE
@@ -482,17 +494,18 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   }
   for (auto& g : groups) {
     g.smem = gba_stream_smem_bytes(g.proto, 0);
-    g.minb = !g.tma ? bps : (g.cluster > 1 ? 1 : tbps);
+    g.shape = g.cluster > 1 ? 1 : tshape;
+    g.minb = !g.tma ? bps : (g.shape == 2 ? 2 : 1);
     if (g.tma) {
       // one ring slot holds a chunk of any member (run-time signatures may
       // differ in columns per member)
-      for (int i : g.members) g.stage_bytes = std::max(g.stage_bytes, gba_stream_tma_slot_bytes(qd[i], g.minb));
-      g.smem = gba_stream_tma_smem_bytes(g.proto, 0, nst, g.stage_bytes);
+      for (int i : g.members) g.stage_bytes = std::max(g.stage_bytes, gba_stream_tma_slot_bytes(qd[i], g.shape));
+      g.smem = gba_stream_tma_smem_bytes(g.proto, 0, nst, g.stage_bytes, g.shape);
     }
     for (int i : g.members) {
       // run-time signatures may differ in accumulator words per member
       int S = !qi[i].p.preagg ? 0
-              : g.tma         ? tma_smem_slots(ctx, qd[i], g.minb, nst, g.stage_bytes)
+              : g.tma         ? tma_smem_slots(ctx, qd[i], g.shape, nst, g.stage_bytes)
                               : batch_smem_slots(ctx, qd[i], bps);
       if (k.smem_slots > 0) S = std::min(S, k.smem_slots);
       // a known-small group count needs only a small shared table (cheaper
@@ -501,7 +514,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
       if (S > 0 && qi[i].pred > 0) S = std::min<int64_t>(S, std::max<int64_t>(256, int64_t(qi[i].pred * 4.0 + 31) / 32 * 32));
       S = S / 4 * 4;  // whole 16-byte buckets
       qi[i].S = S;
-      g.smem = std::max(g.smem, g.tma ? gba_stream_tma_smem_bytes(qd[i], S, nst, g.stage_bytes)
+      g.smem = std::max(g.smem, g.tma ? gba_stream_tma_smem_bytes(qd[i], S, nst, g.stage_bytes, g.shape)
                                            : gba_stream_smem_bytes(qd[i], S));
       qi[i].slot = int(tq.size());
       tq.push_back(i);
@@ -638,7 +651,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   std::vector<int64_t> ipre(nt + 1, 0), cpre(nt + 1, 0);
   for (int j = 0; j < nt; ++j) {
     const QInfo& x = qi[tq[j]];
-    const size_t words = (x.p.table_slots + 1) * (1 + size_t(x.q.naccs));
+    const size_t words = (x.p.table_slots + 1) * size_t(gba_gt_stride(x.q.naccs));
     o_tab[j] = take(words * 8);
     ipre[j + 1] = ipre[j] + int64_t(std::max<size_t>(1, (words + 256 * 16 - 1) / (256 * 16)));
     cpre[j + 1] = cpre[j] + int64_t(std::max<uint64_t>(1, (x.p.table_slots + 2047) / 2048));
@@ -718,7 +731,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
     if (fork && e == cudaSuccess) e = cudaEventRecord(ctx->fork_ev[0], cs);
     if (fork && e == cudaSuccess) e = cudaStreamWaitEvent(ctx->aux_stream, ctx->fork_ev[0], 0);
     for (int g = 0; g < ng && e == cudaSuccess; ++g)
-      e = groups[g].tma ? gba_launch_stream_tma(groups[g].proto, groups[g].cluster, groups[g].minb, d_qs,
+      e = groups[g].tma ? gba_launch_stream_tma(groups[g].proto, groups[g].cluster, groups[g].shape, d_qs,
                                              d_spans + groups[g].item_begin, groups[g].nspans,
                                              groups[g].nitems, d_ctr + g, groups[g].smem, sprobe, groups[g].grid,
                                              nst, groups[g].stage_bytes, fork && (g & 1) ? ctx->aux_stream : cs)
@@ -749,7 +762,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   }
   if (nt > 0) {
     for (int g = 0; g < ng; ++g)
-      GBA_CUDA_TRY(ctx, groups[g].tma ? gba_prepare_stream_tma(groups[g].proto, groups[g].cluster, groups[g].minb)
+      GBA_CUDA_TRY(ctx, groups[g].tma ? gba_prepare_stream_tma(groups[g].proto, groups[g].cluster, groups[g].shape)
                                    : gba_prepare_stream_agg(groups[g].proto, bps));
     if (as_graph) {
       // the graph depends only on launch shapes and buffer addresses
@@ -773,7 +786,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
         key.push_back(g.nspans);
         key.push_back(g.grid);
         key.push_back(int64_t(g.stage_bytes));
-        key.push_back(g.cluster * 16 + g.minb * 2 + (g.tma ? 1 : 0));
+        key.push_back(((g.cluster * 16 + g.minb) * 4 + g.shape) * 2 + (g.tma ? 1 : 0));
       }
       key.push_back(nxq);
       key.push_back(xwin);

@@ -25,6 +25,9 @@ struct gba_context {
   unsigned char* h_small = nullptr;
   size_t h_small_bytes = 0;
   cudaStream_t copy_stream = nullptr;
+  // host-resident batch: the device-to-host stream and one event per part
+  cudaStream_t out_stream = nullptr;
+  std::vector<cudaEvent_t> part_ev;
   cudaEvent_t ev[8] = {};
   cudaEvent_t tev[16] = {};  // timing events (gba_knobs.timing)
   // estimator (device weights + Adam state + gradient scratch)

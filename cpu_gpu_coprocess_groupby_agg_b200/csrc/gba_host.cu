@@ -107,7 +107,7 @@ extern "C" gba_status gba_groupby_host(gba_context* ctx, const gba_query* q, con
   } else {
     // Chunked pipeline: H2D of chunk i+1 overlaps the pre-aggregation of chunk i.
     const int64_t chunk = std::max<int64_t>(int64_t(p.tile_rows), int64_t(1) << 23) / p.tile_rows * p.tile_rows;
-    const size_t stride = 1 + size_t(dq.naccs);
+    const size_t stride = size_t(gba_gt_stride(dq.naccs));
     const size_t table_bytes = (p.table_slots + 1) * stride * 8;
     st = gba_ws_reserve(ctx, table_bytes, s);
     if (st != GBA_OK) return st;

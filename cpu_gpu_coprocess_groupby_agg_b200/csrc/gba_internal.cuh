@@ -165,13 +165,13 @@ __device__ __forceinline__ void global_acc(int op, unsigned long long* p, unsign
 // flag is raised and the pair is dropped (the host re-runs the query with a
 // larger table, so a result is never reported from an overflowed table).
 // NA is the number of accumulators of the query (the table's slot stride is
-// 1 + NA words); kernels are instantiated per NA so no dead accumulator code
-// is emitted.
+// gba_gt_stride(NA) words); kernels are instantiated per NA so no dead
+// accumulator code is emitted.
 template <bool K64, typename Sig>
 __device__ __forceinline__ void gtable_insert(const GTable& t, const QDesc& q, uint64_t key, uint32_t h,
                                               const unsigned long long* vals, unsigned* flags) {
   constexpr int NA = Sig::NA;
-  constexpr int stride = 1 + NA;
+  constexpr int stride = gba_gt_stride(NA);
   unsigned long long* slotp;
   if (key == (K64 ? EMPTY64 : uint64_t(EMPTY32))) {
     slotp = t.base + t.cap * stride;
@@ -208,7 +208,7 @@ __device__ __forceinline__ void gtable_finish(const GTable& t, const QDesc& q, u
                                               unsigned long long cur, const unsigned long long* vals,
                                               unsigned* flags) {
   constexpr int NA = Sig::NA;
-  constexpr int stride = 1 + NA;
+  constexpr int stride = gba_gt_stride(NA);
   unsigned long long* slotp = t.base + s * stride;
   int p = 0;
   for (;;) {

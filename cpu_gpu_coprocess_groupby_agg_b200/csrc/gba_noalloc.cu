@@ -96,7 +96,7 @@ extern "C" gba_status gba_groupby_noalloc(gba_context* ctx, const gba_query* q_i
 
   // Capacity 2 n + 64 (load <= 0.5 even if every key is distinct), walked to
   // the end on a collision chain, so the table cannot overflow.
-  const size_t stride = 1 + size_t(q.naccs);
+  const size_t stride = size_t(gba_gt_stride(q.naccs));
   const uint64_t cap = 2 * uint64_t(q.n) + 64;
   const size_t need = kNoallocTableOffset + (cap + 1) * stride * 8;
   if (need > kNoallocScratchBytes) {

@@ -40,10 +40,10 @@ size_t row_bytes(const QDesc& q) {
 
 // shared-memory slots one partition table can use
 static int part_table_slots(const gba_context* ctx, const QDesc& q) {
-  const size_t slot = (q.key64 ? 8 : 4) + 8 * size_t(q.nwords);
-  // 1 KB stays free for the kernel's static shared memory, the side slot and
+  const size_t slot = (q.key64 ? 8 : 4) + 4 * size_t(q.nwords);
+  // 2 KB stay free for the kernel's static shared memory, the side slot and
   // alignment
-  const size_t room = size_t(ctx->max_smem_optin) - 1024;
+  const size_t room = size_t(ctx->max_smem_optin) - 2048;
   return int(std::min<size_t>(16384, room / slot));
 }
 
@@ -54,7 +54,7 @@ int gba_choose_strategy(const gba_context* ctx, const QDesc& q, const gba_knobs&
   // (126 MB; measured: random 64-bit atomics run at ~190 G/s below ~96 MB of
   // table and fall to 20-60 G/s above it).  Beyond that the partition
   // strategy's shared-memory tables win.
-  const double slot = 8.0 * (1 + q.naccs);
+  const double slot = 8.0 * gba_gt_stride(q.naccs);
   const double groups = predicted_groups > 0 ? predicted_groups : double(q.n);
   (void)p;
   if (groups <= 0.55 * part_table_slots(ctx, q)) return GBA_STRATEGY_TABLE;  // shared table holds all groups
@@ -119,7 +119,7 @@ gba_status gba_run_partition(gba_context* ctx, const QDesc& q, const gba_output*
     const int64_t max_split = n / (2 * Lp) + 1;
     const size_t o_work = cv.take(sizeof(PartWork) * size_t(nseg_final + n / Lp + 2));
     // the fallback table goes last: its final size is known after partitioning
-    const size_t fb_slot_bytes = (1 + size_t(q.naccs)) * 8;
+    const size_t fb_slot_bytes = size_t(gba_gt_stride(q.naccs)) * 8;
     const size_t o_fb = cv.take((fb_cap + 1 + uint64_t(max_split) * uint64_t(S) * 2) * fb_slot_bytes);
     gba_status st = gba_ws_reserve(ctx, cv.off, s);
     if (st != GBA_OK) return st;

@@ -80,7 +80,7 @@ static int64_t ctx_resident_bytes(const gba_context* c) {
 static int64_t request_bytes(const QDesc& q, const gba_knobs& k) {
   const double lf = (k.load_factor > 0.05 && k.load_factor < 0.95) ? k.load_factor : 0.5;
   const uint64_t slots = gba_pow2_ceil(uint64_t(double(std::max<int64_t>(q.n, 1)) / lf));
-  const int64_t table = int64_t(slots + 1) * (1 + q.naccs) * 8;
+  const int64_t table = int64_t(slots + 1) * gba_gt_stride(q.naccs) * 8;
   const int64_t part = 2 * q.n * int64_t(gba_row_bytes(q)) + (int64_t(1) << 24);
   return std::max(table, part) + (int64_t(1) << 20);
 }

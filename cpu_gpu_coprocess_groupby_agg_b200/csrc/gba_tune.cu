@@ -11,7 +11,8 @@
 //                              partition_bits (around the automatic choice),
 //                              learned_load / load_factor (HBM table load)
 //   a batch (gba_groupby_batch): use_tma (which streaming kernel),
-//                              blocks_per_sm, nstages, coalesce, table_slots
+//                              blocks_per_sm, block_threads (the bulk-copy
+//                              kernel's CTA size), nstages, coalesce, table_slots
 //                              (GROW sizing), learned_load / load_factor,
 //                              item_rows, smem_probe_cap (buckets probed)
 // The outputs are written by every trial; the last trial leaves a complete,
@@ -104,6 +105,9 @@ extern "C" gba_status gba_autotune(gba_context* ctx, int32_t nq, const gba_query
                     }});
     axes.push_back({"blocks_per_sm", {nan, 1, 2, 4}, [](gba_knobs& k, double v) {
                       k.blocks_per_sm = std::isnan(v) ? 0 : int32_t(v);
+                    }});
+    axes.push_back({"block_threads", {nan, 512}, [](gba_knobs& k, double v) {
+                      k.block_threads = std::isnan(v) ? 0 : int32_t(v);
                     }});
     axes.push_back({"nstages", {nan, 2, 4}, [](gba_knobs& k, double v) {
                       k.nstages = std::isnan(v) ? 0 : int32_t(v);

@@ -157,7 +157,7 @@ __device__ __forceinline__ void tile_two_phase(const QDesc& q, const GTable& gt,
         row_contrib<Sig>(q, rr, v[u]);
       }
 #pragma unroll
-      for (int u = 0; u < 2; ++u) cur[u] = act[u] ? __ldcg(gt.base + slot[u] * (1 + Sig::NA)) : 0ull;
+      for (int u = 0; u < 2; ++u) cur[u] = act[u] ? __ldcg(gt.base + slot[u] * gba_gt_stride(Sig::NA)) : 0ull;
 #pragma unroll
       for (int u = 0; u < 2; ++u)
         if (act[u]) gtable_finish<K64, Sig>(gt, q, k[u], slot[u], cur[u], v[u], flags);
@@ -312,7 +312,7 @@ __global__ void __launch_bounds__(1024, 1) k_preagg(PreaggParams P) {
 // slot per iteration (no division of a word index by the slot stride).
 __device__ __forceinline__ void init_slots(const GTable& t, int naccs, const unsigned long long (&id)[GBA_MAX_AGGS],
                                            uint64_t first, uint64_t step) {
-  const int stride = 1 + naccs;
+  const int stride = gba_gt_stride(naccs);
   for (uint64_t slot = first; slot <= t.cap; slot += step) {
     unsigned long long* p = t.base + slot * stride;
     p[0] = slot == t.cap ? 0ull : EMPTY64;
@@ -339,7 +339,7 @@ __device__ __forceinline__ void compact_range(const GTable& t, const QDesc& q, c
                                               uint64_t hi) {
   __shared__ unsigned s_warp[kCompactThreads / 32];
   __shared__ unsigned long long s_base;
-  const int stride = 1 + q.naccs;
+  const int stride = gba_gt_stride(q.naccs);
   const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
   unsigned long long k[kCompactPer];
   unsigned cnt = 0;
@@ -387,7 +387,7 @@ __device__ __forceinline__ void compact_range(const GTable& t, const QDesc& q, c
 
 // the all-ones key's side slot, if present (one thread)
 __device__ __forceinline__ void compact_side(const GTable& t, const QDesc& q, const OutDesc& o) {
-  const int stride = 1 + q.naccs;
+  const int stride = gba_gt_stride(q.naccs);
   const unsigned long long* side = t.base + t.cap * stride;
   if (side[0] == 0ull) return;
   const unsigned long long pos = atomicAdd(o.count, 1ull);

@@ -240,7 +240,7 @@ __global__ void __launch_bounds__(kXThreads, 1)
           k = uint64_t(ht.keys[i]);
           if (k == uint64_t(smem_empty_key<K64>())) continue;
         } else {
-          if (!*ht.side_present) continue;
+          if (!*ht.side_present()) continue;
           k = K64 ? EMPTY64 : uint64_t(EMPTY32);
         }
         const unsigned o = unsigned((uint64_t(part_hash(k)) * G) >> 32);
@@ -302,7 +302,7 @@ __global__ void __launch_bounds__(kXThreads, 1)
           s_warp[w] = run;
           run += c;
         }
-        const unsigned side = *st.side_present ? 1u : 0u;
+        const unsigned side = *st.side_present() ? 1u : 0u;
         s_out = run + side ? atomicAdd(o.count, (unsigned long long)(run + side)) : 0ull;
         if (side) {  // the all-ones key's group, after this CTA's others
           const unsigned long long pos = s_out + run;

@@ -371,7 +371,7 @@ __global__ void __launch_bounds__(1024, 1) k_part_agg(PartAgg a) {
       for (int i = threadIdx.x; i < S; i += blockDim.x) mine += st.keys[i] != smem_empty_key<K64>();
       unsigned long long tot;
       unsigned long long before = block_excl_scan(mine, &tot);
-      const bool side = *st.side_present != 0u;
+      const bool side = *st.side_present() != 0u;
       if (threadIdx.x == 0) s_base = atomicAdd(a.out.count, tot + (side ? 1ull : 0ull));
       __syncthreads();
       unsigned long long pos = s_base + before;

@@ -40,16 +40,25 @@
 namespace {
 #include "stream_rows.cuh"
 
-constexpr int kTmaThreads = 512;
 constexpr int kTmaMaxStages = 4;
 
-constexpr int kTmaWarps = kTmaThreads / 32;
+// CTA shapes (template MINB): 1 or 2 CTAs of 512 threads per SM (MINB = 1,
+// 2), or MINB = 0: one CTA of 1024 threads per SM, which holds as many warps
+// as two 512-thread CTAs with one shared table of twice the slots.
+template <int MINB>
+__host__ __device__ constexpr int tma_threads() {
+  return MINB == 0 ? 1024 : 512;
+}
+template <int MINB>
+__host__ __device__ constexpr int tma_ctas_per_sm() {
+  return MINB == 0 ? 1 : MINB;
+}
 
-// rows per lane per chunk: fewer with more accumulators, and fewer when
-// several CTAs share an SM (their registers and shared memory are split).
-// With 16-byte rows a slot holds 2 KB (one CTA per SM) or 1 KB (two), so
-// three slots per warp keep about 64 KB of copies in flight per SM and leave
-// the rest of the shared memory to the tables.
+// rows per lane per chunk: fewer with more accumulators, and fewer when an
+// SM holds 32 warps (their registers are split).  With 16-byte rows a slot
+// holds 2 KB (16 warps per SM) or 1 KB (32), so three slots per warp keep
+// about 64 KB of copies in flight per SM and leave the rest of the shared
+// memory to the tables.
 template <typename Sig, int MINB>
 __host__ __device__ constexpr int tma_rows_per_lane() {
   return MINB == 1 ? (Sig::NA <= 2 ? 4 : (Sig::NA <= 4 ? 2 : 1)) : (Sig::NA <= 2 ? 2 : 1);
@@ -114,22 +123,23 @@ __device__ __forceinline__ bool warp_combine_equal_keys(const QDesc& q, bool liv
 // with a warp whose copy wait gave up stops working but keeps taking part in
 // the cluster's barriers until the queue is empty, so no CTA waits for it.
 template <bool K64, typename Sig, int CL, int MINB>
-__global__ void __launch_bounds__(kTmaThreads, MINB)
+__global__ void __launch_bounds__(tma_threads<MINB>(), tma_ctas_per_sm<MINB>())
     k_stream_tma(const BatchQ* qs, const BatchSpan* spans, int nspans, int64_t nitems, unsigned* item_ctr,
                  int sprobe, int nstages, unsigned slot_bytes) {
   constexpr int R = tma_rows_per_lane<Sig, MINB>();
   constexpr int CR = 32 * R;  // rows per chunk
   constexpr int NA = Sig::NA;
+  constexpr int NW = tma_threads<MINB>() / 32;  // warps
   extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ __align__(8) uint64_t bars[kTmaWarps * kTmaMaxStages];
+  __shared__ __align__(8) uint64_t bars[NW * kTmaMaxStages];
   __shared__ unsigned s_item;
   __shared__ int s_abort;
   __shared__ unsigned long long s_next;
-  __shared__ long long s_chunk[kTmaWarps][kTmaMaxStages];  // warp w's slot s holds rows from s_chunk[w][s]
+  __shared__ long long s_chunk[NW][kTmaMaxStages];  // warp w's slot s holds rows from s_chunk[w][s]
   __shared__ __align__(16) BatchQ s_q;
   const int tid = threadIdx.x;
   const unsigned lane = lane_id(), warp = unsigned(tid) >> 5;
-  const size_t ring = size_t(kTmaWarps) * nstages * slot_bytes;
+  const size_t ring = size_t(NW) * nstages * slot_bytes;
   unsigned char* const wring = smem + size_t(warp) * nstages * slot_bytes;  // this warp's slots
   uint64_t* const wbar = bars + warp * kTmaMaxStages;
   const unsigned rank = CL > 1 ? cluster_ctarank() : 0u;
@@ -330,7 +340,9 @@ __global__ void __launch_bounds__(kTmaThreads, MINB)
 namespace {
 template <typename F>
 cudaError_t with_minb(int minb, F&& f) {
-  return minb == 2 ? f(std::integral_constant<int, 2>{}) : f(std::integral_constant<int, 1>{});
+  return minb == 2   ? f(std::integral_constant<int, 2>{})
+         : minb == 0 ? f(std::integral_constant<int, 0>{})
+                     : f(std::integral_constant<int, 1>{});
 }
 }  // namespace
 
@@ -346,8 +358,9 @@ size_t gba_stream_tma_slot_bytes(const QDesc& q, int minb) {
   return (b + 127) / 128 * 128;
 }
 
-size_t gba_stream_tma_smem_bytes(const QDesc& q, int S, int nstages, size_t slot_bytes) {
-  return size_t(kTmaWarps) * nstages * slot_bytes + smem_table_bytes(S, q.key64, q.nwords) + 64;
+size_t gba_stream_tma_smem_bytes(const QDesc& q, int S, int nstages, size_t slot_bytes, int minb) {
+  const size_t warps = size_t(minb == 0 ? tma_threads<0>() : tma_threads<1>()) / 32;
+  return warps * nstages * slot_bytes + smem_table_bytes(S, q.key64, q.nwords) + 64;
 }
 
 bool gba_stream_tma_cluster_ok(const QDesc& q) {
@@ -372,7 +385,7 @@ template <int CL>
 void cluster_cfg(cudaLaunchConfig_t& cfg, cudaLaunchAttribute (&attr)[1], int grid, size_t smem, cudaStream_t s) {
   cfg = {};
   cfg.gridDim = dim3(unsigned(grid / CL * CL));
-  cfg.blockDim = dim3(kTmaThreads);
+  cfg.blockDim = dim3(tma_threads<1>());
   cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -387,8 +400,8 @@ template <bool K64, typename Sig, int CL, int MINB>
 cudaError_t launch_one(const BatchQ* d_qs, const BatchSpan* d_spans, int nspans, int64_t nitems, unsigned* item_ctr,
                        size_t smem, int sprobe, int grid, int nstages, size_t slot_bytes, cudaStream_t s) {
   if constexpr (CL == 1) {
-    k_stream_tma<K64, Sig, 1, MINB><<<grid, kTmaThreads, smem, s>>>(d_qs, d_spans, nspans, nitems, item_ctr, sprobe,
-                                                                    nstages, unsigned(slot_bytes));
+    k_stream_tma<K64, Sig, 1, MINB><<<grid, tma_threads<MINB>(), smem, s>>>(d_qs, d_spans, nspans, nitems, item_ctr,
+                                                                            sprobe, nstages, unsigned(slot_bytes));
     return cudaGetLastError();
   } else {
     cudaLaunchConfig_t cfg;
@@ -424,7 +437,7 @@ cudaError_t gba_prepare_stream_tma(const QDesc& proto, int cluster, int minb) {
       if (cluster == 2) return prepare_one<k64, Sig, 2, 1>();
     }
     if (cluster != 1) return cudaErrorInvalidValue;
-    return minb == 2 ? prepare_one<k64, Sig, 1, 2>() : prepare_one<k64, Sig, 1, 1>();
+    return with_minb(minb, [&](auto M) -> cudaError_t { return prepare_one<k64, Sig, 1, decltype(M)::value>(); });
   });
 }
 
@@ -467,9 +480,9 @@ cudaError_t gba_launch_stream_tma(const QDesc& proto, int cluster, int minb, con
                                           slot_bytes, s);
     }
     if (cluster != 1) return cudaErrorInvalidValue;
-    return minb == 2 ? launch_one<k64, Sig, 1, 2>(d_qs, d_spans, nspans, nitems, item_ctr, smem, sprobe, grid,
-                                                  nstages, slot_bytes, s)
-                     : launch_one<k64, Sig, 1, 1>(d_qs, d_spans, nspans, nitems, item_ctr, smem, sprobe, grid,
-                                                  nstages, slot_bytes, s);
+    return with_minb(minb, [&](auto M) -> cudaError_t {
+      return launch_one<k64, Sig, 1, decltype(M)::value>(d_qs, d_spans, nspans, nitems, item_ctr, smem, sprobe, grid,
+                                                         nstages, slot_bytes, s);
+    });
   });
 }

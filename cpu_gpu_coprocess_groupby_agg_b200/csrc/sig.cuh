@@ -14,7 +14,8 @@
 // spec code of one accumulator: op | source column << 4 | column type << 8
 constexpr int sig_code(int op, int col, int ctype) { return op | (col << 4) | (ctype << 8); }
 
-constexpr int sig_words(int op) { return op == ACC_ADD_F ? 3 : 1; }
+// 4-byte words of one accumulator in a shared-memory slot (gba_acc_smem_words)
+constexpr int sig_words(int op) { return op == ACC_CNT ? 1 : op == ACC_ADD_F ? 6 : 2; }
 
 // run-time signature with NA accumulators
 template <int NA_>

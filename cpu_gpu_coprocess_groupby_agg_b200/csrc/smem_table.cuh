@@ -26,10 +26,19 @@ template <bool K64>
 struct SmemTable {
   typedef typename std::conditional<K64, unsigned long long, unsigned>::type KeyW;
   KeyW* keys;
-  unsigned long long* acc;   // [NA][S]
-  unsigned long long* side;  // [NA] accumulators of the all-ones key
-  unsigned* side_present;
+  unsigned long long* acc;  // nw columns of SS 4-byte words
   int S;
+  int SS;  // column length: S rounded up to even, so every column starts 8-byte aligned
+  int nw;  // 4-byte words per slot
+  // after the columns: one 8-byte word per column index for the all-ones
+  // key's accumulators (6 per accumulator at most), then its presence flag
+  // (computed where used: fewer registers live through the row loops)
+  __device__ __forceinline__ unsigned long long* side() const {
+    return reinterpret_cast<unsigned long long*>(reinterpret_cast<unsigned*>(acc) + size_t(SS) * nw);
+  }
+  __device__ __forceinline__ unsigned* side_present() const {
+    return reinterpret_cast<unsigned*>(side() + 6 * GBA_MAX_AGGS);
+  }
 };
 
 template <bool K64>
@@ -55,17 +64,19 @@ __device__ __forceinline__ int smem_find_or_insert(const SmemTable<K64>& t, uint
   return -1;
 }
 
-// Where one 8-byte accumulator word of a slot lives.  In the table, word w
-// of slot i is split in two 32-bit halves: the low half at L[i] and the high
-// half at L[S + i], L being w's region (8 S bytes) read as 32-bit words.  The
-// 32-bit atomics of lanes updating different slots then hit consecutive
+// Where an accumulator of a slot lives.  The table's accumulators are
+// columns of SS 32-bit words, column c of slot i at C[c * SS + i] (C the
+// accumulator area read as 32-bit words).  A COUNT takes one column.  An
+// 8-byte accumulator starting at column w takes columns w and w + 1, split in
+// two 32-bit halves: the low half at column w, the high half at column w + 1.
+// The 32-bit atomics of lanes updating different slots then hit consecutive
 // banks (as whole 8-byte words, slot i's low half sat in bank 2i mod 32, half
 // the banks went unused and 78% of the partition kernel's atomic wavefronts
 // conflicted; measured end to end the change is small: +2% on the skewed and
 // serving queries, -2% on high cardinality).  MIN and MAX words, updated by
-// 64-bit atomics, and the
-// fp64 residual of an fp32 SUM stay whole: (8-byte words)[i] of the region.
-// The side slot keeps whole words, its halves in place.
+// 64-bit atomics, and the fp64 residual of an fp32 SUM stay whole: the two
+// columns read as one array of SS 8-byte words, (8-byte words)[i].
+// The side slot keeps one whole 8-byte word per column index, halves in place.
 struct AccRef {
   unsigned* lo;             // low 32 bits (split words)
   unsigned* hi;             // high 32 bits (split words)
@@ -76,14 +87,14 @@ template <bool K64>
 __device__ __forceinline__ AccRef smem_ref(const SmemTable<K64>& t, int w, int i) {
   AccRef r;
   if (i < 0) {
-    r.w64 = t.side + w;
+    r.w64 = t.side() + w;
     r.lo = reinterpret_cast<unsigned*>(r.w64);
     r.hi = r.lo + 1;
   } else {
-    unsigned long long* region = t.acc + size_t(w) * t.S;
-    r.w64 = region + i;
-    r.lo = reinterpret_cast<unsigned*>(region) + i;
-    r.hi = reinterpret_cast<unsigned*>(region) + t.S + i;
+    unsigned* region = reinterpret_cast<unsigned*>(t.acc) + size_t(w) * t.SS;
+    r.w64 = reinterpret_cast<unsigned long long*>(region) + i;
+    r.lo = region + i;
+    r.hi = region + t.SS + i;
   }
   return r;
 }
@@ -180,9 +191,10 @@ __device__ __forceinline__ unsigned long long smem_acc_read(const SmemTable<K64>
   const int op = Sig::op(q, a);
   const AccRef r = smem_ref<K64>(t, w, i);
   if (op == ACC_MIN_I || op == ACC_MAX_I) return *r.w64;
+  if (op == ACC_CNT) return *r.lo;
   const unsigned long long x = (unsigned long long)*r.hi << 32 | *r.lo;
   if (op != ACC_ADD_F) return x;
-  const AccRef r1 = smem_ref<K64>(t, w + 1, i), r2 = smem_ref<K64>(t, w + 2, i);
+  const AccRef r1 = smem_ref<K64>(t, w + 2, i), r2 = smem_ref<K64>(t, w + 4, i);
   const long long hi = (long long)((unsigned long long)*r1.hi << 32 | *r1.lo);
   const double d = double(hi) + double(x) * 0x1p-64 + __longlong_as_double(*r2.w64);
   return __double_as_longlong(d);
@@ -203,7 +215,7 @@ __device__ __forceinline__ void smem_flush_to_gtable(const QDesc& q, const GTabl
     for (int a = 0; a < Sig::NA; ++a) v[a] = smem_acc_read<K64, Sig>(st, q, a, i);
     gtable_insert<K64, Sig>(gt, q, k, table_hash(k), v, flags);
   }
-  if (threadIdx.x == 0 && *st.side_present) {
+  if (threadIdx.x == 0 && *st.side_present()) {
     unsigned long long v[Sig::NA];
 #pragma unroll
     for (int a = 0; a < Sig::NA; ++a) v[a] = smem_acc_read<K64, Sig>(st, q, a, -1);
@@ -221,24 +233,26 @@ __device__ __forceinline__ void smem_table_init(const SmemTable<K64>& t, const Q
       const AccRef r = smem_ref<K64>(t, w, i);
       if (op == ACC_MIN_I || op == ACC_MAX_I) {
         *r.w64 = acc_identity(op);
+      } else if (op == ACC_CNT) {
+        *r.lo = 0u;
       } else {
         *r.lo = 0u;
         *r.hi = 0u;
         if (op == ACC_ADD_F) {
-          const AccRef r1 = smem_ref<K64>(t, w + 1, i);
+          const AccRef r1 = smem_ref<K64>(t, w + 2, i);
           *r1.lo = 0u;
           *r1.hi = 0u;
-          *smem_ref<K64>(t, w + 2, i).w64 = 0ull;
+          *smem_ref<K64>(t, w + 4, i).w64 = 0ull;
         }
       }
     }
   }
   if (threadIdx.x == 0) {
-    for (int w = 0; w < Sig::nwords(q); ++w) t.side[w] = 0ull;
+    for (int w = 0; w < Sig::nwords(q); ++w) t.side()[w] = 0ull;
 #pragma unroll
     for (int a = 0; a < Sig::NA; ++a)
-      if (Sig::op(q, a) != ACC_ADD_F) t.side[Sig::woff(q, a)] = acc_identity(Sig::op(q, a));
-    *t.side_present = 0u;
+      if (Sig::op(q, a) != ACC_ADD_F) t.side()[Sig::woff(q, a)] = acc_identity(Sig::op(q, a));
+    *t.side_present() = 0u;
   }
 }
 
@@ -304,7 +318,7 @@ __device__ __forceinline__ void smem_apply(const SmemTable<K64>& t, const QDesc&
   for (int a = 0; a < Sig::NA; ++a) {
     const int w = Sig::woff(q, a);
     if (Sig::op(q, a) == ACC_ADD_F)
-      smem_fsum(smem_ref<K64>(t, w, slot), smem_ref<K64>(t, w + 1, slot), smem_ref<K64>(t, w + 2, slot),
+      smem_fsum(smem_ref<K64>(t, w, slot), smem_ref<K64>(t, w + 2, slot), smem_ref<K64>(t, w + 4, slot),
                 __longlong_as_double(v[a]));
     else smem_acc(Sig::op(q, a), smem_ref<K64>(t, w, slot), v[a]);
   }
@@ -313,21 +327,22 @@ __device__ __forceinline__ void smem_apply(const SmemTable<K64>& t, const QDesc&
 template <bool K64, typename Sig>
 __device__ __forceinline__ void smem_apply_side(const SmemTable<K64>& t, const QDesc& q,
                                                 const unsigned long long (&v)[Sig::NA]) {
-  if (*(volatile unsigned*)t.side_present == 0u) atomicExch(t.side_present, 1u);
+  if (*(volatile unsigned*)t.side_present() == 0u) atomicExch(t.side_present(), 1u);
 #pragma unroll
   for (int a = 0; a < Sig::NA; ++a) {
     const int w = Sig::woff(q, a);
     if (Sig::op(q, a) == ACC_ADD_F)
-      smem_fsum(smem_ref<K64>(t, w, -1), smem_ref<K64>(t, w + 1, -1), smem_ref<K64>(t, w + 2, -1),
+      smem_fsum(smem_ref<K64>(t, w, -1), smem_ref<K64>(t, w + 2, -1), smem_ref<K64>(t, w + 4, -1),
                 __longlong_as_double(v[a]));
     else smem_acc(Sig::op(q, a), smem_ref<K64>(t, w, -1), v[a]);
   }
 }
 
-// smem bytes of a table with S slots of `nwords` accumulator words
+// smem bytes of a table with S slots of `nwords` 4-byte accumulator words
+// (side slot: one 8-byte word per column, at most 6 columns per accumulator)
 __host__ __device__ inline size_t smem_table_bytes(int S, int key64, int nwords) {
   const size_t kb = key64 ? 8 : 4;
-  return ((size_t(S) * kb + 15) & ~size_t(15)) + size_t(S) * nwords * 8 + 3 * GBA_MAX_AGGS * 8 + 16;
+  return ((size_t(S) * kb + 15) & ~size_t(15)) + size_t((S + 1) & ~1) * nwords * 4 + 6 * GBA_MAX_AGGS * 8 + 16;
 }
 
 // carve a table at `base` (16-byte aligned)
@@ -335,14 +350,12 @@ template <bool K64>
 __device__ __forceinline__ SmemTable<K64> smem_table_carve(unsigned char* base, int S, int nwords) {
   SmemTable<K64> t;
   t.S = S;
+  t.SS = (S + 1) & ~1;
   size_t off = 0;
   t.keys = reinterpret_cast<typename SmemTable<K64>::KeyW*>(base + off);
   off += (size_t(S) * (K64 ? 8 : 4) + 15) & ~size_t(15);
   t.acc = reinterpret_cast<unsigned long long*>(base + off);
-  off += size_t(S) * nwords * 8;
-  t.side = reinterpret_cast<unsigned long long*>(base + off);
-  off += 3 * GBA_MAX_AGGS * 8;
-  t.side_present = reinterpret_cast<unsigned*>(base + off);
+  t.nw = nwords;
   return t;
 }
 

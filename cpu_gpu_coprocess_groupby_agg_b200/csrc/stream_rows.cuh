@@ -82,8 +82,9 @@ __device__ __forceinline__ void smem_apply_rows(const SmemTable<K64>& t, const Q
   for (int a = 0; a < Sig::NA; ++a) {
     const int op = Sig::op(q, a);
     const int w = Sig::woff(q, a);
-    // split word: low halves at lo32[slot], high halves at lo32[S + slot]
-    unsigned* lo32 = reinterpret_cast<unsigned*>(t.acc + size_t(w) * t.S);
+    // column w: low halves (a COUNT's only column) at lo32[slot], high halves
+    // in the next column, lo32[SS + slot]
+    unsigned* lo32 = reinterpret_cast<unsigned*>(t.acc) + size_t(w) * t.SS;
     if (op == ACC_CNT) {
 #pragma unroll
       for (int i = 0; i < R; ++i)
@@ -100,14 +101,14 @@ __device__ __forceinline__ void smem_apply_rows(const SmemTable<K64>& t, const Q
         if (!(rows >> i & 1u)) continue;
         const unsigned lo = unsigned(v[i][a]), hi = unsigned(v[i][a] >> 32);
         const unsigned add_hi = hi + ((old[i] + lo) < old[i] ? 1u : 0u);
-        if (add_hi) atomicAdd(lo32 + t.S + slot[i], add_hi);
+        if (add_hi) atomicAdd(lo32 + t.SS + slot[i], add_hi);
       }
     } else {
 #pragma unroll
       for (int i = 0; i < R; ++i) {
         if (!(rows >> i & 1u)) continue;
         if (op == ACC_ADD_F)
-          smem_fsum(smem_ref<K64>(t, w, slot[i]), smem_ref<K64>(t, w + 1, slot[i]), smem_ref<K64>(t, w + 2, slot[i]),
+          smem_fsum(smem_ref<K64>(t, w, slot[i]), smem_ref<K64>(t, w + 2, slot[i]), smem_ref<K64>(t, w + 4, slot[i]),
                     __longlong_as_double(v[i][a]));
         else smem_acc(op, smem_ref<K64>(t, w, slot[i]), v[i][a]);
       }
@@ -142,7 +143,7 @@ __device__ __forceinline__ void hbm_rows(const BatchQ& bq, const uint64_t (&key)
                                          const unsigned long long (&v)[R][Sig::NA], const uint32_t (&h)[R],
                                          unsigned miss) {
   constexpr int NA = Sig::NA;
-  constexpr int stride = 1 + NA;
+  constexpr int stride = gba_gt_stride(NA);
   const QDesc& q = bq.q;
   uint64_t home[R];
   unsigned long long cur[R];
@@ -350,7 +351,7 @@ __device__ __forceinline__ void stream_rows_cluster(const BatchQ& bq, const Smem
   }
 #pragma unroll
   for (int a = 0; a < NA; ++a) {
-    const uint32_t lo_local = acc_local + uint32_t(Sig::woff(q, a)) * uint32_t(st.S) * 8u;
+    const uint32_t lo_local = acc_local + uint32_t(Sig::woff(q, a)) * uint32_t(st.SS) * 4u;
     if (Sig::op(q, a) == ACC_CNT) {
 #pragma unroll
       for (int i = 0; i < R; ++i)
@@ -369,7 +370,7 @@ __device__ __forceinline__ void stream_rows_cluster(const BatchQ& bq, const Smem
         const unsigned lo = unsigned(v[i][a]), hi = unsigned(v[i][a] >> 32);
         const unsigned add_hi = hi + ((old[i] + lo) < old[i] ? 1u : 0u);
         if (add_hi)
-          dsmem_red_add_u32(dsmem_map(lo_local, owner[i]) + uint32_t(st.S + slot[i]) * 4u, add_hi);
+          dsmem_red_add_u32(dsmem_map(lo_local, owner[i]) + uint32_t(st.SS + slot[i]) * 4u, add_hi);
       }
     }
   }

@@ -128,8 +128,12 @@ typedef struct gba_knobs {
   int32_t smem_slots;     /* shared-memory table slots per CTA */
   int32_t partition_bits; /* radix fan-out 2^bits */
   int32_t blocks_per_sm;  /* single query: CTAs per SM of the pre-aggregation grid; batch: 1, 2, 3 or 4 (0 = 3)
-                             for the register-loading kernel, 1 or 2 (0 = 2) for the bulk-copy one */
-  int32_t block_threads;
+                             for the register-loading kernel, and 1 or 2 CTAs of 512 threads for the
+                             bulk-copy one (0: see block_threads) */
+  int32_t block_threads;  /* single query: threads per CTA of its kernels.  Batch: the bulk-copy kernel's
+                             CTAs, one of 1024 threads per SM (automatic: one shared table of twice the
+                             slots for as many warps) or, with 512 or blocks_per_sm 1 or 2, CTAs of 512
+                             threads */
   int32_t tile_rows;
   int32_t nstages;        /* TMA pipeline depth */
   int32_t use_tma;        /* -1 auto, 0 off, 1 on.  Single query: the TMA tile loader of the table
@@ -221,6 +225,18 @@ gba_status gba_groupby_host(gba_context* ctx, const gba_query* q, const gba_outp
  * host thread at a time: group_then_partition.cu:332-424). */
 gba_status gba_groupby_batch(gba_context* ctx, int32_t n_queries, const gba_query* qs, const gba_output* outs,
                              const gba_knobs* knobs, void* stream, int64_t* n_groups);
+
+/* gba_groupby_batch over HOST columns (and validity bitmaps) and HOST output
+ * buffers.  The queries are cut, in order, into parts of about a quarter of
+ * the input bytes; all input copies are queued at once on a copy stream, part
+ * p runs as one gba_groupby_batch call while part p + 1 crosses the link, and
+ * part p's groups are copied back on a third stream while later parts run.
+ * Pinned host memory gives full link speed.  Returns after every group is in
+ * the host buffers; gba_last_stats describes the last part.  No reference
+ * counterpart (its host-resident tiling runs one query:
+ * group_then_partition.cu:353-418). */
+gba_status gba_groupby_batch_host(gba_context* ctx, int32_t n_queries, const gba_query* qs, const gba_output* outs,
+                                  const gba_knobs* knobs, void* stream, int64_t* n_groups);
 
 /* gba_groupby without any device allocation: the table strategy (plain
  * sizing, 2 n + 64 slots) over a fixed 16 MiB scratch that is a static device

@@ -79,7 +79,9 @@ def test_batch_graph_replay_and_direct_launch_agree(ctx):
                                    dict(use_tma=0), dict(use_tma=0, blocks_per_sm=4), dict(nstages=1),
                                    dict(nstages=2), dict(nstages=4), dict(coalesce=1), dict(coalesce=0),
                                    dict(coalesce=1, smem_slots=64), dict(sizing="grow"),
-                                   dict(sizing="grow", table_slots=256)])
+                                   dict(sizing="grow", table_slots=256), dict(use_tma=1, block_threads=512),
+                                   dict(use_tma=1, block_threads=1024, nstages=4, coalesce=1),
+                                   dict(sizing="learned", block_threads=512)])
 def test_batch_knobs_do_not_change_results(ctx, knobs):
     qs = _queries(12, seed=7)
     _check(qs, ctx.groupby_batch(_device(qs), knobs=knobs), str(knobs))
@@ -136,7 +138,8 @@ def test_batch_bulk_copy_kernel_ragged_and_unaligned(ctx):
     vb[1:] = torch.from_numpy(cols[0]).cuda()
     qs.append((keys, cols, [("sum", 0), ("count", None), ("min", 0)]))
     dq.append((kb[1:], [vb[1:]], qs[-1][2], False, [False]))
-    for knobs in (dict(), dict(coalesce=1), dict(nstages=1)):
+    for knobs in (dict(), dict(coalesce=1), dict(nstages=1), dict(use_tma=1, block_threads=512),
+                  dict(use_tma=1, block_threads=1024)):
         _check(qs, ctx.groupby_batch(dq, knobs=knobs), f"ragged {knobs}")
 
 
@@ -207,3 +210,52 @@ def test_batch_owner_exchange_on_the_batch_class_256_4096(ctx):
         gk = r.keys[order].cpu().numpy()
         ga = [a[order].cpu().numpy() for a in r.aggs]
         compare(gk, ga, k.cpu().numpy(), [x.cpu().numpy() for x in c], q.aggs, label=q.name, presorted=True)
+
+
+def _host_outs(qs, pinned=True):
+    import torch
+    from cpu_gpu_coprocess_groupby_agg_b200 import _abi as AB
+    from cpu_gpu_coprocess_groupby_agg_b200.api import agg_is_fp, parse_aggs, _np_type
+
+    def buf(n, dt):
+        if not pinned:
+            return np.empty(n, dtype=dt)
+        t = torch.empty(n * np.dtype(dt).itemsize, dtype=torch.uint8).pin_memory()
+        return t.numpy().view(dt)
+
+    outs = []
+    for keys, cols, aggs in qs:
+        cap = max(len(keys), 1) + 1
+        oaggs = [buf(cap, np.float64 if (op != AB.COUNT and agg_is_fp(op, _np_type(cols[c]))) else np.int64)
+                 for op, c in parse_aggs(aggs)]
+        outs.append((buf(cap, keys.dtype), oaggs))
+    return outs
+
+
+@pytest.mark.parametrize("knobs", [dict(), dict(sizing="learned")])
+def test_batch_host_matches_oracle(ctx, knobs):
+    """gba_groupby_batch_host: host columns in, host buffers out, the queries
+    cut into parts whose copies overlap the previous part's aggregation."""
+    if knobs.get("sizing") == "learned" and not E.load_default(ctx):
+        pytest.skip("no estimator weights")
+    qs = _queries(14, seed=21, max_n=400_000)
+    # two large queries, so that the batch spans several parts of >= 64 MB
+    for j in range(2):
+        keys, cols = _data(3_000_000 + j, [np.int64, np.uint32][j], 200_000, seed=77 + j, zipf=0.6)
+        qs.insert(5 * j + 2, (keys, cols, AGGS_ALL))
+    res = ctx.groupby_batch_host(qs, _host_outs(qs), knobs=knobs)
+    for i, ((keys, cols, aggs), r) in enumerate(zip(qs, res)):
+        compare(r.keys, r.aggs, keys, cols, aggs, f"host batch {knobs} query {i}")
+
+
+def test_batch_host_pageable_and_empty(ctx):
+    """Pageable host buffers, empty queries and a batch of one."""
+    qs = _queries(5, seed=23, max_n=20_000)
+    qs.append((np.zeros(0, dtype=np.int64), _data(0, np.int64, 1)[1], [("count", None)]))
+    res = ctx.groupby_batch_host(qs, _host_outs(qs, pinned=False))
+    for i, ((keys, cols, aggs), r) in enumerate(zip(qs, res)):
+        compare(r.keys, r.aggs, keys, cols, aggs, f"pageable query {i}")
+    assert ctx.groupby_batch_host([], []) == []
+    one = qs[:1]
+    r = ctx.groupby_batch_host(one, _host_outs(one))[0]
+    compare(r.keys, r.aggs, *one[0], "batch of one")
