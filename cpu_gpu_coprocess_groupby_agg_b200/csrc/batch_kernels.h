@@ -10,6 +10,11 @@ struct BatchQ {
   unsigned* flags;  // this query's status bits
   int S;            // its shared-table slots (0 = no pre-aggregation)
   int pad;          // bit 0: keys and columns 16-byte aligned (vector loads)
+  // a query whose HBM table is built in 2^hbits passes has one entry per
+  // pass: entry hpart takes the rows whose table hash starts with hpart (its
+  // top hbits bits) into a table of its own, hashed by the remaining bits
+  int hbits;
+  int hpart;
 };
 
 // The work-queue items of one query, described at once: items first_item ..

@@ -67,7 +67,8 @@ struct QInfo {
   bool tma = false;  // streamed by the bulk-copy kernel (else the register-loading one)
   bool xch = false;  // aggregated by the owner-exchange kernel
   int hot = 0;       // exchange: hot-table slots per CTA
-  int slot = -1;     // index among the table-strategy queries
+  int slot = -1;     // index of its (first) entry among the table-strategy entries
+  int hbits = 0;     // its HBM table is built in 2^hbits passes over hash ranges (one entry each)
 };
 
 struct Group {
@@ -400,9 +401,9 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
     gba_make_plan(ctx, qd[i], k, pred[i], &qi[i].p);
     qi[i].pred = pred[i];
     double table_bytes = double(qi[i].p.table_slots + 1) * 8.0 * double(gba_gt_stride(qd[i].naccs));
-    // A learned-sized table that cannot stay in L2 at the batch's load anyway
-    // (above twice its 126 MB) is sized at load 0.5: half the DRAM footprint for
-    // its inserts, at the cost of longer probes (an under-estimate still regrows).
+    // A learned-sized table above 32 MB is sized at load 0.5: half the
+    // footprint to clear, compact and keep in L2, at the cost of longer probes
+    // (an under-estimate still regrows).
     if (k.sizing == GBA_SIZING_LEARNED && pred[i] > 0 && table_bytes > 32.0 * double(1 << 20)) {
       const double g = std::min(double(std::max<int64_t>(qd[i].n, 1)), pred[i] * 1.25 + 64.0);
       const uint64_t at_half = uint64_t(g / 0.5) + 1;
@@ -478,7 +479,19 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
 
   // ---- group the table-strategy queries by aggregate signature (and cluster) ----
   std::vector<Group> groups;
-  std::vector<int> tq;  // table-strategy queries, group by group
+  std::vector<int> tq;     // table-strategy entries (query of each), group by group
+  std::vector<int> tpart;  // the hash range each entry builds (0 for a query in one pass)
+  // With knobs.split_mb > 0, a table larger than split_bytes is built in
+  // passes: its query gets one entry per hash range of at most split_bytes
+  // (up to 16), each with a table of its own, and the entries' items follow
+  // one another in the queue, so that one range's table stays in L2 while it
+  // is built; every entry reads all of the query's rows and keeps those of
+  // its range.  Off by default: measured on the batch's queries of >= 2^20
+  // ids (kernel ms), 1.99 in one pass, 2.69 in ranges of 64 MB, 3.88 of
+  // 32 MB, 6.04 of 16 MB; each pass pays every row's load, hash and chunk
+  // bookkeeping, which cost more than the DRAM round trips the L2-resident
+  // ranges save.
+  const double split_bytes = k.split_mb > 0 ? double(k.split_mb) * double(1 << 20) : 0.0;
   for (int i = 0; i < nq; ++i) {
     if (qi[i].strategy != GBA_STRATEGY_TABLE || qi[i].xch) continue;
     // one launch per signature, key width, kernel and cluster size
@@ -516,8 +529,16 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
       qi[i].S = S;
       g.smem = std::max(g.smem, g.tma ? gba_stream_tma_smem_bytes(qd[i], S, nst, g.stage_bytes, g.shape)
                                            : gba_stream_smem_bytes(qd[i], S));
+      qi[i].hbits = 0;
+      if (split_bytes > 0 && g.cluster == 1) {  // (a cluster's table is one table)
+        const double tb = double(qi[i].p.table_slots + 1) * 8.0 * double(gba_gt_stride(qd[i].naccs));
+        while (qi[i].hbits < 4 && tb / double(1 << qi[i].hbits) > split_bytes) ++qi[i].hbits;
+      }
       qi[i].slot = int(tq.size());
-      tq.push_back(i);
+      for (int p = 0; p < (1 << qi[i].hbits); ++p) {
+        tq.push_back(i);
+        tpart.push_back(p);
+      }
     }
     // a cluster launch fills as many clusters as can be resident at once;
     // where none can, its queries run as single CTAs (smaller tables, same
@@ -551,6 +572,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
     it->smem = std::max(it->smem, gba_exchange_smem_bytes(qd[i], qi[i].S, qi[i].hot));
     qi[i].slot = int(tq.size());
     tq.push_back(i);
+    tpart.push_back(0);
     xwin = std::max<int64_t>(xwin, qd[i].n);
     xstride = std::max<int64_t>(xstride, 1 + qd[i].ncols);
     if (qi[i].hot) {  // hot tables leave as partial records of 1 + naccs words
@@ -605,8 +627,11 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
       ir = std::min(item_cap, std::max<int64_t>(T, (ir + T - 1) / T * T));
       const int64_t nit = (qd[i].n + ir - 1) / ir;
       if (nit == 0) continue;
-      spans.push_back(BatchSpan{qi[i].slot, 0, ir, first});
-      first += nit;
+      // a table built in passes: the entries' items one after another
+      for (int p = 0; p < (1 << qi[i].hbits); ++p) {
+        spans.push_back(BatchSpan{qi[i].slot + p, 0, ir, first});
+        first += nit;
+      }
     }
     g.nspans = int(int64_t(spans.size()) - g.item_begin);
     g.nitems = first;
@@ -648,13 +673,17 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   const size_t o_xstat = o_stat + 16 * size_t(nt) + 4 * size_t(ng);
   const size_t o_xbuf = nxq ? take(2 * size_t(xgrid) * size_t(xregion) * size_t(xstride) * 8) : 0;
   std::vector<size_t> o_tab(nt);
+  std::vector<uint64_t> tcap(nt);  // slots of each entry's table
   std::vector<int64_t> ipre(nt + 1, 0), cpre(nt + 1, 0);
   for (int j = 0; j < nt; ++j) {
     const QInfo& x = qi[tq[j]];
-    const size_t words = (x.p.table_slots + 1) * size_t(gba_gt_stride(x.q.naccs));
+    // one hash range's table: its share of the slots, with 1.6% and 64 slots
+    // to spare for the ranges' uneven group counts
+    tcap[j] = x.hbits ? (x.p.table_slots >> x.hbits) + (x.p.table_slots >> (x.hbits + 6)) + 64 : x.p.table_slots;
+    const size_t words = (tcap[j] + 1) * size_t(gba_gt_stride(x.q.naccs));
     o_tab[j] = take(words * 8);
     ipre[j + 1] = ipre[j] + int64_t(std::max<size_t>(1, (words + 256 * 16 - 1) / (256 * 16)));
-    cpre[j + 1] = cpre[j] + int64_t(std::max<uint64_t>(1, (x.p.table_slots + 2047) / 2048));
+    cpre[j + 1] = cpre[j] + int64_t(std::max<uint64_t>(1, (tcap[j] + 2047) / 2048));
   }
   if (nt > 0) {
     gba_status st = gba_ws_reserve(ctx, off, s);
@@ -673,14 +702,18 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
       std::memset(&b, 0, sizeof(b));
       b.q = qd[i];
       b.gt.base = reinterpret_cast<unsigned long long*>(d + o_tab[j]);
-      b.gt.cap = qi[i].p.table_slots;
+      b.gt.cap = tcap[j];
       b.gt.probe_cap = qi[i].p.probe_cap;
       b.out.keys = outs[i].keys;
       for (int a = 0; a < GBA_MAX_AGGS; ++a) b.out.accs[a] = static_cast<unsigned long long*>(outs[i].aggs[a]);
       b.out.capacity = outs[i].capacity;
-      b.out.count = reinterpret_cast<unsigned long long*>(d + o_stat + 16 * size_t(j) + 8);
+      // the entries of a query built in passes append to one output: the
+      // group counter of its first entry
+      b.out.count = reinterpret_cast<unsigned long long*>(d + o_stat + 16 * size_t(qi[i].slot) + 8);
       b.flags = reinterpret_cast<unsigned*>(d + o_stat + 16 * size_t(j));
       b.S = qi[i].S;
+      b.hbits = qi[i].hbits;
+      b.hpart = tpart[j];
       bool vec = aligned16(qd[i].keys);
       for (int c = 0; c < qd[i].ncols; ++c) vec = vec && aligned16(qd[i].cols[c]);
       // bits 8..15: buckets probed per row; a table the query's groups will
@@ -826,9 +859,10 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
       if (cudaEventElapsedTime(&ms, ctx->tev[r], ctx->tev[r + 1]) == cudaSuccess) ctx->stats.kernel_ms[r] += ms;
     }
     ctx->stats.kernel_launches += 2 + ng + int(xgroups.size());
-    for (int i : tq) {
-      ctx->stats.main_rows += qd[i].n;
-      ctx->stats.main_bytes += qd[i].n * int64_t(gba_row_bytes(qd[i]));
+    for (int j = 0; j < nt; ++j) {
+      if (tpart[j]) continue;  // a query's rows count once, whatever its passes
+      ctx->stats.main_rows += qd[tq[j]].n;
+      ctx->stats.main_bytes += qd[tq[j]].n * int64_t(gba_row_bytes(qd[tq[j]]));
     }
   }
 
@@ -840,11 +874,17 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
     return GBA_ERR_TIMEOUT;
   }
   std::vector<int> rerun;
+  // a query's status: the bits of all its entries; its group count: its first entry's counter
+  std::vector<unsigned> qflags(nq, 0u);
   for (int j = 0; j < nt; ++j) {
+    qflags[tq[j]] |= *reinterpret_cast<const unsigned*>(h + h_stat + 16 * size_t(j));
+    acc.table_slots += int64_t(tcap[j]);
+  }
+  for (int j = 0; j < nt; ++j) {
+    if (tpart[j]) continue;
     const int i = tq[j];
-    const unsigned flags = *reinterpret_cast<const unsigned*>(h + h_stat + 16 * size_t(j));
+    const unsigned flags = qflags[i];
     const unsigned long long cnt = *reinterpret_cast<const unsigned long long*>(h + h_stat + 16 * size_t(j) + 8);
-    acc.table_slots += int64_t(qi[i].p.table_slots);
     if (flags & GBA_FLAG_WAIT_TIMEOUT) {
       ctx->err = "query " + std::to_string(i) + ": a bounded device wait timed out";
       return GBA_ERR_TIMEOUT;
@@ -901,7 +941,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   trace.mark("partition_queries_and_reruns");
   acc.strategy = nt == nq ? GBA_STRATEGY_TABLE : (nt == 0 ? GBA_STRATEGY_PARTITION : GBA_STRATEGY_AUTO);
   acc.preagg = 0;
-  for (int j = 0; j < nt; ++j) acc.preagg += qi[tq[j]].S > 0;
+  for (int j = 0; j < nt; ++j) acc.preagg += tpart[j] == 0 && qi[tq[j]].S > 0;
   acc.n_groups = 0;
   for (int i = 0; i < nq; ++i) acc.n_groups += n_groups[i];
   ctx->stats = acc;

@@ -160,6 +160,8 @@ __global__ void __launch_bounds__(kXThreads, 1)
 #pragma unroll
           for (int i = 0; i < kXRows; ++i) row_contrib<Sig>(q, raw[i], v[i]);
           uint32_t hh[kXRows];
+#pragma unroll
+          for (int i = 0; i < kXRows; ++i) hh[i] = table_hash(key[i]);
           const unsigned miss = smem_rows<K64, Sig, kXRows>(ht, q, 1, key, v, live, hh);
 #pragma unroll
           for (int i = 0; i < kXRows; ++i) live[i] = (miss >> i) & 1u;

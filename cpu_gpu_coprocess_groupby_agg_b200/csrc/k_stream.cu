@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(512, MINB) k_stream_agg(const BatchQ* qs, cons
       stream_chunk<K64, Sig, R>(s_q, st, nbk, int64_t(c0), item.row_end, vec);
     }
     __syncthreads();
-    if (s_q.S > 0) smem_flush_to_gtable<K64, Sig>(s_q.q, s_q.gt, st, s_q.flags);
+    if (s_q.S > 0) smem_flush_to_gtable<K64, Sig>(s_q.q, s_q.gt, st, s_q.flags, s_q.hbits);
     __syncthreads();  // s_q and the table are rewritten by the next item
   }
 }
