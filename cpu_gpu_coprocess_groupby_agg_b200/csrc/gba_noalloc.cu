@@ -70,6 +70,14 @@ extern "C" gba_status gba_groupby_noalloc(gba_context* ctx, const gba_query* q_i
                                           void* stream, int64_t* n_groups) {
   if (!ctx || !q_in || !out || !n_groups) return GBA_ERR_INVALID_ARG;
   GBA_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  // the call reads its group count back and synchronises the stream: it
+  // cannot be part of a stream capture
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  GBA_CUDA_TRY(ctx, cudaStreamIsCapturing(static_cast<cudaStream_t>(stream), &capture));
+  if (capture != cudaStreamCaptureStatusNone) {
+    ctx->err = "gba_groupby_noalloc: the stream is being captured; the call synchronises it and cannot be captured";
+    return GBA_ERR_INVALID_ARG;
+  }
   ctx->stats = gba_stats{};
   ctx->stats.predicted_groups = -1;
   // per-aggregate validity outputs and a second key output belong to the

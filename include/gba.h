@@ -255,8 +255,11 @@ gba_status gba_groupby_batch_host(gba_context* ctx, int32_t n_queries, const gba
  * Limit: (2 n_rows + 65) * (1 + n_aggs) * 8 + 256 bytes must fit in 16 MiB
  * (about 349,000 rows with 2 aggregates); larger queries return
  * GBA_ERR_INVALID_ARG with the limit in gba_last_error and launch nothing.
- * The first call on a device looks up the scratch's address, which may load
- * the library's device code: make it before any stream capture begins.  The
+ * The call synchronises `stream` to read its group count back, so no call can
+ * be captured into a CUDA graph: on a capturing stream it returns
+ * GBA_ERR_INVALID_ARG and launches nothing.  The first call on a device looks
+ * up the scratch's address, which may load the library's device code (while
+ * another thread captures a stream, that load may break its capture).  The
  * address is kept until the process exits, so do not call this entry point
  * after resetting the device (cudaDeviceReset).  Nullable columns, validity
  * outputs and composite keys return GBA_ERR_UNSUPPORTED.  Every

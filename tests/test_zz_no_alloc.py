@@ -132,6 +132,24 @@ def test_noalloc_rejects_queries_beyond_the_scratch(ctx):
     assert str(SCRATCH_BYTES) in msg and "rows" in msg, msg
 
 
+def test_noalloc_refuses_a_capturing_stream(ctx):
+    """The call synchronises its stream, so under stream capture it returns
+    GBA_ERR_INVALID_ARG before any CUDA work (the capture stays valid)."""
+    import torch
+    keys, cols = _data(1000, np.int64, 50, seed=5)
+    dk = torch.from_numpy(keys).cuda()
+    dcols = [torch.from_numpy(c).cuda() for c in cols]
+    assert _noalloc(ctx, dk, dcols, AGGS)[0] == A.OK  # address lookup outside any capture
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        st = _noalloc(ctx, dk, dcols, AGGS)[0]
+    assert st == A.ERR_INVALID_ARG
+    assert "captured" in ctx._lib.gba_last_error(ctx._h).decode()
+    del g
+    assert _noalloc(ctx, dk, dcols, AGGS)[0] == A.OK
+
+
 def test_noalloc_rejects_validity_outputs(ctx):
     import torch
     keys, cols = _data(1000, np.int64, 50, seed=3)
