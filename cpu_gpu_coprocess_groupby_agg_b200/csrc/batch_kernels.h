@@ -42,11 +42,13 @@ cudaError_t gba_prepare_stream_agg(const QDesc& proto, int minb);
 cudaError_t gba_launch_stream_agg(const QDesc& proto, int minb, const BatchQ* d_qs, const BatchSpan* d_spans,
                                   int nspans, int64_t nitems, unsigned* item_ctr, size_t smem, int sprobe, int grid,
                                   cudaStream_t s);
-// blk_prefix[i]: first block of query i (nq + 1 entries, blk_prefix[nq] = nblocks)
+// Table init and compaction of the table entries whose blocks are block0 ..
+// block0 + nblocks - 1: blk_prefix[i] is the first block of entry i (entries
+// 0 .. nq - 1 searched, blk_prefix[nq] >= block0 + nblocks)
 cudaError_t gba_launch_batch_init(const BatchQ* d_qs, const int64_t* blk_prefix, int nq, int64_t nblocks,
-                                  cudaStream_t s);
+                                  int64_t block0, cudaStream_t s);
 cudaError_t gba_launch_batch_compact(const BatchQ* d_qs, const int64_t* blk_prefix, int nq, int64_t nblocks,
-                                     cudaStream_t s);
+                                     int64_t block0, cudaStream_t s);
 // Streaming aggregation with bulk-copy staging (k_stream_tma.cu): CTAs of
 // 512 threads, minb (1 or 2) per SM, or (minb 0) one CTA of 1024 threads per
 // SM; every warp stages chunks of rows through

@@ -82,6 +82,7 @@ struct Group {
   int shape = 1;             // bulk-copy kernel: its CTA shape (1 or 2 CTAs of 512 threads per SM, 0: one of 1024)
   bool tma = false;          // bulk-copy kernel (k_stream_tma) or register-loading one (k_stream_agg)
   int64_t item_begin = 0, nitems = 0;  // item_begin: index of the group's first span
+  int entry_begin = 0, entry_end = 0;   // its table entries
   int nspans = 0;
   int grid = 0;
 };
@@ -515,6 +516,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
       for (int i : g.members) g.stage_bytes = std::max(g.stage_bytes, gba_stream_tma_slot_bytes(qd[i], g.shape));
       g.smem = gba_stream_tma_smem_bytes(g.proto, 0, nst, g.stage_bytes, g.shape);
     }
+    g.entry_begin = int(tq.size());
     for (int i : g.members) {
       // run-time signatures may differ in accumulator words per member
       int S = !qi[i].p.preagg ? 0
@@ -540,6 +542,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
         tpart.push_back(p);
       }
     }
+    g.entry_end = int(tq.size());
     // a cluster launch fills as many clusters as can be resident at once;
     // where none can, its queries run as single CTAs (smaller tables, same
     // results)
@@ -555,6 +558,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
     }
   }
   // exchange launches: one per signature and key width, queries largest first
+  const int x_entry_begin = int(tq.size());
   std::vector<XGroup> xgroups;
   int64_t xwin = 0, xstride = 1;
   int xhot = 0;
@@ -751,26 +755,47 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
     // inside a capture the event record must be an external graph node
     return as_graph ? cudaEventRecordWithFlags(ctx->tev[i], cs, cudaEventRecordExternal) : cudaEventRecord(ctx->tev[i], cs);
   };
+  const int64_t* d_ipre = reinterpret_cast<const int64_t*>(d + o_ipre);
+  const int64_t* d_cpre = reinterpret_cast<const int64_t*>(d + o_cpre);
+  // table init / compaction of the entries [jb, je)
+  auto init_range = [&](int jb, int je, cudaStream_t st) {
+    return gba_launch_batch_init(d_qs, d_ipre, je, ipre[je] - ipre[jb], ipre[jb], st);
+  };
+  auto compact_range = [&](int jb, int je, cudaStream_t st) {
+    return gba_launch_batch_compact(d_qs, d_cpre, je, cpre[je] - cpre[jb], cpre[jb], st);
+  };
+  auto launch_group = [&](int g, cudaStream_t st) {
+    return groups[g].tma ? gba_launch_stream_tma(groups[g].proto, groups[g].cluster, groups[g].shape, d_qs,
+                                                 d_spans + groups[g].item_begin, groups[g].nspans, groups[g].nitems,
+                                                 d_ctr + g, groups[g].smem, sprobe, groups[g].grid, nst,
+                                                 groups[g].stage_bytes, st)
+                         : gba_launch_stream_agg(groups[g].proto, bps, d_qs, d_spans + groups[g].item_begin,
+                                                 groups[g].nspans, groups[g].nitems, d_ctr + g, groups[g].smem,
+                                                 sprobe, groups[g].grid, st);
+  };
+  // The streaming launches alternate between two streams, so one launch's
+  // tail (its last, small items) overlaps the next launch.  Each launch's
+  // tables are cleared just before it and compacted just after it on its own
+  // stream, so that the other stream's latency-bound streaming kernel runs
+  // beside those bandwidth-bound passes.  With kernel timing on, every clear
+  // runs before and every compaction after all streaming launches (the three
+  // roles' times are then separate).
+  const bool fork = ng >= 2;
+  const bool per_group = fork && !timing;
   auto enqueue = [&](cudaStream_t cs) -> cudaError_t {
     cudaError_t e = cudaMemcpyAsync(d, h, desc_bytes, cudaMemcpyHostToDevice, cs);
     if (e == cudaSuccess) e = cudaMemsetAsync(d + o_stat, 0, stat_bytes, cs);
     if (e == cudaSuccess) e = mark(0, cs);
-    if (e == cudaSuccess)
-      e = gba_launch_batch_init(d_qs, reinterpret_cast<const int64_t*>(d + o_ipre), nt, ipre[nt], cs);
+    if (e == cudaSuccess) e = per_group ? init_range(x_entry_begin, nt, cs) : init_range(0, nt, cs);
     if (e == cudaSuccess) e = mark(1, cs);
-    // the streaming launches alternate between two streams, so one launch's
-    // tail (its last, small items) overlaps the next launch
-    const bool fork = ng >= 2;
     if (fork && e == cudaSuccess) e = cudaEventRecord(ctx->fork_ev[0], cs);
     if (fork && e == cudaSuccess) e = cudaStreamWaitEvent(ctx->aux_stream, ctx->fork_ev[0], 0);
-    for (int g = 0; g < ng && e == cudaSuccess; ++g)
-      e = groups[g].tma ? gba_launch_stream_tma(groups[g].proto, groups[g].cluster, groups[g].shape, d_qs,
-                                             d_spans + groups[g].item_begin, groups[g].nspans,
-                                             groups[g].nitems, d_ctr + g, groups[g].smem, sprobe, groups[g].grid,
-                                             nst, groups[g].stage_bytes, fork && (g & 1) ? ctx->aux_stream : cs)
-                     : gba_launch_stream_agg(groups[g].proto, bps, d_qs, d_spans + groups[g].item_begin,
-                                             groups[g].nspans, groups[g].nitems, d_ctr + g, groups[g].smem, sprobe,
-                                             groups[g].grid, fork && (g & 1) ? ctx->aux_stream : cs);
+    for (int g = 0; g < ng && e == cudaSuccess; ++g) {
+      const cudaStream_t st = fork && (g & 1) ? ctx->aux_stream : cs;
+      if (per_group) e = init_range(groups[g].entry_begin, groups[g].entry_end, st);
+      if (e == cudaSuccess) e = launch_group(g, st);
+      if (per_group && e == cudaSuccess) e = compact_range(groups[g].entry_begin, groups[g].entry_end, st);
+    }
     if (fork && e == cudaSuccess) e = cudaEventRecord(ctx->fork_ev[1], ctx->aux_stream);
     if (fork && e == cudaSuccess) e = cudaStreamWaitEvent(cs, ctx->fork_ev[1], 0);
     for (size_t g = 0; g < xgroups.size() && e == cudaSuccess; ++g)
@@ -782,8 +807,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
                               reinterpret_cast<unsigned*>(d + o_xstat),
                               reinterpret_cast<unsigned*>(d + o_xstat + 8), xgroups[g].smem, sprobe, xgrid, cs);
     if (e == cudaSuccess) e = mark(2, cs);
-    if (e == cudaSuccess)
-      e = gba_launch_batch_compact(d_qs, reinterpret_cast<const int64_t*>(d + o_cpre), nt, cpre[nt], cs);
+    if (e == cudaSuccess) e = per_group ? compact_range(x_entry_begin, nt, cs) : compact_range(0, nt, cs);
     if (e == cudaSuccess) e = mark(3, cs);
     if (e == cudaSuccess) e = cudaMemcpyAsync(h + h_stat, d + o_stat, stat_bytes, cudaMemcpyDeviceToHost, cs);
     return e;
@@ -820,7 +844,15 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
         key.push_back(g.grid);
         key.push_back(int64_t(g.stage_bytes));
         key.push_back(((g.cluster * 16 + g.minb) * 4 + g.shape) * 2 + (g.tma ? 1 : 0));
+        // its clear and compaction launches
+        key.push_back(g.entry_begin);
+        key.push_back(g.entry_end);
+        key.push_back(ipre[g.entry_begin]);
+        key.push_back(cpre[g.entry_begin]);
       }
+      key.push_back(x_entry_begin);
+      key.push_back(ipre[x_entry_begin]);
+      key.push_back(cpre[x_entry_begin]);
       key.push_back(nxq);
       key.push_back(xwin);
       key.push_back(xregion);

@@ -419,9 +419,11 @@ __device__ __forceinline__ int batch_query_of_block(const int64_t* blk_prefix, i
   return lo;
 }
 
-__global__ void __launch_bounds__(256) k_batch_init(const BatchQ* qs, const int64_t* blk_prefix, int nq) {
-  const int qi = batch_query_of_block(blk_prefix, nq, blockIdx.x);
-  const int64_t b = int64_t(blockIdx.x) - blk_prefix[qi];
+__global__ void __launch_bounds__(256) k_batch_init(const BatchQ* qs, const int64_t* blk_prefix, int nq,
+                                                    int64_t block0) {
+  const int64_t blk = block0 + int64_t(blockIdx.x);
+  const int qi = batch_query_of_block(blk_prefix, nq, blk);
+  const int64_t b = blk - blk_prefix[qi];
   const int64_t nb = blk_prefix[qi + 1] - blk_prefix[qi];
   const GTable t = qs[qi].gt;
   const QDesc& q = qs[qi].q;
@@ -435,9 +437,10 @@ __global__ void __launch_bounds__(256) k_batch_init(const BatchQ* qs, const int6
 // in k_batch_init, one block per 2048 slots; block 0 of a query also emits
 // its all-ones-key side slot)
 __global__ void __launch_bounds__(kCompactThreads) k_batch_compact(const BatchQ* qs, const int64_t* blk_prefix,
-                                                                   int nq) {
-  const int qi = batch_query_of_block(blk_prefix, nq, blockIdx.x);
-  const int64_t b = int64_t(blockIdx.x) - blk_prefix[qi];
+                                                                   int nq, int64_t block0) {
+  const int64_t blk = block0 + int64_t(blockIdx.x);
+  const int qi = batch_query_of_block(blk_prefix, nq, blk);
+  const int64_t b = blk - blk_prefix[qi];
   const int64_t nb = blk_prefix[qi + 1] - blk_prefix[qi];
   const GTable t = qs[qi].gt;
   const QDesc q = qs[qi].q;
@@ -524,15 +527,15 @@ int gba_batch_sig_id(const QDesc& q) {
 }
 
 cudaError_t gba_launch_batch_init(const BatchQ* d_qs, const int64_t* blk_prefix, int nq, int64_t nblocks,
-                                  cudaStream_t s) {
-  if (nq <= 0) return cudaSuccess;
-  k_batch_init<<<unsigned(nblocks), 256, 0, s>>>(d_qs, blk_prefix, nq);
+                                  int64_t block0, cudaStream_t s) {
+  if (nq <= 0 || nblocks <= 0) return cudaSuccess;
+  k_batch_init<<<unsigned(nblocks), 256, 0, s>>>(d_qs, blk_prefix, nq, block0);
   return cudaGetLastError();
 }
 
 cudaError_t gba_launch_batch_compact(const BatchQ* d_qs, const int64_t* blk_prefix, int nq, int64_t nblocks,
-                                     cudaStream_t s) {
-  if (nq <= 0) return cudaSuccess;
-  k_batch_compact<<<unsigned(nblocks), kCompactThreads, 0, s>>>(d_qs, blk_prefix, nq);
+                                     int64_t block0, cudaStream_t s) {
+  if (nq <= 0 || nblocks <= 0) return cudaSuccess;
+  k_batch_compact<<<unsigned(nblocks), kCompactThreads, 0, s>>>(d_qs, blk_prefix, nq, block0);
   return cudaGetLastError();
 }
