@@ -439,8 +439,7 @@ def run_batch(args, ws, rank, local, pg):
         return {"use_tma": k.use_tma, "nstages": k.nstages, "coalesce": k.coalesce,
                 "blocks_per_sm": k.blocks_per_sm, "block_threads": k.block_threads,
                 "learned_load": k.learned_load, "load_factor": k.load_factor,
-                "item_rows": k.item_rows, "smem_probe_cap": k.smem_probe_cap, "table_slots": k.table_slots,
-                "split_mb": k.split_mb}
+                "item_rows": k.item_rows, "smem_probe_cap": k.smem_probe_cap, "table_slots": k.table_slots}
 
     pb = ctx.prepare_batch(dq, outs)
 

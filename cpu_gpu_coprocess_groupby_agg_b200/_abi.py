@@ -83,7 +83,6 @@ class Knobs(C.Structure):
         ("sort_output", C.c_int32),
         ("cluster_ctas", C.c_int32),
         ("exchange", C.c_int32),
-        ("split_mb", C.c_int32),
     ]
 
 

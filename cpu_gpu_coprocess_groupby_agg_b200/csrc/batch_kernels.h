@@ -10,11 +10,6 @@ struct BatchQ {
   unsigned* flags;  // this query's status bits
   int S;            // its shared-table slots (0 = no pre-aggregation)
   int pad;          // bit 0: keys and columns 16-byte aligned (vector loads)
-  // a query whose HBM table is built in 2^hbits passes has one entry per
-  // pass: entry hpart takes the rows whose table hash starts with hpart (its
-  // top hbits bits) into a table of its own, hashed by the remaining bits
-  int hbits;
-  int hpart;
 };
 
 // The work-queue items of one query, described at once: items first_item ..
@@ -34,14 +29,16 @@ int gba_batch_sig_id(const QDesc& q);
 // Streaming aggregation (k_stream.cu): one persistent launch over the nitems
 // work items of nspans query spans (item_rows a multiple of 256).  *item_ctr
 // must be zero at launch.  minb = CTAs per SM the launch is built for: 1 (512
-// threads with the whole shared memory and all registers), 2 or 4 (that many
-// such CTAs, each with its share of both).
+// threads with the whole shared memory and all registers), 2, 3 or 4 (that
+// many such CTAs, each with its share of both).  hbm: every query of the
+// launch has BatchQ.S == 0 (no shared table): a kernel without table code
+// (minb 2 or 3; others run the general kernel).
 size_t gba_stream_smem_bytes(const QDesc& q, int S);
 int gba_stream_rows_per_chunk(const QDesc& q, int minb);
-cudaError_t gba_prepare_stream_agg(const QDesc& proto, int minb);
-cudaError_t gba_launch_stream_agg(const QDesc& proto, int minb, const BatchQ* d_qs, const BatchSpan* d_spans,
-                                  int nspans, int64_t nitems, unsigned* item_ctr, size_t smem, int sprobe, int grid,
-                                  cudaStream_t s);
+cudaError_t gba_prepare_stream_agg(const QDesc& proto, int minb, bool hbm);
+cudaError_t gba_launch_stream_agg(const QDesc& proto, int minb, bool hbm, const BatchQ* d_qs,
+                                  const BatchSpan* d_spans, int nspans, int64_t nitems, unsigned* item_ctr,
+                                  size_t smem, int sprobe, int grid, cudaStream_t s);
 // Table init and compaction of the table entries whose blocks are block0 ..
 // block0 + nblocks - 1: blk_prefix[i] is the first block of entry i (entries
 // 0 .. nq - 1 searched, blk_prefix[nq] >= block0 + nblocks)

@@ -35,7 +35,6 @@ extern "C" void gba_default_knobs(gba_knobs* k) {
   k->max_regrow = 4;
   k->use_graph = -1;
   k->exchange = 0;  // owner exchange: opt-in until measured
-  k->split_mb = 0;
 }
 
 extern "C" const char* gba_status_string(gba_status s) {

@@ -67,8 +67,7 @@ struct QInfo {
   bool tma = false;  // streamed by the bulk-copy kernel (else the register-loading one)
   bool xch = false;  // aggregated by the owner-exchange kernel
   int hot = 0;       // exchange: hot-table slots per CTA
-  int slot = -1;     // index of its (first) entry among the table-strategy entries
-  int hbits = 0;     // its HBM table is built in 2^hbits passes over hash ranges (one entry each)
+  int slot = -1;     // index among the table-strategy queries
 };
 
 struct Group {
@@ -81,6 +80,7 @@ struct Group {
   int minb = 1;              // CTAs per SM of the launch
   int shape = 1;             // bulk-copy kernel: its CTA shape (1 or 2 CTAs of 512 threads per SM, 0: one of 1024)
   bool tma = false;          // bulk-copy kernel (k_stream_tma) or register-loading one (k_stream_agg)
+  bool hbm = false;          // register-loading kernel, queries without a shared table only
   int64_t item_begin = 0, nitems = 0;  // item_begin: index of the group's first span
   int entry_begin = 0, entry_end = 0;   // its table entries
   int nspans = 0;
@@ -479,29 +479,25 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   }
 
   // ---- group the table-strategy queries by aggregate signature (and cluster) ----
+  constexpr bool kHbmLaunch = true;
   std::vector<Group> groups;
-  std::vector<int> tq;     // table-strategy entries (query of each), group by group
-  std::vector<int> tpart;  // the hash range each entry builds (0 for a query in one pass)
-  // With knobs.split_mb > 0, a table larger than split_bytes is built in
-  // passes: its query gets one entry per hash range of at most split_bytes
-  // (up to 16), each with a table of its own, and the entries' items follow
-  // one another in the queue, so that one range's table stays in L2 while it
-  // is built; every entry reads all of the query's rows and keeps those of
-  // its range.  Off by default: measured on the batch's queries of >= 2^20
-  // ids (kernel ms), 1.99 in one pass, 2.69 in ranges of 64 MB, 3.88 of
-  // 32 MB, 6.04 of 16 MB; each pass pays every row's load, hash and chunk
-  // bookkeeping, which cost more than the DRAM round trips the L2-resident
-  // ranges save.
-  const double split_bytes = k.split_mb > 0 ? double(k.split_mb) * double(1 << 20) : 0.0;
+  std::vector<int> tq;  // table-strategy queries, group by group
   for (int i = 0; i < nq; ++i) {
     if (qi[i].strategy != GBA_STRATEGY_TABLE || qi[i].xch) continue;
     // one launch per signature, key width, kernel and cluster size
-    const int sig = ((2 * gba_batch_sig_id(qd[i]) + (qd[i].key64 ? 1 : 0)) * 2 + (qi[i].tma ? 1 : 0)) * 32 + qi[i].cl;
+    // register-loading queries without a shared table get a launch of their
+    // own, on the kernel built without table code (measured on the batch:
+    // 10.20 against 11.04 ms a step in one call)
+    const bool hbm = kHbmLaunch && !qi[i].tma && !qi[i].p.preagg;
+    const int sig =
+        (((2 * gba_batch_sig_id(qd[i]) + (qd[i].key64 ? 1 : 0)) * 2 + (qi[i].tma ? 1 : 0)) * 2 + (hbm ? 1 : 0)) * 32 +
+        qi[i].cl;
     auto it = std::find_if(groups.begin(), groups.end(), [&](const Group& g) { return g.sig == sig; });
     if (it == groups.end()) {
       groups.push_back(Group{sig, qd[i], {}});
       groups.back().cluster = qi[i].cl;
       groups.back().tma = qi[i].tma;
+      groups.back().hbm = hbm;
       it = groups.end() - 1;
     }
     it->members.push_back(i);
@@ -531,16 +527,8 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
       qi[i].S = S;
       g.smem = std::max(g.smem, g.tma ? gba_stream_tma_smem_bytes(qd[i], S, nst, g.stage_bytes, g.shape)
                                            : gba_stream_smem_bytes(qd[i], S));
-      qi[i].hbits = 0;
-      if (split_bytes > 0 && g.cluster == 1) {  // (a cluster's table is one table)
-        const double tb = double(qi[i].p.table_slots + 1) * 8.0 * double(gba_gt_stride(qd[i].naccs));
-        while (qi[i].hbits < 4 && tb / double(1 << qi[i].hbits) > split_bytes) ++qi[i].hbits;
-      }
       qi[i].slot = int(tq.size());
-      for (int p = 0; p < (1 << qi[i].hbits); ++p) {
-        tq.push_back(i);
-        tpart.push_back(p);
-      }
+      tq.push_back(i);
     }
     g.entry_end = int(tq.size());
     // a cluster launch fills as many clusters as can be resident at once;
@@ -576,7 +564,6 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
     it->smem = std::max(it->smem, gba_exchange_smem_bytes(qd[i], qi[i].S, qi[i].hot));
     qi[i].slot = int(tq.size());
     tq.push_back(i);
-    tpart.push_back(0);
     xwin = std::max<int64_t>(xwin, qd[i].n);
     xstride = std::max<int64_t>(xstride, 1 + qd[i].ncols);
     if (qi[i].hot) {  // hot tables leave as partial records of 1 + naccs words
@@ -631,11 +618,8 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
       ir = std::min(item_cap, std::max<int64_t>(T, (ir + T - 1) / T * T));
       const int64_t nit = (qd[i].n + ir - 1) / ir;
       if (nit == 0) continue;
-      // a table built in passes: the entries' items one after another
-      for (int p = 0; p < (1 << qi[i].hbits); ++p) {
-        spans.push_back(BatchSpan{qi[i].slot + p, 0, ir, first});
-        first += nit;
-      }
+      spans.push_back(BatchSpan{qi[i].slot, 0, ir, first});
+      first += nit;
     }
     g.nspans = int(int64_t(spans.size()) - g.item_begin);
     g.nitems = first;
@@ -677,17 +661,13 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   const size_t o_xstat = o_stat + 16 * size_t(nt) + 4 * size_t(ng);
   const size_t o_xbuf = nxq ? take(2 * size_t(xgrid) * size_t(xregion) * size_t(xstride) * 8) : 0;
   std::vector<size_t> o_tab(nt);
-  std::vector<uint64_t> tcap(nt);  // slots of each entry's table
   std::vector<int64_t> ipre(nt + 1, 0), cpre(nt + 1, 0);
   for (int j = 0; j < nt; ++j) {
     const QInfo& x = qi[tq[j]];
-    // one hash range's table: its share of the slots, with 1.6% and 64 slots
-    // to spare for the ranges' uneven group counts
-    tcap[j] = x.hbits ? (x.p.table_slots >> x.hbits) + (x.p.table_slots >> (x.hbits + 6)) + 64 : x.p.table_slots;
-    const size_t words = (tcap[j] + 1) * size_t(gba_gt_stride(x.q.naccs));
+    const size_t words = (x.p.table_slots + 1) * size_t(gba_gt_stride(x.q.naccs));
     o_tab[j] = take(words * 8);
     ipre[j + 1] = ipre[j] + int64_t(std::max<size_t>(1, (words + 256 * 16 - 1) / (256 * 16)));
-    cpre[j + 1] = cpre[j] + int64_t(std::max<uint64_t>(1, (tcap[j] + 2047) / 2048));
+    cpre[j + 1] = cpre[j] + int64_t(std::max<uint64_t>(1, (x.p.table_slots + 2047) / 2048));
   }
   if (nt > 0) {
     gba_status st = gba_ws_reserve(ctx, off, s);
@@ -706,18 +686,14 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
       std::memset(&b, 0, sizeof(b));
       b.q = qd[i];
       b.gt.base = reinterpret_cast<unsigned long long*>(d + o_tab[j]);
-      b.gt.cap = tcap[j];
+      b.gt.cap = qi[i].p.table_slots;
       b.gt.probe_cap = qi[i].p.probe_cap;
       b.out.keys = outs[i].keys;
       for (int a = 0; a < GBA_MAX_AGGS; ++a) b.out.accs[a] = static_cast<unsigned long long*>(outs[i].aggs[a]);
       b.out.capacity = outs[i].capacity;
-      // the entries of a query built in passes append to one output: the
-      // group counter of its first entry
-      b.out.count = reinterpret_cast<unsigned long long*>(d + o_stat + 16 * size_t(qi[i].slot) + 8);
+      b.out.count = reinterpret_cast<unsigned long long*>(d + o_stat + 16 * size_t(j) + 8);
       b.flags = reinterpret_cast<unsigned*>(d + o_stat + 16 * size_t(j));
       b.S = qi[i].S;
-      b.hbits = qi[i].hbits;
-      b.hpart = tpart[j];
       bool vec = aligned16(qd[i].keys);
       for (int c = 0; c < qd[i].ncols; ++c) vec = vec && aligned16(qd[i].cols[c]);
       // bits 8..15: buckets probed per row; a table the query's groups will
@@ -769,7 +745,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
                                                  d_spans + groups[g].item_begin, groups[g].nspans, groups[g].nitems,
                                                  d_ctr + g, groups[g].smem, sprobe, groups[g].grid, nst,
                                                  groups[g].stage_bytes, st)
-                         : gba_launch_stream_agg(groups[g].proto, bps, d_qs, d_spans + groups[g].item_begin,
+                         : gba_launch_stream_agg(groups[g].proto, bps, groups[g].hbm, d_qs, d_spans + groups[g].item_begin,
                                                  groups[g].nspans, groups[g].nitems, d_ctr + g, groups[g].smem,
                                                  sprobe, groups[g].grid, st);
   };
@@ -820,7 +796,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   if (nt > 0) {
     for (int g = 0; g < ng; ++g)
       GBA_CUDA_TRY(ctx, groups[g].tma ? gba_prepare_stream_tma(groups[g].proto, groups[g].cluster, groups[g].shape)
-                                   : gba_prepare_stream_agg(groups[g].proto, bps));
+                                   : gba_prepare_stream_agg(groups[g].proto, bps, groups[g].hbm));
     if (as_graph) {
       // the graph depends only on launch shapes and buffer addresses
       std::vector<int64_t> key = {nt,
@@ -891,10 +867,9 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
       if (cudaEventElapsedTime(&ms, ctx->tev[r], ctx->tev[r + 1]) == cudaSuccess) ctx->stats.kernel_ms[r] += ms;
     }
     ctx->stats.kernel_launches += 2 + ng + int(xgroups.size());
-    for (int j = 0; j < nt; ++j) {
-      if (tpart[j]) continue;  // a query's rows count once, whatever its passes
-      ctx->stats.main_rows += qd[tq[j]].n;
-      ctx->stats.main_bytes += qd[tq[j]].n * int64_t(gba_row_bytes(qd[tq[j]]));
+    for (int i : tq) {
+      ctx->stats.main_rows += qd[i].n;
+      ctx->stats.main_bytes += qd[i].n * int64_t(gba_row_bytes(qd[i]));
     }
   }
 
@@ -906,16 +881,10 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
     return GBA_ERR_TIMEOUT;
   }
   std::vector<int> rerun;
-  // a query's status: the bits of all its entries; its group count: its first entry's counter
-  std::vector<unsigned> qflags(nq, 0u);
   for (int j = 0; j < nt; ++j) {
-    qflags[tq[j]] |= *reinterpret_cast<const unsigned*>(h + h_stat + 16 * size_t(j));
-    acc.table_slots += int64_t(tcap[j]);
-  }
-  for (int j = 0; j < nt; ++j) {
-    if (tpart[j]) continue;
     const int i = tq[j];
-    const unsigned flags = qflags[i];
+    const unsigned flags = *reinterpret_cast<const unsigned*>(h + h_stat + 16 * size_t(j));
+    acc.table_slots += int64_t(qi[i].p.table_slots);
     const unsigned long long cnt = *reinterpret_cast<const unsigned long long*>(h + h_stat + 16 * size_t(j) + 8);
     if (flags & GBA_FLAG_WAIT_TIMEOUT) {
       ctx->err = "query " + std::to_string(i) + ": a bounded device wait timed out";
@@ -973,7 +942,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   trace.mark("partition_queries_and_reruns");
   acc.strategy = nt == nq ? GBA_STRATEGY_TABLE : (nt == 0 ? GBA_STRATEGY_PARTITION : GBA_STRATEGY_AUTO);
   acc.preagg = 0;
-  for (int j = 0; j < nt; ++j) acc.preagg += tpart[j] == 0 && qi[tq[j]].S > 0;
+  for (int j = 0; j < nt; ++j) acc.preagg += qi[tq[j]].S > 0;
   acc.n_groups = 0;
   for (int i = 0; i < nq; ++i) acc.n_groups += n_groups[i];
   ctx->stats = acc;

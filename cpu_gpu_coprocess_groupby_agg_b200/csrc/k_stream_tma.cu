@@ -324,11 +324,11 @@ __global__ void __launch_bounds__(tma_threads<MINB>(), tma_ctas_per_sm<MINB>())
     if (s_abort) dead = true;
     if constexpr (CL > 1) {
       cluster_sync_all();  // every row of the item applied, in every CTA's table part
-      if (!dead && s_q.S > 0) smem_flush_to_gtable<K64, Sig>(q, s_q.gt, st, s_q.flags, s_q.hbits);
+      if (!dead && s_q.S > 0) smem_flush_to_gtable<K64, Sig>(q, s_q.gt, st, s_q.flags);
       __syncthreads();  // s_q and the table are rewritten by the next item
     } else {
       if (dead) return;
-      if (s_q.S > 0) smem_flush_to_gtable<K64, Sig>(q, s_q.gt, st, s_q.flags, s_q.hbits);
+      if (s_q.S > 0) smem_flush_to_gtable<K64, Sig>(q, s_q.gt, st, s_q.flags);
       __syncthreads();  // s_q and the table are rewritten by the next item
     }
   }

@@ -203,19 +203,17 @@ __device__ __forceinline__ unsigned long long smem_acc_read(const SmemTable<K64>
 // init all slots (called by the whole CTA; caller syncs): every accumulator
 // word starts at its op's identity (fixed-point words and residual at 0)
 // Merges every group of a shared table into an HBM table (all threads of the
-// block; the caller syncs before and after).  hshift: the table is hashed by
-// the table hash shifted left by that many bits (one hash range of a table
-// built in passes).
+// block; the caller syncs before and after).
 template <bool K64, typename Sig>
 __device__ __forceinline__ void smem_flush_to_gtable(const QDesc& q, const GTable& gt, const SmemTable<K64>& st,
-                                                     unsigned* flags, int hshift = 0) {
+                                                     unsigned* flags) {
   for (int i = threadIdx.x; i < st.S; i += blockDim.x) {
     const uint64_t k = st.keys[i];
     if (k == uint64_t(smem_empty_key<K64>())) continue;
     unsigned long long v[Sig::NA];
 #pragma unroll
     for (int a = 0; a < Sig::NA; ++a) v[a] = smem_acc_read<K64, Sig>(st, q, a, i);
-    gtable_insert<K64, Sig>(gt, q, k, hshift > 0 ? table_hash(k) << hshift : table_hash(k), v, flags);
+    gtable_insert<K64, Sig>(gt, q, k, table_hash(k), v, flags);
   }
   if (threadIdx.x == 0 && *st.side_present()) {
     unsigned long long v[Sig::NA];

@@ -215,36 +215,17 @@ __device__ __forceinline__ unsigned smem_rows(const SmemTable<K64>& st, const QD
   return miss;
 }
 
-// The table hashes of a thread's R rows, and which of them the entry takes:
-// an entry that builds one hash range of its query's table (BatchQ.hbits > 0)
-// takes the rows whose hash starts with its range number (hpart) and hashes
-// them by their remaining bits.
-template <int R>
-__device__ __forceinline__ void entry_hashes(const BatchQ& bq, const uint64_t (&key)[R], const bool (&live)[R],
-                                             uint32_t (&h)[R], bool (&take)[R]) {
-  const int hb = bq.hbits;
-#pragma unroll
-  for (int i = 0; i < R; ++i) {
-    h[i] = table_hash(key[i]);
-    take[i] = live[i];
-    if (hb > 0) {
-      take[i] = take[i] && (h[i] >> (32 - hb)) == unsigned(bq.hpart);
-      h[i] <<= hb;
-    }
-  }
-}
-
 // A thread's R rows into the item's shared table, or, for rows whose key is
 // not in it and cannot enter it, into the query's HBM table.
 template <bool K64, typename Sig, int R>
 __device__ __forceinline__ void stream_rows(const BatchQ& bq, const SmemTable<K64>& st, int nbk, const uint64_t (&key)[R],
-                                            const unsigned long long (&v)[R][Sig::NA], const bool (&live0)[R]) {
+                                            const unsigned long long (&v)[R][Sig::NA], const bool (&live)[R]) {
   const QDesc& q = bq.q;
   const uint64_t emptyk = K64 ? EMPTY64 : uint64_t(EMPTY32);
   unsigned miss = 0;
   uint32_t h[R];
-  bool live[R];
-  entry_hashes<R>(bq, key, live0, h, live);
+#pragma unroll
+  for (int i = 0; i < R; ++i) h[i] = table_hash(key[i]);
   if (bq.S > 0) {
     miss = smem_rows<K64, Sig, R>(st, q, nbk, key, v, live, h);
   } else {
@@ -257,6 +238,24 @@ __device__ __forceinline__ void stream_rows(const BatchQ& bq, const SmemTable<K6
   }
   if (miss == 0) return;
   hbm_rows<K64, Sig, R>(bq, key, v, h, miss);
+}
+
+// A thread's R rows straight into the query's HBM table (a query without a
+// shared table: BatchQ.S == 0).
+template <bool K64, typename Sig, int R>
+__device__ __forceinline__ void stream_rows_hbm(const BatchQ& bq, const uint64_t (&key)[R],
+                                                const unsigned long long (&v)[R][Sig::NA], const bool (&live)[R]) {
+  const uint64_t emptyk = K64 ? EMPTY64 : uint64_t(EMPTY32);
+  uint32_t h[R];
+  unsigned miss = 0;
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    h[i] = table_hash(key[i]);
+    if (!live[i]) continue;
+    if (key[i] == emptyk) gtable_insert<K64, Sig>(bq.gt, bq.q, key[i], 0u, v[i], bq.flags);
+    else miss |= 1u << i;
+  }
+  if (miss) hbm_rows<K64, Sig, R>(bq, key, v, h, miss);
 }
 
 // ---------------------------------------------------------------------------

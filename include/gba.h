@@ -164,10 +164,6 @@ typedef struct gba_knobs {
                              learned sizing, queries of at least 2^19 rows whose predicted groups
                              outgrow one CTA's table but fit the SMs' tables together, without a key
                              taking 1/32 of the sample */
-  int32_t split_mb;       /* batch, opt-in: a query whose HBM table exceeds this many MB builds it in
-                             passes over hash ranges of at most that size (up to 16), one range's table
-                             at a time in L2, each pass reading all its rows (0 or -1 = one pass, the
-                             default: measured slower, every pass pays each row's load and hash) */
 } gba_knobs;
 
 /* What the last call on a context did. */

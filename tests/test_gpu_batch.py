@@ -81,9 +81,7 @@ def test_batch_graph_replay_and_direct_launch_agree(ctx):
                                    dict(coalesce=1, smem_slots=64), dict(sizing="grow"),
                                    dict(sizing="grow", table_slots=256), dict(use_tma=1, block_threads=512),
                                    dict(use_tma=1, block_threads=1024, nstages=4, coalesce=1),
-                                   dict(sizing="learned", block_threads=512), dict(split_mb=1),
-                                   dict(split_mb=1, use_tma=1), dict(split_mb=1, use_tma=0, sizing="learned"),
-                                   dict(split_mb=-1)])
+                                   dict(sizing="learned", block_threads=512)])
 def test_batch_knobs_do_not_change_results(ctx, knobs):
     qs = _queries(12, seed=7)
     _check(qs, ctx.groupby_batch(_device(qs), knobs=knobs), str(knobs))
@@ -262,23 +260,3 @@ def test_batch_host_pageable_and_empty(ctx):
     r = ctx.groupby_batch_host(one, _host_outs(one))[0]
     compare(r.keys, r.aggs, *one[0], "batch of one")
 
-
-def test_batch_tables_built_in_passes(ctx):
-    """Tables split over hash ranges (split_mb=1: every table above 1 MB gets
-    up to 16 entries, one per range), with the all-ones key in some queries,
-    and an overflowing split table that reruns its query alone."""
-    qs = []
-    for i, (n, kdt, ndv) in enumerate([(300_000, np.int64, 120_000), (250_000, np.uint32, 90_000),
-                                       (200_000, np.int32, 2_000), (400_000, np.int64, 300_000)]):
-        keys, cols = _data(n, kdt, ndv, seed=500 + i, zipf=0.3 * i)
-        if i % 2 == 0:
-            keys[::97] = np.array(-1).astype(kdt)  # the all-ones key (the tables' empty marker)
-        else:
-            keys[::89] = np.iinfo(kdt).max if kdt == np.uint32 else keys[::89]
-        qs.append((keys, cols, AGGS_ALL if i % 2 else [("sum", 0), ("count", None), ("max", 0)]))
-    for knobs in (dict(split_mb=1), dict(split_mb=1, sizing="learned"), dict(split_mb=1, use_tma=1)):
-        _check(qs, ctx.groupby_batch(_device(qs), knobs=knobs), f"passes {knobs}")
-    res = ctx.groupby_batch(_device(qs), knobs=dict(split_mb=1, sizing="fixed", table_slots=200_000, probe_cap=16,
-                                                     max_regrow=8, strategy="table"))
-    _check(qs, res, "passes with overflow")
-    assert res[0].stats["regrows"] >= 1
