@@ -480,6 +480,9 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
 
   // ---- group the table-strategy queries by aggregate signature (and cluster) ----
   constexpr bool kHbmLaunch = true;
+  // CTAs per SM of that launch: measured 10.09 ms a step at 3 (40 registers,
+  // 2 rows per lane) against 10.20 at 2 (4 rows per lane, no spills)
+  constexpr int kHbmCtas = 3;
   std::vector<Group> groups;
   std::vector<int> tq;  // table-strategy queries, group by group
   for (int i = 0; i < nq; ++i) {
@@ -505,7 +508,9 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   for (auto& g : groups) {
     g.smem = gba_stream_smem_bytes(g.proto, 0);
     g.shape = g.cluster > 1 ? 1 : tshape;
-    g.minb = !g.tma ? bps : (g.shape == 2 ? 2 : 1);
+    // (the launch of queries without a shared table: kHbmCtas CTAs per SM
+    // unless blocks_per_sm is set)
+    g.minb = !g.tma ? (g.hbm && k.blocks_per_sm <= 0 ? kHbmCtas : bps) : (g.shape == 2 ? 2 : 1);
     if (g.tma) {
       // one ring slot holds a chunk of any member (run-time signatures may
       // differ in columns per member)
@@ -745,7 +750,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
                                                  d_spans + groups[g].item_begin, groups[g].nspans, groups[g].nitems,
                                                  d_ctr + g, groups[g].smem, sprobe, groups[g].grid, nst,
                                                  groups[g].stage_bytes, st)
-                         : gba_launch_stream_agg(groups[g].proto, bps, groups[g].hbm, d_qs, d_spans + groups[g].item_begin,
+                         : gba_launch_stream_agg(groups[g].proto, groups[g].minb, groups[g].hbm, d_qs, d_spans + groups[g].item_begin,
                                                  groups[g].nspans, groups[g].nitems, d_ctr + g, groups[g].smem,
                                                  sprobe, groups[g].grid, st);
   };
@@ -796,7 +801,7 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   if (nt > 0) {
     for (int g = 0; g < ng; ++g)
       GBA_CUDA_TRY(ctx, groups[g].tma ? gba_prepare_stream_tma(groups[g].proto, groups[g].cluster, groups[g].shape)
-                                   : gba_prepare_stream_agg(groups[g].proto, bps, groups[g].hbm));
+                                   : gba_prepare_stream_agg(groups[g].proto, groups[g].minb, groups[g].hbm));
     if (as_graph) {
       // the graph depends only on launch shapes and buffer addresses
       std::vector<int64_t> key = {nt,
