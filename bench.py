@@ -702,6 +702,7 @@ def run_serve(args, ws, rank, local, pg):
             collect(1.0)
         t_end = time.perf_counter()
         err = sv._lib.gba_server_last_error(sv._h).decode()
+        counters = sv.counters()
         sv.close()
         bad = [x for x, _, _ in infos if x.status != 0]
         if bad:
@@ -718,6 +719,7 @@ def run_serve(args, ws, rank, local, pg):
                 "seconds": round(t_end - t0, 3), "offered_seconds": round(float(np.sum(gaps)), 3),
                 "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
                 "mean_batch": round(float(np.mean([x.batch_size for x, _, _ in infos])), 2),
+                "service_p99_ms": pct(svc, 99), "server": counters,
                 "large_requests": {"count": int(big.sum()), "p50_ms": pct(lat[big], 50), "p99_ms": pct(lat[big], 99),
                                    "service_p50_ms": pct(svc[big], 50)},
                 "small_requests": {"count": int((~big).sum()), "p50_ms": pct(lat[~big], 50),

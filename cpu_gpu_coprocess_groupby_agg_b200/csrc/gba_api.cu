@@ -116,8 +116,29 @@ extern "C" gba_status gba_last_stats(const gba_context* ctx, gba_stats* out) {
   return GBA_OK;
 }
 
+// Device buffers grow to at least 1.5 times their old size, so that a
+// workload whose calls need a little more each time (a server's batches of
+// varying shapes) reallocates a few times, not at every new high: each
+// reallocation synchronises the device, stalling every stream on it.  If the
+// larger block does not fit, the exact size is tried.
+static cudaError_t grow_alloc(void** p, size_t bytes, size_t cur, size_t min_bytes, size_t* got) {
+  const size_t exact = gba_round_up(std::max(bytes, min_bytes), size_t(1) << 21);
+  const size_t roomy = gba_round_up(std::max(exact, cur + cur / 2), size_t(1) << 21);
+  cudaError_t e = cudaMalloc(p, roomy);
+  if (e == cudaSuccess) {
+    *got = roomy;
+    return e;
+  }
+  cudaGetLastError();
+  if (roomy == exact) return e;
+  e = cudaMalloc(p, exact);
+  if (e == cudaSuccess) *got = exact;
+  return e;
+}
+
 gba_status gba_ws_reserve(gba_context* ctx, size_t bytes, cudaStream_t s) {
   if (bytes <= ctx->ws_bytes) return GBA_OK;
+  const size_t cur = ctx->ws_bytes;
   if (ctx->ws) {
     GBA_CUDA_TRY(ctx, cudaStreamSynchronize(s));
     GBA_CUDA_TRY(ctx, cudaDeviceSynchronize());
@@ -125,12 +146,12 @@ gba_status gba_ws_reserve(gba_context* ctx, size_t bytes, cudaStream_t s) {
     ctx->ws = nullptr;
     ctx->ws_bytes = 0;
   }
-  const size_t want = gba_round_up(std::max(bytes, size_t(1) << 24), size_t(1) << 21);
-  cudaError_t e = cudaMalloc(&ctx->ws, want);
+  size_t want = 0;
+  cudaError_t e = grow_alloc(&ctx->ws, bytes, cur, size_t(1) << 24, &want);
   if (e != cudaSuccess) {
     cudaGetLastError();
     ctx->ws = nullptr;
-    ctx->err = std::string("workspace cudaMalloc(") + std::to_string(want) + "): " + cudaGetErrorString(e);
+    ctx->err = std::string("workspace cudaMalloc(") + std::to_string(bytes) + "): " + cudaGetErrorString(e);
     return GBA_ERR_OOM;
   }
   ctx->ws_bytes = want;
@@ -139,6 +160,7 @@ gba_status gba_ws_reserve(gba_context* ctx, size_t bytes, cudaStream_t s) {
 
 gba_status gba_stage_reserve(gba_context* ctx, size_t bytes, cudaStream_t s) {
   if (bytes <= ctx->stage_bytes) return GBA_OK;
+  const size_t cur = ctx->stage_bytes;
   if (ctx->stage) {
     GBA_CUDA_TRY(ctx, cudaStreamSynchronize(s));
     GBA_CUDA_TRY(ctx, cudaDeviceSynchronize());
@@ -146,12 +168,12 @@ gba_status gba_stage_reserve(gba_context* ctx, size_t bytes, cudaStream_t s) {
     ctx->stage = nullptr;
     ctx->stage_bytes = 0;
   }
-  const size_t want = gba_round_up(std::max(bytes, size_t(1) << 24), size_t(1) << 21);
-  cudaError_t e = cudaMalloc(&ctx->stage, want);
+  size_t want = 0;
+  cudaError_t e = grow_alloc(&ctx->stage, bytes, cur, size_t(1) << 24, &want);
   if (e != cudaSuccess) {
     cudaGetLastError();
     ctx->stage = nullptr;
-    ctx->err = std::string("staging cudaMalloc(") + std::to_string(want) + "): " + cudaGetErrorString(e);
+    ctx->err = std::string("staging cudaMalloc(") + std::to_string(bytes) + "): " + cudaGetErrorString(e);
     return GBA_ERR_OOM;
   }
   ctx->stage_bytes = want;
@@ -160,6 +182,7 @@ gba_status gba_stage_reserve(gba_context* ctx, size_t bytes, cudaStream_t s) {
 
 gba_status gba_est_reserve(gba_context* ctx, size_t bytes, cudaStream_t s) {
   if (bytes <= ctx->est_ws_bytes) return GBA_OK;
+  const size_t cur = ctx->est_ws_bytes;
   if (ctx->est_ws) {
     GBA_CUDA_TRY(ctx, cudaStreamSynchronize(s));
     GBA_CUDA_TRY(ctx, cudaDeviceSynchronize());
@@ -167,18 +190,19 @@ gba_status gba_est_reserve(gba_context* ctx, size_t bytes, cudaStream_t s) {
     ctx->est_ws = nullptr;
     ctx->est_ws_bytes = 0;
   }
-  const size_t want = gba_round_up(std::max(bytes, size_t(1) << 22), size_t(1) << 21);
-  GBA_CUDA_TRY(ctx, cudaMalloc(&ctx->est_ws, want));
+  size_t want = 0;
+  GBA_CUDA_TRY(ctx, grow_alloc(&ctx->est_ws, bytes, cur, size_t(1) << 22, &want));
   ctx->est_ws_bytes = want;
   return GBA_OK;
 }
 
 gba_status gba_batch_host_reserve(gba_context* ctx, size_t bytes) {
   if (bytes <= ctx->h_batch_bytes) return GBA_OK;
+  const size_t prev = ctx->h_batch_bytes;  // pinned buffers grow by 1.5 times too
   if (ctx->h_batch) cudaFreeHost(ctx->h_batch);
   ctx->h_batch = nullptr;
   ctx->h_batch_bytes = 0;
-  const size_t want = gba_round_up(std::max(bytes, size_t(1) << 20), size_t(1) << 16);
+  const size_t want = gba_round_up(std::max({bytes, size_t(1) << 20, prev + prev / 2}), size_t(1) << 16);
   GBA_CUDA_TRY(ctx, cudaMallocHost(&ctx->h_batch, want));
   ctx->h_batch_bytes = want;
   return GBA_OK;

@@ -68,6 +68,10 @@ struct gba_server {
   gba_context* admin = nullptr;  // validates queries at submit (under mu)
   std::string last_failure;      // message of the latest failed request (or failed batch)
   int64_t batch_failures = 0;    // batch calls that failed and were rerun request by request
+  // where the time goes: lane calls, the longest one, workspace releases
+  // (a release synchronises the device) and the longest of them
+  int64_t lane_calls = 0, ws_releases = 0;
+  double lane_ms_max = 0.0, release_ms_max = 0.0;
 };
 
 static int64_t ctx_resident_bytes(const gba_context* c) {
@@ -161,6 +165,7 @@ static void lane_main(gba_server* sv, int lane) {
       }
     }
     const auto t_end = Clock::now();
+    const double call_ms = nb ? ms_between(take[0]->t_start, t_end) : 0.0;
     // release the workspace if the lanes together hold more than the budget
     int64_t mine = ctx_resident_bytes(ctx);
     {
@@ -168,12 +173,17 @@ static void lane_main(gba_server* sv, int lane) {
       int64_t total = 0;
       for (int64_t b : sv->resident) total += b;
       total += mine - sv->resident[lane];
+      ++sv->lane_calls;
+      sv->lane_ms_max = std::max(sv->lane_ms_max, call_ms);
       if (total > sv->cfg.memory_budget && ctx->ws) {
+        const auto t_rel = Clock::now();
         cudaStreamSynchronize(s);
         cudaFree(ctx->ws);
         ctx->ws = nullptr;
         ctx->ws_bytes = 0;
         mine = ctx_resident_bytes(ctx);
+        ++sv->ws_releases;
+        sv->release_ms_max = std::max(sv->release_ms_max, ms_between(t_rel, Clock::now()));
       }
       sv->resident[lane] = mine;
       for (Request* r : take)
@@ -236,11 +246,26 @@ extern "C" gba_status gba_server_create(gba_server** out, const gba_server_confi
     return st;
   }
   cudaSetDevice(c.device);
+  // Each lane reserves 90% of its share of the budget up front as workspace
+  // (at most 60% of the device's free memory between the lanes), and learned
+  // sizing's sampling scratch and the batch descriptors' pinned staging too,
+  // so that serving rarely grows a buffer: a growth frees the old block, and
+  // cudaFree synchronises the device, stalling every lane.  (The other 10%
+  // covers those smaller buffers, so the lanes together stay within the
+  // budget and keep their workspaces.)
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = 0;
+  const size_t share = std::min<size_t>(size_t(c.memory_budget) / size_t(c.lanes) / 10 * 9,
+                                        free_b / 10 * 6 / size_t(c.lanes));
+  const size_t est_share = std::min<size_t>(size_t(512) << 20, size_t(c.memory_budget) / size_t(c.lanes) / 20);
   for (int i = 0; i < c.lanes; ++i) {
     gba_context* ctx = nullptr;
     cudaStream_t s = nullptr;
     st = gba_create(&ctx, c.device);
     if (st == GBA_OK && cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) st = GBA_ERR_CUDA;
+    if (st == GBA_OK && share > 0) st = gba_ws_reserve(ctx, share, s);
+    if (st == GBA_OK && c.knobs.sizing == GBA_SIZING_LEARNED && est_share > 0) st = gba_est_reserve(ctx, est_share, s);
+    if (st == GBA_OK) st = gba_batch_host_reserve(ctx, size_t(4) << 20);
     if (st != GBA_OK) {
       if (ctx) gba_destroy(ctx);
       for (size_t j = 0; j < sv->ctxs.size(); ++j) {
@@ -345,6 +370,18 @@ extern "C" gba_status gba_server_pending(gba_server* sv, int64_t* queued, int64_
   if (queued) *queued = int64_t(sv->queue.size());
   if (running) *running = sv->submitted - sv->finished - int64_t(sv->queue.size());
   if (inflight_bytes) *inflight_bytes = sv->inflight_bytes;
+  return GBA_OK;
+}
+
+extern "C" gba_status gba_server_counters(gba_server* sv, int64_t* lane_calls, int64_t* batch_failures,
+                                          int64_t* ws_releases, double* lane_ms_max, double* release_ms_max) {
+  if (!sv) return GBA_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(sv->mu);
+  if (lane_calls) *lane_calls = sv->lane_calls;
+  if (batch_failures) *batch_failures = sv->batch_failures;
+  if (ws_releases) *ws_releases = sv->ws_releases;
+  if (lane_ms_max) *lane_ms_max = sv->lane_ms_max;
+  if (release_ms_max) *release_ms_max = sv->release_ms_max;
   return GBA_OK;
 }
 

@@ -77,7 +77,9 @@ def test_results_same_alone_and_in_the_mix(sizing):
     outs = [_outputs(k, c, aggs) for (sp, n, aggs), (k, c) in zip(reqs, data)]
     tickets = [sv.submit(k, c, aggs, o) for (sp, n, aggs), (k, c), o in zip(reqs, data, outs)]
     infos = [sv.wait(t, timeout=120) for t in tickets]
+    cnt = sv.counters()
     sv.close()
+    assert cnt["lane_calls"] >= 1 and cnt["batch_failures"] == 0 and cnt["lane_ms_max"] > 0, cnt
     assert max(i.batch_size for i in infos) > 1, "no request ran in a batch"
     assert len({i.lane for i in infos}) > 1, "only one lane ran"
     assert infos[-1].batch_size == 1, "the large request should run alone"
@@ -113,7 +115,9 @@ def test_budget_refuses_oversized_and_admits_within():
     outs = [_outputs(k, c, [("sum", 0)]) for _ in range(6)]
     ts = [sv.submit(k, c, [("sum", 0)], o) for o in outs]
     infos = [sv.wait(t) for t in ts]
+    cnt = sv.counters()
     sv.close()
+    assert cnt["lane_calls"] >= 2 and cnt["ws_releases"] >= 0 and cnt["release_ms_max"] >= 0, cnt
     assert all(i.status == A.OK and i.n_groups == infos[0].n_groups for i in infos)
     assert infos[0].n_groups == len(np.unique(k.cpu().numpy()))
 
