@@ -375,7 +375,10 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   // register-loading vs bulk-copy): ids < 256: 0.69 vs 0.89; 256-4096: 1.47 vs
   // 1.53; 4096-16384: 1.60 vs 1.40; 16384-65536: 2.60 vs 2.36; 65536-262144:
   // 1.32 vs 1.04; 262144-2^20: 2.35 vs 2.25; above 2^20: 2.94 vs 2.65.
-  const int nst = k.nstages >= 1 && k.nstages <= 4 ? k.nstages : 3;
+  // ring slots per warp (automatic 2: measured 10.04-10.07 ms a step against
+  // 10.16-10.22 with 3, whose larger rings leave less shared memory to the
+  // tables of the 1024-thread CTAs)
+  const int nst = k.nstages >= 1 && k.nstages <= 4 ? k.nstages : 2;
   const int bps = k.blocks_per_sm >= 1 && k.blocks_per_sm <= 4 ? k.blocks_per_sm : 3;
   // bulk-copy kernel CTA shape: one CTA of 1024 threads per SM (automatic;
   // one shared table of twice the slots for as many warps as two 512-thread

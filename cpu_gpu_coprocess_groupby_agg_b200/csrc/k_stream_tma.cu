@@ -56,8 +56,8 @@ __host__ __device__ constexpr int tma_ctas_per_sm() {
 
 // rows per lane per chunk: fewer with more accumulators, and fewer when an
 // SM holds 32 warps (their registers are split).  With 16-byte rows a slot
-// holds 2 KB (16 warps per SM) or 1 KB (32), so three slots per warp keep
-// about 64 KB of copies in flight per SM and leave the rest of the shared
+// holds 2 KB (16 warps per SM) or 1 KB (32), so two or three slots per warp
+// keep 64-96 KB of copies in flight per SM and leave the rest of the shared
 // memory to the tables.
 template <typename Sig, int MINB>
 __host__ __device__ constexpr int tma_rows_per_lane() {
