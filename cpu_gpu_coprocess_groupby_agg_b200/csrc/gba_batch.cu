@@ -318,6 +318,10 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
   gba_knobs k;
   if (knobs) k = *knobs;
   else gba_default_knobs(&k);
+  // A batch's learned-sized tables default to load 0.25 (a single query's to
+  // 0.35): measured on the 256-query batch, 9.92 against 10.00 ms a step
+  // (the autotuner's usual pick there too)
+  if (!(k.learned_load > 0.05 && k.learned_load < 0.95)) k.learned_load = 0.25;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   PhaseTrace trace;
 
@@ -392,7 +396,8 @@ static gba_status batch_device(gba_context* ctx, int32_t nq, const gba_query* qs
                                                                                               : 0;
   bool any_tma = false;
   // buckets probed in a shared table before a row goes to the HBM table
-  const int sprobe = k.smem_probe_cap > 0 ? k.smem_probe_cap : 2;
+  // (automatic 4: 9.87 against 9.92 ms a step with 2, at load 0.25)
+  const int sprobe = k.smem_probe_cap > 0 ? k.smem_probe_cap : 4;
   // Strategy: a query alone leaves the HBM-table strategy once its table
   // outgrows L2 (gba_choose_strategy), but in a batch such a query still runs
   // inside the shared persistent launch, while a partition-strategy query runs

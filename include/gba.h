@@ -147,7 +147,8 @@ typedef struct gba_knobs {
   int32_t timing;         /* 1: time each kernel with CUDA events (gba_stats.kernel_ms) */
   int32_t use_graph;      /* batch: -1 auto (on), 0 off, 1 on: replay the launch sequence as a CUDA graph */
   int32_t item_rows;      /* batch: rows per work-queue item (0 = auto) */
-  double learned_load;    /* learned sizing: HBM table load at the predicted group count (0 = auto, 0.35) */
+  double learned_load;    /* learned sizing: HBM table load at the predicted group count (0 = auto: 0.35 for
+                             one query, 0.25 in a batch) */
   int64_t learned_min_rows; /* single query, learned sizing: smaller queries are sized plainly
                                (0 = auto: while the plain table is <= 256 MB; -1 = always estimate) */
   int32_t sort_output;    /* gba_groupby, gba_groupby_batch, gba_groupby_host: 1 = groups in ascending key
