@@ -172,7 +172,7 @@ SIGNATURES = {
     "gba_server_pending": (C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "gba_server_last_error": (C.c_char_p, [_P]),
     "gba_server_counters": (C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
-                                      C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+                                      C.POINTER(C.c_int64), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "gba_server_destroy": (C.c_int, [_P]),
     "gba_estimator_features": (C.c_int, [_P, C.POINTER(Query), C.c_int64, _P, C.POINTER(C.c_float)]),
     "gba_estimator_param_count": (C.c_int64, []),

@@ -575,13 +575,13 @@ class Server:
         return q.value, r.value, b.value
 
     def counters(self) -> dict:
-        """Lane calls, failed batches, workspace releases, and the longest lane
-        call and release (ms) so far (gba_server_counters)."""
-        n, f, rel = C.c_int64(0), C.c_int64(0), C.c_int64(0)
+        """Lane calls, failed batches, workspace releases, overflow reruns, and
+        the longest lane call and release (ms) so far (gba_server_counters)."""
+        n, f, rel, rg = C.c_int64(0), C.c_int64(0), C.c_int64(0), C.c_int64(0)
         lm, rm = C.c_double(0), C.c_double(0)
-        self._check(self._lib.gba_server_counters(self._h, C.byref(n), C.byref(f), C.byref(rel), C.byref(lm),
-                                                  C.byref(rm)))
-        return {"lane_calls": n.value, "batch_failures": f.value, "ws_releases": rel.value,
+        self._check(self._lib.gba_server_counters(self._h, C.byref(n), C.byref(f), C.byref(rel), C.byref(rg),
+                                                  C.byref(lm), C.byref(rm)))
+        return {"lane_calls": n.value, "batch_failures": f.value, "ws_releases": rel.value, "regrows": rg.value,
                 "lane_ms_max": round(lm.value, 3), "release_ms_max": round(rm.value, 3)}
 
     def close(self):

@@ -70,7 +70,7 @@ struct gba_server {
   int64_t batch_failures = 0;    // batch calls that failed and were rerun request by request
   // where the time goes: lane calls, the longest one, workspace releases
   // (a release synchronises the device) and the longest of them
-  int64_t lane_calls = 0, ws_releases = 0;
+  int64_t lane_calls = 0, ws_releases = 0, regrows = 0;
   double lane_ms_max = 0.0, release_ms_max = 0.0;
 };
 
@@ -174,6 +174,7 @@ static void lane_main(gba_server* sv, int lane) {
       for (int64_t b : sv->resident) total += b;
       total += mine - sv->resident[lane];
       ++sv->lane_calls;
+      sv->regrows += ctx->stats.regrows;
       sv->lane_ms_max = std::max(sv->lane_ms_max, call_ms);
       if (total > sv->cfg.memory_budget && ctx->ws) {
         const auto t_rel = Clock::now();
@@ -374,10 +375,12 @@ extern "C" gba_status gba_server_pending(gba_server* sv, int64_t* queued, int64_
 }
 
 extern "C" gba_status gba_server_counters(gba_server* sv, int64_t* lane_calls, int64_t* batch_failures,
-                                          int64_t* ws_releases, double* lane_ms_max, double* release_ms_max) {
+                                          int64_t* ws_releases, int64_t* regrows, double* lane_ms_max,
+                                          double* release_ms_max) {
   if (!sv) return GBA_ERR_INVALID_ARG;
   std::lock_guard<std::mutex> lk(sv->mu);
   if (lane_calls) *lane_calls = sv->lane_calls;
+  if (regrows) *regrows = sv->regrows;
   if (batch_failures) *batch_failures = sv->batch_failures;
   if (ws_releases) *ws_releases = sv->ws_releases;
   if (lane_ms_max) *lane_ms_max = sv->lane_ms_max;

@@ -351,10 +351,11 @@ gba_status gba_server_pending(gba_server* sv, int64_t* queued, int64_t* running,
 /* Where the server's time went so far (any pointer may be null): lane calls
  * made, batch calls that failed and were rerun request by request, workspace
  * releases (a lane frees its workspace when the lanes together hold more than
- * the budget; cudaFree synchronises the device), the longest lane call and the
- * longest release in milliseconds. */
+ * the budget; cudaFree synchronises the device), queries rerun with a larger
+ * table after an overflow, the longest lane call and the longest release in
+ * milliseconds. */
 gba_status gba_server_counters(gba_server* sv, int64_t* lane_calls, int64_t* batch_failures, int64_t* ws_releases,
-                               double* lane_ms_max, double* release_ms_max);
+                               int64_t* regrows, double* lane_ms_max, double* release_ms_max);
 /* The latest failed request's lane and message, else the latest refused submit's. */
 const char* gba_server_last_error(const gba_server* sv);
 /* Finishes every submitted request, then stops the lanes and frees them. */
